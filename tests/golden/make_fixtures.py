@@ -1,0 +1,48 @@
+"""Copy the reference's own golden decks into tests/golden/.
+
+The HAMS-MREL reference ships its regression data as input decks
+(ControlFile.in, .pnl meshes, Hydrostatic.in, generalized-mode files) with
+the HAMS-format outputs its Fortran build produced.  The GPU box used for the
+CUDA tests has no copy of the reference, so the decks the parity tests need
+are committed here.  Run this script in a checkout that has the reference
+next to it:
+
+    python tests/golden/make_fixtures.py /path/to/HAMS-MREL
+
+Decks copied (reference path -> fixture name):
+  test/data/config1                       -> config1   (3 bodies x 234 panels, h = 70 m)
+  examples/example2_multi_bodies_wave_fields -> example2 (10 bodies x 234, h = 14.5 m)
+  examples/example5_single_body           -> example5  (1 body, 234 panels + 383 lid panels)
+Only the HAMS-format outputs (OAMASS/ODAMPING/OEXFOR) are kept as expected data.
+"""
+import os
+import shutil
+import sys
+
+DECKS = {
+    "config1": ("test/data/config1/input", "test/data/config1/expected_output"),
+    "example2": ("examples/example2_multi_bodies_wave_fields/Input",
+                 "examples/example2_multi_bodies_wave_fields/Output/Hams_format"),
+    "example5": ("examples/example5_single_body/Input",
+                 "examples/example5_single_body/Output/Hams_format"),
+}
+OUTPUTS = [f"{k}{m}.txt" for k in ("OAMASS", "ODAMPING", "OEXFOR") for m in range(1, 7)]
+
+
+def main(ref_root: str) -> None:
+    here = os.path.dirname(os.path.abspath(__file__))
+    for name, (inp, exp) in DECKS.items():
+        dst_in = os.path.join(here, name, "input")
+        dst_exp = os.path.join(here, name, "expected")
+        os.makedirs(dst_in, exist_ok=True)
+        os.makedirs(dst_exp, exist_ok=True)
+        src_in = os.path.join(ref_root, inp)
+        for f in sorted(os.listdir(src_in)):
+            shutil.copyfile(os.path.join(src_in, f), os.path.join(dst_in, f))
+        for f in OUTPUTS:
+            shutil.copyfile(os.path.join(ref_root, exp, f), os.path.join(dst_exp, f))
+        print(f"{name}: {len(os.listdir(dst_in))} input files, {len(OUTPUTS)} expected files")
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
