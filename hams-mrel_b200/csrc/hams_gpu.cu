@@ -1,0 +1,1017 @@
+// hams_gpu.cu -- B200 per-frequency BEM build-and-solve behind the C ABI of
+// include/hams_gpu.h.
+//
+// Device pipeline of one frequency (N hull panels, NL lid panels, TN = N+NL
+// field points, NB bodies, NBETA headings):
+//   1. green kernels  -- per Green-function branch, over the branch's sorted
+//      pair list: FINGREEN3D / INFGREEN3D for the pair, fused with the
+//      BODINT_MULTI_LEFT / RBC algebra, writes A(I,J) (double layer) and
+//      S(I,J) (single layer) in FP64 complex, column-major TN x N.
+//   2. rhs kernels    -- B_rad(I,6b+m) = sum_{J in b} S(I,J) n_m(J) and
+//      B_dif(I,beta) = -sum_J S(I,J) (grad phi_I . n)(J), chunked over J with
+//      a fixed-order final sum (deterministic).
+//   3. lid rows       -- C = A^T A, D = A^T B (plain transpose, as
+//      AssbMatx_irrMulti.f90:151-169,300-315,447-460) with cuBLAS ZGEMM.
+//   4. solve          -- FP64: cuSOLVER ZGETRF/ZGETRS.  Mixed: complex64
+//      CGETRF of a rounded copy, then FP64 iterative refinement with the
+//      FP64 matrix kept in HBM (residual r = b - A x by ZGEMM, correction by
+//      CGETRS, update in FP64).
+//   5. force kernels  -- RFORCE_MULTI / EFORCE_MULTI reductions.
+// Frequency-independent work (Rankine panel integrals, branch sort of the
+// pairs) happens once in hams_ctx_create.
+#include <cublas_v2.h>
+#include <cuda_runtime.h>
+#include <cusolverDn.h>
+
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/hams_gpu.h"
+#include "green.cuh"
+#include "rankine.cuh"
+
+using hams::cplx;
+using hams::grn4;
+
+// ---------------------------------------------------------------------------
+// error reporting
+// ---------------------------------------------------------------------------
+static thread_local std::string g_err;
+
+static int fail(int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_err = buf;
+  return code;
+}
+
+#define CU(call)                                                                                \
+  do {                                                                                          \
+    cudaError_t e_ = (call);                                                                    \
+    if (e_ != cudaSuccess) return fail(HAMS_ERR_CUDA, "%s:%d %s: %s", __FILE__, __LINE__, #call, \
+                                       cudaGetErrorString(e_));                                 \
+  } while (0)
+#define CUB_(call)                                                                                       \
+  do {                                                                                                   \
+    cublasStatus_t e_ = (call);                                                                          \
+    if (e_ != CUBLAS_STATUS_SUCCESS) return fail(HAMS_ERR_CUDA, "%s:%d %s: cublas status %d", __FILE__, \
+                                                 __LINE__, #call, (int)e_);                              \
+  } while (0)
+#define CUS(call)                                                                                          \
+  do {                                                                                                     \
+    cusolverStatus_t e_ = (call);                                                                          \
+    if (e_ != CUSOLVER_STATUS_SUCCESS) return fail(HAMS_ERR_CUDA, "%s:%d %s: cusolver status %d", __FILE__, \
+                                                   __LINE__, #call, (int)e_);                              \
+  } while (0)
+#define TRY(call)           \
+  do {                      \
+    int rc_ = (call);       \
+    if (rc_ < 0) return rc_; \
+  } while (0)
+
+// ---------------------------------------------------------------------------
+// geometry as the kernels see it
+// ---------------------------------------------------------------------------
+struct DevGeom {
+  int n, tn, nb;
+  const double* xq;    // source centres (n,3)
+  const double* fxyz;  // field points (tn,3): hull centres then lid centres
+  const double* ds;    // (n)
+  const double* pnsz;  // (n)
+  const double* nrm;   // (n,6)
+  const double* vtx;   // (n,4,3): vertices of each source panel (v = 0..3)
+  const int* ncn;      // (n)
+  const int* body;     // (n) body of each source panel
+  const int* bstart;   // (nb+1)
+};
+
+struct WaveDev {
+  double v, wk, w1, h;
+  int limit;  // 0 regular, 1 zero frequency, 2 infinite frequency
+};
+
+__device__ __forceinline__ int near_flag(const DevGeom& g, int i, int j) {
+  double dx = g.fxyz[i] - g.xq[j], dy = g.fxyz[i + g.tn] - g.xq[j + g.n], dz = g.fxyz[i + 2 * g.tn] - g.xq[j + 2 * g.n];
+  return sqrt(dx * dx + dy * dy + dz * dz) <= 50.0 * g.pnsz[j] ? 1 : 0;
+}
+
+// ---------------------------------------------------------------------------
+// setup kernels
+// ---------------------------------------------------------------------------
+// Rankine integrals of every (field, source) pair: rs = FLAG * SIJ,
+// rd = FLAG * DIJ . n_J (the only Rankine quantities the assembly uses).
+__global__ void k_rankine(DevGeom g, double* __restrict__ rs, double* __restrict__ rd) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  int j = blockIdx.y;
+  if (i >= g.tn) return;
+  size_t p = (size_t)i + (size_t)j * g.tn;
+  if (!near_flag(g, i, j)) {
+    rs[p] = 0.0;
+    rd[p] = 0.0;
+    return;
+  }
+  double xf[3] = {g.fxyz[i], g.fxyz[i + g.tn], g.fxyz[i + 2 * g.tn]};
+  hams::rk4 r;
+  if (g.ncn[j] == 3) {
+    double q[3][3];
+    for (int v = 0; v < 3; ++v)
+      for (int c = 0; c < 3; ++c) q[v][c] = g.vtx[(size_t)j * 12 + v * 3 + c];
+    r = hams::sglint_tri(xf, q);
+  } else {
+    double q[4][3];
+    for (int v = 0; v < 4; ++v)
+      for (int c = 0; c < 3; ++c) q[v][c] = g.vtx[(size_t)j * 12 + v * 3 + c];
+    r = hams::sglint_quad(xf, q);
+  }
+  rs[p] = r.s;
+  rd[p] = r.dx * g.nrm[j] + r.dy * g.nrm[j + g.n] + r.dz * g.nrm[j + 2 * g.n];
+}
+
+// Sort key of a pair: branch (2 bits) and epsilon-table length (8 bits).
+__global__ void k_pair_keys(DevGeom g, double h, uint32_t* __restrict__ keys, uint32_t* __restrict__ idx) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  int j = blockIdx.y;
+  if (i >= g.tn) return;
+  size_t p = (size_t)i + (size_t)j * g.tn;
+  double dx = g.xq[j] - g.fxyz[i], dy = g.xq[j + g.n] - g.fxyz[i + g.tn];
+  double rr = sqrt(dx * dx + dy * dy);
+  int b = hams::fin_branch(rr, h);
+  int nt = hams::fin_terms(rr, h);
+  keys[p] = (uint32_t)(b << 8) | (uint32_t)(nt & 0xff);
+  idx[p] = (uint32_t)p;
+}
+
+// ---------------------------------------------------------------------------
+// per-frequency assembly: Green function fused with the pair algebra
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void store_pair(const DevGeom& g, size_t p, int i, int j, const grn4& G,
+                                           const double* __restrict__ rs, const double* __restrict__ rd,
+                                           double2* __restrict__ A, double2* __restrict__ S) {
+  double ds = g.ds[j], n1 = g.nrm[j], n2 = g.nrm[j + g.n], n3 = g.nrm[j + 2 * g.n];
+  double are = rd[p] + ds * (G.g[1].re * n1 + G.g[2].re * n2 + G.g[3].re * n3);
+  double aim = ds * (G.g[1].im * n1 + G.g[2].im * n2 + G.g[3].im * n3);
+  if (i == j) are += 2.0 * 3.141592653589793;  // A(I,I) = 2 pi on hull rows (AssbMatxMulti.f90:75)
+  A[p] = make_double2(are, aim);
+  S[p] = make_double2(rs[p] + G.g[0].re * ds, G.g[0].im * ds);
+}
+
+template <int BR>
+__global__ void __launch_bounds__(128) k_green_fin(DevGeom g, WaveDev w, const double* __restrict__ wvn,
+                                                   const uint32_t* __restrict__ pairs, long long count,
+                                                   const double* __restrict__ rs, const double* __restrict__ rd,
+                                                   double2* __restrict__ A, double2* __restrict__ S, int* ovf) {
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= count) return;
+  size_t p = pairs[t];
+  int i = (int)(p % (size_t)g.tn), j = (int)(p / (size_t)g.tn);
+  int flag = near_flag(g, i, j);
+  double xp = g.fxyz[i], yp = g.fxyz[i + g.tn], zp = g.fxyz[i + 2 * g.tn];
+  double xq = g.xq[j], yq = g.xq[j + g.n], zq = g.xq[j + 2 * g.n];
+  grn4 G;
+  if (w.limit) {
+    G = hams::green_limit(w.limit == 2, xq, xp, yq, yp, zq, zp, flag);
+  } else {
+    int o = 0;
+    if (BR == hams::kPidcock || BR == hams::kEigenE) {
+      hams::SeriesScratch sc;
+      G = hams::fingreen3d<BR>(xq, xp, yq, yp, zq, zp, w.v, wvn, w.h, flag, &sc, &o);
+    } else {
+      G = hams::fingreen3d<BR>(xq, xp, yq, yp, zq, zp, w.v, wvn, w.h, flag, nullptr, &o);
+    }
+    if (o) atomicOr(ovf, 1);
+  }
+  store_pair(g, p, i, j, G, rs, rd, A, S);
+}
+
+__global__ void __launch_bounds__(128) k_green_inf(DevGeom g, WaveDev w, const double* __restrict__ rs,
+                                                   const double* __restrict__ rd, double2* __restrict__ A,
+                                                   double2* __restrict__ S) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  int j = blockIdx.y;
+  if (i >= g.tn) return;
+  size_t p = (size_t)i + (size_t)j * g.tn;
+  int flag = near_flag(g, i, j);
+  double xp = g.fxyz[i], yp = g.fxyz[i + g.tn], zp = g.fxyz[i + 2 * g.tn];
+  double xq = g.xq[j], yq = g.xq[j + g.n], zq = g.xq[j + 2 * g.n];
+  grn4 G = w.limit ? hams::green_limit(w.limit == 2, xq, xp, yq, yp, zq, zp, flag)
+                   : hams::infgreen3d(xq, xp, yq, yp, zq, zp, w.v, flag);
+  store_pair(g, p, i, j, G, rs, rd, A, S);
+}
+
+// ---------------------------------------------------------------------------
+// incident wave (PatclVelct.f90:42-123)
+// ---------------------------------------------------------------------------
+struct IncWave {
+  double w0, wk0, h, amp, g, xw0, xw1;
+};
+
+__host__ __device__ inline IncWave inc_params(const WaveDev& w, double amp, double g, double xw0, double xw1) {
+  IncWave o;
+  if (fabs(w.v) < HAMS_F4(1.E-8)) {
+    o.w0 = HAMS_F4(1.E-20);
+    o.wk0 = HAMS_F4(1.E-20);
+  } else if (fabs(w.v + 1.0) < HAMS_F4(1.E-8)) {
+    o.w0 = HAMS_F4(1.E+20);
+    o.wk0 = HAMS_F4(1.E+20);
+  } else {
+    o.w0 = w.w1;
+    o.wk0 = w.wk;
+  }
+  o.h = w.h;
+  o.amp = amp;
+  o.g = g;
+  o.xw0 = xw0;
+  o.xw1 = xw1;
+  return o;
+}
+
+// grad(phi_I) . n at (x,y,z) for heading beta (DINP, PatclVelct.f90:83)
+__device__ __forceinline__ cplx dinp_n(const IncWave& q, double x, double y, double z, double beta, double n1,
+                                        double n2, double n3) {
+  double sb, cb, s, c;
+  sincos(beta, &sb, &cb);
+  double wkx = q.wk0 * ((x - q.xw0) * cb + (y - q.xw1) * sb);
+  sincos(wkx, &s, &c);
+  double fh, fv;
+  if (q.h < 0.0) {
+    fh = fv = exp(q.wk0 * z);
+  } else {
+    double sh = sinh(q.wk0 * q.h);
+    fh = cosh(q.wk0 * (z + q.h)) / sh;
+    fv = sinh(q.wk0 * (z + q.h)) / sh;
+  }
+  // DPOX/CI = -i * w0 amp fh e^{i wkx} cos(beta); DPOZ/CI = -w0 amp fv e^{i wkx}
+  double a = q.w0 * q.amp;
+  cplx e = hams::cmk(c, s);
+  cplx dx = hams::cmk(e.im, -e.re) * (a * fh * cb);
+  cplx dy = hams::cmk(e.im, -e.re) * (a * fh * sb);
+  cplx dz = e * (-a * fv);
+  return dx * n1 + dy * n2 + dz * n3;
+}
+
+// phi_I at (x,y,z) (VINP, PatclVelct.f90:42)
+__device__ __forceinline__ cplx vinp(const IncWave& q, double x, double y, double z, double beta) {
+  double sb, cb, s, c;
+  sincos(beta, &sb, &cb);
+  double wkx = q.wk0 * ((x - q.xw0) * cb + (y - q.xw1) * sb);
+  sincos(wkx, &s, &c);
+  cplx e = hams::cmk(c, s);
+  if (q.h < 0.0 || q.h > 500.0) {
+    // (-i amp g / w0 e^{k z} e^{i wkx}) / i
+    return e * (-q.amp * q.g / q.w0 * exp(q.wk0 * z));
+  }
+  double dum = -q.amp * q.w0 / (q.wk0 * sinh(q.wk0 * q.h));
+  return e * (dum * cosh(q.wk0 * (z + q.h)));
+}
+
+// w(J,beta) = grad(phi_I)(x_J) . n_J for every source panel and heading
+__global__ void k_dbc_weights(DevGeom g, WaveDev w, IncWave q, const double* __restrict__ beta, int nbeta,
+                              double2* __restrict__ wd) {
+  int j = blockIdx.x * blockDim.x + threadIdx.x;
+  int b = blockIdx.y;
+  if (j >= g.n || b >= nbeta) return;
+  cplx r = dinp_n(q, g.xq[j], g.xq[j + g.n], g.xq[j + 2 * g.n], beta[b], g.nrm[j], g.nrm[j + g.n],
+                  g.nrm[j + 2 * g.n]);
+  wd[j + (size_t)b * g.n] = make_double2(r.re, r.im);
+}
+
+// ---------------------------------------------------------------------------
+// right-hand sides: chunked reductions over source panels
+// ---------------------------------------------------------------------------
+constexpr int kChunk = 256;  // source panels per chunk (chunks never straddle bodies)
+
+// part(c, I, k): k < 6 radiation mode k of the chunk's body, k >= 6 heading k-6.
+__global__ void __launch_bounds__(128) k_rhs_partial(DevGeom g, const double2* __restrict__ S,
+                                                     const int2* __restrict__ chunks, const double2* __restrict__ wd,
+                                                     int nbeta, double2* __restrict__ part) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  int c = blockIdx.y;
+  if (i >= g.tn) return;
+  int j0 = chunks[c].x, j1 = chunks[c].y;
+  int nk = 6 + nbeta;
+  double2* out = part + ((size_t)c * g.tn + i) * nk;
+  double rr[6] = {0, 0, 0, 0, 0, 0}, ri[6] = {0, 0, 0, 0, 0, 0};
+  for (int j = j0; j < j1; ++j) {
+    double2 s = S[(size_t)i + (size_t)j * g.tn];
+#pragma unroll
+    for (int m = 0; m < 6; ++m) {
+      double nm = g.nrm[j + (size_t)m * g.n];
+      rr[m] += s.x * nm;
+      ri[m] += s.y * nm;
+    }
+  }
+  for (int m = 0; m < 6; ++m) out[m] = make_double2(rr[m], ri[m]);
+  for (int b0 = 0; b0 < nbeta; b0 += 8) {
+    double dr[8] = {0, 0, 0, 0, 0, 0, 0, 0}, di[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    int nbb = min(8, nbeta - b0);
+    for (int j = j0; j < j1; ++j) {
+      double2 s = S[(size_t)i + (size_t)j * g.tn];
+#pragma unroll
+      for (int b = 0; b < 8; ++b)
+        if (b < nbb) {
+          double2 wv = wd[j + (size_t)(b0 + b) * g.n];
+          dr[b] -= s.x * wv.x - s.y * wv.y;
+          di[b] -= s.x * wv.y + s.y * wv.x;
+        }
+    }
+    for (int b = 0; b < nbb; ++b) out[6 + b0 + b] = make_double2(dr[b], di[b]);
+  }
+}
+
+// B (tn, 6nb + nbeta): radiation columns of body b, then diffraction columns.
+__global__ void k_rhs_final(int tn, int nb, int nchunks, const int* __restrict__ chunk_body,
+                            const double2* __restrict__ part, int nbeta, double2* __restrict__ B) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= tn) return;
+  int nk = 6 + nbeta, ldb = tn;
+  for (int b = 0; b < nb; ++b)
+    for (int m = 0; m < 6; ++m) B[i + (size_t)(6 * b + m) * ldb] = make_double2(0.0, 0.0);
+  for (int c = 0; c < nchunks; ++c) {
+    const double2* p = part + ((size_t)c * tn + i) * nk;
+    int b = chunk_body[c];
+    for (int m = 0; m < 6; ++m) {
+      double2 v = B[i + (size_t)(6 * b + m) * ldb];
+      B[i + (size_t)(6 * b + m) * ldb] = make_double2(v.x + p[m].x, v.y + p[m].y);
+    }
+  }
+  for (int k = 0; k < nbeta; ++k) {
+    double sr = 0.0, si = 0.0;
+    for (int c = 0; c < nchunks; ++c) {
+      const double2* p = part + ((size_t)c * tn + i) * nk;
+      sr += p[6 + k].x;
+      si += p[6 + k].y;
+    }
+    B[i + (size_t)(6 * nb + k) * ldb] = make_double2(sr, si);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// reductions (RFORCE_MULTI / EFORCE_MULTI)
+// ---------------------------------------------------------------------------
+// One block per (body bm, mode k, solution column col).
+//   col < 6nb : amas(6bm+k, col) = rho sum DS n_k Re X ; bdmp = rho w1 sum DS n_k Im X
+//   col >= 6nb: exfc(beta, 6bm+k) = i w1 rho sum (X + phi_I) DS n_k
+__global__ void k_forces(DevGeom g, WaveDev w, IncWave q, const double* __restrict__ beta, int nbeta, int isol,
+                         double rho, const double2* __restrict__ X, int ldx, double* __restrict__ amas,
+                         double* __restrict__ bdmp, double2* __restrict__ exfc) {
+  int bm = blockIdx.x, k = blockIdx.y, col = blockIdx.z;
+  int ndof = 6 * g.nb;
+  int i0 = g.bstart[bm], i1 = g.bstart[bm + 1];
+  double sr = 0.0, si = 0.0;
+  for (int i = i0 + threadIdx.x; i < i1; i += blockDim.x) {
+    double2 x = X[i + (size_t)col * ldx];
+    if (col >= ndof && isol == 1) {
+      cplx f = vinp(q, g.xq[i], g.xq[i + g.n], g.xq[i + 2 * g.n], beta[col - ndof]);
+      x.x += f.re;
+      x.y += f.im;
+    }
+    double wgt = g.ds[i] * g.nrm[i + (size_t)k * g.n];
+    sr += x.x * wgt;
+    si += x.y * wgt;
+  }
+  __shared__ double shr[256], shi[256];
+  shr[threadIdx.x] = sr;
+  shi[threadIdx.x] = si;
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s) {
+      shr[threadIdx.x] += shr[threadIdx.x + s];
+      shi[threadIdx.x] += shi[threadIdx.x + s];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x != 0) return;
+  sr = shr[0];
+  si = shi[0];
+  if (col < ndof) {
+    amas[(6 * bm + k) + (size_t)col * ndof] = rho * sr;
+    bdmp[(6 * bm + k) + (size_t)col * ndof] = rho * w.w1 * si;
+  } else {
+    // i * w1 * rho * (sr + i si)
+    exfc[(col - ndof) + (size_t)(6 * bm + k) * nbeta] = make_double2(-w.w1 * rho * si, w.w1 * rho * sr);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// mixed precision helpers
+// ---------------------------------------------------------------------------
+__global__ void k_z2c(const double2* __restrict__ a, float2* __restrict__ b, size_t n) {
+  size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  for (; t < n; t += (size_t)gridDim.x * blockDim.x) b[t] = make_float2((float)a[t].x, (float)a[t].y);
+}
+__global__ void k_c2z_add(const float2* __restrict__ a, double2* __restrict__ b, size_t n) {
+  size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  for (; t < n; t += (size_t)gridDim.x * blockDim.x) b[t] = make_double2(b[t].x + (double)a[t].x, b[t].y + (double)a[t].y);
+}
+__global__ void k_c2z(const float2* __restrict__ a, double2* __restrict__ b, size_t n) {
+  size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  for (; t < n; t += (size_t)gridDim.x * blockDim.x) b[t] = make_double2((double)a[t].x, (double)a[t].y);
+}
+// per-column max |r| / max |b| ratios -> out[col]
+__global__ void k_colnorm_ratio(const double2* __restrict__ r, const double2* __restrict__ b, int n, int ld,
+                                double* __restrict__ out) {
+  int col = blockIdx.x;
+  double mr = 0.0, mb = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    double2 x = r[i + (size_t)col * ld], y = b[i + (size_t)col * ld];
+    mr = fmax(mr, fabs(x.x) + fabs(x.y));
+    mb = fmax(mb, fabs(y.x) + fabs(y.y));
+  }
+  __shared__ double s1[256], s2[256];
+  s1[threadIdx.x] = mr;
+  s2[threadIdx.x] = mb;
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s) {
+      s1[threadIdx.x] = fmax(s1[threadIdx.x], s1[threadIdx.x + s]);
+      s2[threadIdx.x] = fmax(s2[threadIdx.x], s2[threadIdx.x + s]);
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[col] = s2[0] > 0.0 ? s1[0] / s2[0] : s1[0];
+}
+
+// ---------------------------------------------------------------------------
+// batch Green evaluation (hams_eval_green)
+// ---------------------------------------------------------------------------
+__global__ void k_eval_green(int npts, const double* __restrict__ pts, const int* __restrict__ flag, WaveDev w,
+                             const double* __restrict__ wvn, double2* __restrict__ out, int* ovf) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= npts) return;
+  double xq = pts[t], yq = pts[t + npts], zq = pts[t + 2 * (size_t)npts];
+  double xp = pts[t + 3 * (size_t)npts], yp = pts[t + 4 * (size_t)npts], zp = pts[t + 5 * (size_t)npts];
+  grn4 G;
+  if (w.limit) {
+    G = hams::green_limit(w.limit == 2, xq, xp, yq, yp, zq, zp, flag[t]);
+  } else if (w.h < 0.0) {
+    G = hams::infgreen3d(xq, xp, yq, yp, zq, zp, w.v, flag[t]);
+  } else {
+    hams::SeriesScratch sc;
+    int o = 0;
+    double rr = sqrt((xq - xp) * (xq - xp) + (yq - yp) * (yq - yp));
+    switch (hams::fin_branch(rr, w.h)) {
+      case hams::kLinton: G = hams::fingreen3d<hams::kLinton>(xq, xp, yq, yp, zq, zp, w.v, wvn, w.h, flag[t], &sc, &o); break;
+      case hams::kPidcock: G = hams::fingreen3d<hams::kPidcock>(xq, xp, yq, yp, zq, zp, w.v, wvn, w.h, flag[t], &sc, &o); break;
+      case hams::kEigenE: G = hams::fingreen3d<hams::kEigenE>(xq, xp, yq, yp, zq, zp, w.v, wvn, w.h, flag[t], &sc, &o); break;
+      default: G = hams::fingreen3d<hams::kEigen>(xq, xp, yq, yp, zq, zp, w.v, wvn, w.h, flag[t], &sc, &o); break;
+    }
+    if (o) atomicOr(ovf, 1);
+  }
+  for (int k = 0; k < 4; ++k) out[t + (size_t)k * npts] = make_double2(G.g[k].re, G.g[k].im);
+}
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+template <class T>
+struct DBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  DBuf() = default;
+  DBuf(const DBuf&) = delete;
+  DBuf& operator=(const DBuf&) = delete;
+  ~DBuf() { release(); }
+  int alloc(size_t count) {
+    if (count <= n && p) return 0;
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+    if (count == 0) return 0;
+    if (cudaMalloc(&p, count * sizeof(T)) != cudaSuccess) {
+      p = nullptr;
+      return fail(HAMS_ERR_NOMEM, "cudaMalloc of %zu bytes failed", count * sizeof(T));
+    }
+    n = count;
+    return 0;
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+};
+
+struct hams_ctx {
+  int dev = 0;
+  cudaStream_t st = nullptr;
+  cublasHandle_t blas = nullptr;
+  cusolverDnHandle_t solver = nullptr;
+  hams_opts opts{};
+  int n = 0, nl = 0, tn = 0, nb = 0;
+  std::vector<int> body_nelem;
+  // geometry
+  DBuf<double> xq, fxyz, ds, pnsz, nrm, vtx;
+  DBuf<int> ncn, body, bstart;
+  DevGeom g{};
+  // frequency-independent pair data
+  DBuf<double> rs, rd;
+  DBuf<uint32_t> pairs;
+  long long bin_off[5] = {0, 0, 0, 0, 0};  // [branch] start offsets into pairs, bin_off[4] = total
+  // chunks of source panels for the RHS reduction
+  std::vector<int2> chunks_h;
+  DBuf<int2> chunks;
+  DBuf<int> chunk_body;
+  // per-frequency buffers
+  DBuf<double2> A, S, B, part, wd, C, D, X, R;
+  DBuf<float2> Af, Xf;
+  DBuf<double> wvn, beta, outbuf, colratio;
+  DBuf<int> ipiv, info, ovf;
+  DBuf<char> work;
+  DBuf<char> work32;
+  // timing: ev[0..5] stage marks, evb[0..4] branch marks, evf after the factorisation
+  cudaEvent_t ev[6] = {};
+  cudaEvent_t evb[5] = {};
+  cudaEvent_t evf = nullptr;
+  static constexpr int kTimings = 15;
+  double last_ms[kTimings] = {};
+  std::atomic<long long> launches{0};
+  int refine_sweeps = 0;
+};
+
+static int launch_check(hams_ctx* c, int count = 1) {
+  c->launches += count;
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return fail(HAMS_ERR_CUDA, "kernel launch: %s", cudaGetErrorString(e));
+  return 0;
+}
+
+extern "C" int hams_wave_properties(int32_t inft, double value, double depth, double g, int32_t sybo_kk,
+                                    hams_wave* o);
+
+extern "C" const char* hams_last_error(void) { return g_err.c_str(); }
+
+extern "C" void hams_ctx_destroy(hams_ctx* c) {
+  if (!c) return;
+  cudaSetDevice(c->dev);
+  if (c->st) cudaStreamSynchronize(c->st);
+  c->xq.release(); c->fxyz.release(); c->ds.release(); c->pnsz.release(); c->nrm.release(); c->vtx.release();
+  c->ncn.release(); c->body.release(); c->bstart.release(); c->rs.release(); c->rd.release(); c->pairs.release();
+  c->chunks.release(); c->chunk_body.release(); c->A.release(); c->S.release(); c->B.release(); c->part.release();
+  c->wd.release(); c->C.release(); c->D.release(); c->X.release(); c->R.release(); c->Af.release(); c->Xf.release();
+  c->wvn.release(); c->beta.release(); c->outbuf.release(); c->colratio.release(); c->ipiv.release();
+  c->info.release(); c->ovf.release(); c->work.release(); c->work32.release();
+  for (auto& e : c->ev)
+    if (e) cudaEventDestroy(e);
+  for (auto& e : c->evb)
+    if (e) cudaEventDestroy(e);
+  if (c->evf) cudaEventDestroy(c->evf);
+  if (c->solver) cusolverDnDestroy(c->solver);
+  if (c->blas) cublasDestroy(c->blas);
+  if (c->st) cudaStreamDestroy(c->st);
+  delete c;
+}
+
+static int ctx_setup(hams_ctx* c, const hams_geom* geo) {
+  const int n = c->n, tn = c->tn, nb = c->nb;
+  // host staging: source centres, normals, vertices, field points
+  std::vector<double> xq(3 * (size_t)n), fx(3 * (size_t)tn), vtx(12 * (size_t)n, 0.0);
+  std::vector<int> body(n), bst(nb + 1, 0);
+  for (int k = 0; k < 3; ++k)
+    for (int i = 0; i < n; ++i) {
+      xq[i + (size_t)k * n] = geo->xyz_p[i + (size_t)k * n];
+      fx[i + (size_t)k * tn] = geo->xyz_p[i + (size_t)k * n];
+    }
+  for (int k = 0; k < 3; ++k)
+    for (int i = 0; i < c->nl; ++i) fx[n + i + (size_t)k * tn] = geo->ixyz_p[i + (size_t)k * c->nl];
+  for (int j = 0; j < n; ++j) {
+    int nc = geo->ncn[j];
+    if (nc != 3 && nc != 4) return fail(HAMS_ERR_ARG, "panel %d has %d vertices (3 or 4 expected)", j + 1, nc);
+    for (int v = 0; v < nc; ++v) {
+      int id = geo->ncon[j + (size_t)v * n];
+      if (id < 1 || id > geo->ntnd) return fail(HAMS_ERR_ARG, "panel %d vertex %d: node id %d out of range", j + 1, v + 1, id);
+      for (int k = 0; k < 3; ++k) vtx[(size_t)j * 12 + v * 3 + k] = geo->xyz[(id - 1) + (size_t)k * geo->ntnd];
+    }
+  }
+  int off = 0;
+  for (int b = 0; b < nb; ++b) {
+    bst[b] = off;
+    for (int i = 0; i < geo->body_nelem[b]; ++i) body[off + i] = b;
+    off += geo->body_nelem[b];
+  }
+  bst[nb] = off;
+  if (off != n) return fail(HAMS_ERR_ARG, "body_nelem sums to %d, nelem is %d", off, n);
+  TRY(c->xq.alloc(3 * (size_t)n)); TRY(c->fxyz.alloc(3 * (size_t)tn)); TRY(c->ds.alloc(n)); TRY(c->pnsz.alloc(n));
+  TRY(c->nrm.alloc(6 * (size_t)n)); TRY(c->vtx.alloc(12 * (size_t)n)); TRY(c->ncn.alloc(n)); TRY(c->body.alloc(n));
+  TRY(c->bstart.alloc(nb + 1));
+  CU(cudaMemcpyAsync(c->xq.p, xq.data(), 3 * (size_t)n * 8, cudaMemcpyHostToDevice, c->st));
+  CU(cudaMemcpyAsync(c->fxyz.p, fx.data(), 3 * (size_t)tn * 8, cudaMemcpyHostToDevice, c->st));
+  CU(cudaMemcpyAsync(c->ds.p, geo->ds, (size_t)n * 8, cudaMemcpyHostToDevice, c->st));
+  CU(cudaMemcpyAsync(c->pnsz.p, geo->pnsz, (size_t)n * 8, cudaMemcpyHostToDevice, c->st));
+  CU(cudaMemcpyAsync(c->nrm.p, geo->dxyz, 6 * (size_t)n * 8, cudaMemcpyHostToDevice, c->st));
+  CU(cudaMemcpyAsync(c->vtx.p, vtx.data(), 12 * (size_t)n * 8, cudaMemcpyHostToDevice, c->st));
+  CU(cudaMemcpyAsync(c->ncn.p, geo->ncn, (size_t)n * 4, cudaMemcpyHostToDevice, c->st));
+  CU(cudaMemcpyAsync(c->body.p, body.data(), (size_t)n * 4, cudaMemcpyHostToDevice, c->st));
+  CU(cudaMemcpyAsync(c->bstart.p, bst.data(), (size_t)(nb + 1) * 4, cudaMemcpyHostToDevice, c->st));
+  c->g = DevGeom{n, tn, nb, c->xq.p, c->fxyz.p, c->ds.p, c->pnsz.p, c->nrm.p, c->vtx.p, c->ncn.p, c->body.p, c->bstart.p};
+
+  // Rankine tables
+  size_t np = (size_t)tn * n;
+  TRY(c->rs.alloc(np));
+  TRY(c->rd.alloc(np));
+  dim3 grid2((tn + 127) / 128, n);
+  k_rankine<<<grid2, 128, 0, c->st>>>(c->g, c->rs.p, c->rd.p);
+  TRY(launch_check(c));
+
+  // branch-sorted pair list (finite depth)
+  if (c->opts.depth >= 0.0) {
+    if (np > 0xffffffffull) return fail(HAMS_ERR_UNSUPPORTED, "%zu pairs exceed the 32-bit pair index", np);
+    DBuf<uint32_t> keys, keys2, idx;
+    TRY(keys.alloc(np)); TRY(keys2.alloc(np)); TRY(idx.alloc(np)); TRY(c->pairs.alloc(np));
+    k_pair_keys<<<grid2, 128, 0, c->st>>>(c->g, c->opts.depth, keys.p, idx.p);
+    TRY(launch_check(c));
+    size_t tmp = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, tmp, keys.p, keys2.p, idx.p, c->pairs.p, np, 0, 10, c->st);
+    DBuf<char> tbuf;
+    TRY(tbuf.alloc(tmp));
+    CU(cub::DeviceRadixSort::SortPairs(tbuf.p, tmp, keys.p, keys2.p, idx.p, c->pairs.p, np, 0, 10, c->st));
+    c->launches += 4;
+    // bin boundaries: first index of each branch in the sorted keys
+    std::vector<uint32_t> hk(np);
+    CU(cudaMemcpyAsync(hk.data(), keys2.p, np * 4, cudaMemcpyDeviceToHost, c->st));
+    CU(cudaStreamSynchronize(c->st));
+    for (int b = 0; b <= 4; ++b)
+      c->bin_off[b] = std::lower_bound(hk.begin(), hk.end(), (uint32_t)(b << 8), [](uint32_t a, uint32_t v) { return a < v; }) - hk.begin();
+    keys.release(); keys2.release(); idx.release(); tbuf.release();
+  }
+
+  // chunks of source panels for the RHS reduction
+  c->chunks_h.clear();
+  std::vector<int> cb;
+  for (int b = 0; b < nb; ++b)
+    for (int j = bst[b]; j < bst[b + 1]; j += kChunk) {
+      c->chunks_h.push_back(make_int2(j, std::min(j + kChunk, bst[b + 1])));
+      cb.push_back(b);
+    }
+  TRY(c->chunks.alloc(c->chunks_h.size()));
+  TRY(c->chunk_body.alloc(cb.size()));
+  CU(cudaMemcpyAsync(c->chunks.p, c->chunks_h.data(), c->chunks_h.size() * sizeof(int2), cudaMemcpyHostToDevice, c->st));
+  CU(cudaMemcpyAsync(c->chunk_body.p, cb.data(), cb.size() * sizeof(int), cudaMemcpyHostToDevice, c->st));
+
+  TRY(c->A.alloc(np));
+  TRY(c->S.alloc(np));
+  TRY(c->wvn.alloc(HAMS_NK));
+  TRY(c->ovf.alloc(1));
+  TRY(c->ipiv.alloc(n));
+  TRY(c->info.alloc(1));
+  CU(cudaStreamSynchronize(c->st));
+  return 0;
+}
+
+extern "C" int hams_ctx_create(const hams_geom* geo, const hams_opts* opts, hams_ctx** out) {
+  g_err.clear();
+  if (!geo || !opts || !out) return fail(HAMS_ERR_ARG, "null argument");
+  *out = nullptr;
+  if (geo->nelem <= 0 || geo->nbody <= 0 || !geo->xyz || !geo->ncn || !geo->ncon || !geo->xyz_p || !geo->ds ||
+      !geo->pnsz || !geo->dxyz || !geo->body_nelem)
+    return fail(HAMS_ERR_ARG, "incomplete geometry");
+  if (geo->isx != 0 || geo->isy != 0)
+    return fail(HAMS_ERR_UNSUPPORTED, "geometric symmetry (ISX/ISY != 0) is not built in the GPU path");
+  if (opts->irsp == 1 && (geo->inelem <= 0 || !geo->ixyz_p)) return fail(HAMS_ERR_ARG, "irsp=1 needs water-plane panels");
+  if (opts->precision != HAMS_PREC_FP64 && opts->precision != HAMS_PREC_MIXED)
+    return fail(HAMS_ERR_ARG, "unknown precision %d", opts->precision);
+  hams_ctx* c = new hams_ctx();
+  c->opts = *opts;
+  c->dev = opts->device;
+  c->n = geo->nelem;
+  c->nl = opts->irsp == 1 ? geo->inelem : 0;
+  c->tn = c->n + c->nl;
+  c->nb = geo->nbody;
+  c->body_nelem.assign(geo->body_nelem, geo->body_nelem + geo->nbody);
+  int rc = 0;
+  if (cudaSetDevice(c->dev) != cudaSuccess) rc = fail(HAMS_ERR_CUDA, "cudaSetDevice(%d) failed", c->dev);
+  if (!rc && cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking) != cudaSuccess)
+    rc = fail(HAMS_ERR_CUDA, "stream creation failed");
+  if (!rc && cublasCreate(&c->blas) != CUBLAS_STATUS_SUCCESS) rc = fail(HAMS_ERR_CUDA, "cublasCreate failed");
+  if (!rc && cusolverDnCreate(&c->solver) != CUSOLVER_STATUS_SUCCESS) rc = fail(HAMS_ERR_CUDA, "cusolverDnCreate failed");
+  if (!rc) {
+    cublasSetStream(c->blas, c->st);
+    cusolverDnSetStream(c->solver, c->st);
+    for (auto& e : c->ev) cudaEventCreate(&e);
+    for (auto& e : c->evb) cudaEventCreate(&e);
+    cudaEventCreate(&c->evf);
+    rc = ctx_setup(c, geo);
+  }
+  if (rc < 0) {
+    std::string keep = g_err;
+    hams_ctx_destroy(c);
+    g_err = keep;
+    return rc;
+  }
+  *out = c;
+  return 0;
+}
+
+static WaveDev wave_dev(const hams_ctx* c, const hams_wave* w) {
+  WaveDev d;
+  d.v = w->v;
+  d.wk = w->wk;
+  d.w1 = w->w1;
+  d.h = c->opts.depth;
+  d.limit = 0;
+  if (fabs(w->v) < HAMS_F4(1.E-8)) d.limit = 1;
+  else if (fabs(w->v + 1.0) < HAMS_F4(1.E-8)) d.limit = 2;
+  return d;
+}
+
+// Assemble A (tn x n) and the right-hand sides B (tn x (6nb+nbeta)) on the device.
+static int assemble_dev(hams_ctx* c, const hams_wave* w, int nbeta) {
+  const int n = c->n, tn = c->tn, nb = c->nb, nrhs = 6 * nb + nbeta;
+  WaveDev wd = wave_dev(c, w);
+  if (c->opts.depth >= 0.0 && !wd.limit) CU(cudaMemcpyAsync(c->wvn.p, w->wvn, HAMS_NK * 8, cudaMemcpyHostToDevice, c->st));
+  CU(cudaMemsetAsync(c->ovf.p, 0, sizeof(int), c->st));
+  CU(cudaEventRecord(c->ev[0], c->st));
+  if (c->opts.depth < 0.0) {
+    dim3 grid((tn + 127) / 128, n);
+    k_green_inf<<<grid, 128, 0, c->st>>>(c->g, wd, c->rs.p, c->rd.p, c->A.p, c->S.p);
+    TRY(launch_check(c));
+  } else {
+    for (int br = 0; br < 4; ++br) {
+      long long cnt = c->bin_off[br + 1] - c->bin_off[br];
+      CU(cudaEventRecord(c->evb[br], c->st));
+      if (cnt <= 0) continue;
+      const uint32_t* lst = c->pairs.p + c->bin_off[br];
+      unsigned blocks = (unsigned)((cnt + 127) / 128);
+      switch (br) {
+        case 0: k_green_fin<0><<<blocks, 128, 0, c->st>>>(c->g, wd, c->wvn.p, lst, cnt, c->rs.p, c->rd.p, c->A.p, c->S.p, c->ovf.p); break;
+        case 1: k_green_fin<1><<<blocks, 128, 0, c->st>>>(c->g, wd, c->wvn.p, lst, cnt, c->rs.p, c->rd.p, c->A.p, c->S.p, c->ovf.p); break;
+        case 2: k_green_fin<2><<<blocks, 128, 0, c->st>>>(c->g, wd, c->wvn.p, lst, cnt, c->rs.p, c->rd.p, c->A.p, c->S.p, c->ovf.p); break;
+        default: k_green_fin<3><<<blocks, 128, 0, c->st>>>(c->g, wd, c->wvn.p, lst, cnt, c->rs.p, c->rd.p, c->A.p, c->S.p, c->ovf.p); break;
+      }
+      TRY(launch_check(c));
+    }
+    CU(cudaEventRecord(c->evb[4], c->st));
+  }
+  CU(cudaEventRecord(c->ev[1], c->st));
+  // right-hand sides
+  int nch = (int)c->chunks_h.size();
+  TRY(c->wd.alloc((size_t)n * std::max(nbeta, 1)));
+  TRY(c->part.alloc((size_t)nch * tn * (6 + nbeta)));
+  TRY(c->B.alloc((size_t)tn * nrhs));
+  if (nbeta > 0) {
+    IncWave q = inc_params(wd, c->opts.amp, c->opts.g, c->opts.xw[0], c->opts.xw[1]);
+    k_dbc_weights<<<dim3((n + 127) / 128, nbeta), 128, 0, c->st>>>(c->g, wd, q, c->beta.p, nbeta, c->wd.p);
+    TRY(launch_check(c));
+  }
+  k_rhs_partial<<<dim3((tn + 127) / 128, nch), 128, 0, c->st>>>(c->g, c->S.p, c->chunks.p, c->wd.p, nbeta, c->part.p);
+  TRY(launch_check(c));
+  k_rhs_final<<<(tn + 127) / 128, 128, 0, c->st>>>(tn, nb, nch, c->chunk_body.p, c->part.p, nbeta, c->B.p);
+  TRY(launch_check(c));
+  CU(cudaEventRecord(c->ev[2], c->st));
+  return 0;
+}
+
+// Solve on the device: X (n x nrhs) from A, B (or normal equations with lids).
+static int solve_dev(hams_ctx* c, int nrhs, int* info_host) {
+  const int n = c->n, tn = c->tn;
+  const cuDoubleComplex one = make_cuDoubleComplex(1.0, 0.0), zero = make_cuDoubleComplex(0.0, 0.0);
+  double2* M = c->A.p;  // matrix to factor
+  double2* rhs = c->B.p;
+  int ldr = tn;
+  if (c->nl > 0) {
+    TRY(c->C.alloc((size_t)n * n));
+    TRY(c->D.alloc((size_t)n * nrhs));
+    CUB_(cublasZgemm(c->blas, CUBLAS_OP_T, CUBLAS_OP_N, n, n, tn, &one, (cuDoubleComplex*)c->A.p, tn,
+                     (cuDoubleComplex*)c->A.p, tn, &zero, (cuDoubleComplex*)c->C.p, n));
+    CUB_(cublasZgemm(c->blas, CUBLAS_OP_T, CUBLAS_OP_N, n, nrhs, tn, &one, (cuDoubleComplex*)c->A.p, tn,
+                     (cuDoubleComplex*)c->B.p, tn, &zero, (cuDoubleComplex*)c->D.p, n));
+    c->launches += 2;
+    M = c->C.p;
+    rhs = c->D.p;
+    ldr = n;
+  }
+  TRY(c->X.alloc((size_t)n * nrhs));
+  CU(cudaMemcpy2DAsync(c->X.p, (size_t)n * 16, rhs, (size_t)ldr * 16, (size_t)n * 16, nrhs, cudaMemcpyDeviceToDevice, c->st));
+  *info_host = 0;
+  if (c->opts.precision == HAMS_PREC_FP64) {
+    int lw = 0;
+    CUS(cusolverDnZgetrf_bufferSize(c->solver, n, n, (cuDoubleComplex*)M, n, &lw));
+    TRY(c->work.alloc((size_t)lw * sizeof(cuDoubleComplex)));
+    // M is overwritten by its factors
+    CUS(cusolverDnZgetrf(c->solver, n, n, (cuDoubleComplex*)M, n, (cuDoubleComplex*)c->work.p, c->ipiv.p, c->info.p));
+    CU(cudaEventRecord(c->evf, c->st));
+    CUS(cusolverDnZgetrs(c->solver, CUBLAS_OP_N, n, nrhs, (cuDoubleComplex*)M, n, c->ipiv.p, (cuDoubleComplex*)c->X.p, n, c->info.p));
+    c->launches += 2;
+    CU(cudaMemcpyAsync(info_host, c->info.p, sizeof(int), cudaMemcpyDeviceToHost, c->st));
+    return 0;
+  }
+  // mixed: complex64 LU of a rounded copy + FP64 iterative refinement
+  size_t nn = (size_t)n * n, nx = (size_t)n * nrhs;
+  TRY(c->Af.alloc(nn));
+  TRY(c->Xf.alloc(nx));
+  TRY(c->R.alloc(nx));
+  TRY(c->colratio.alloc(nrhs));
+  k_z2c<<<1184, 256, 0, c->st>>>(M, c->Af.p, nn);
+  TRY(launch_check(c));
+  int lw = 0;
+  CUS(cusolverDnCgetrf_bufferSize(c->solver, n, n, (cuComplex*)c->Af.p, n, &lw));
+  TRY(c->work32.alloc((size_t)lw * sizeof(cuComplex)));
+  CUS(cusolverDnCgetrf(c->solver, n, n, (cuComplex*)c->Af.p, n, (cuComplex*)c->work32.p, c->ipiv.p, c->info.p));
+  CU(cudaEventRecord(c->evf, c->st));
+  c->launches += 1;
+  CU(cudaMemcpyAsync(info_host, c->info.p, sizeof(int), cudaMemcpyDeviceToHost, c->st));
+  // x0 = LU^-1 b (in complex64), then refine
+  k_z2c<<<592, 256, 0, c->st>>>(c->X.p, c->Xf.p, nx);
+  TRY(launch_check(c));
+  CUS(cusolverDnCgetrs(c->solver, CUBLAS_OP_N, n, nrhs, (cuComplex*)c->Af.p, n, c->ipiv.p, (cuComplex*)c->Xf.p, n, c->info.p));
+  k_c2z<<<592, 256, 0, c->st>>>(c->Xf.p, c->X.p, nx);
+  TRY(launch_check(c, 2));
+  const double tol = c->opts.refine_tol > 0.0 ? c->opts.refine_tol : 1e-12;
+  const int maxit = c->opts.refine_max > 0 ? c->opts.refine_max : 30;
+  const cuDoubleComplex mone = make_cuDoubleComplex(-1.0, 0.0);
+  std::vector<double> ratio(nrhs);
+  double prev = 1e300;
+  c->refine_sweeps = 0;
+  for (int it = 0; it < maxit; ++it) {
+    // R = rhs - M_fp64 X   (M still holds the FP64 matrix)
+    CU(cudaMemcpy2DAsync(c->R.p, (size_t)n * 16, rhs, (size_t)ldr * 16, (size_t)n * 16, nrhs, cudaMemcpyDeviceToDevice, c->st));
+    CUB_(cublasZgemm(c->blas, CUBLAS_OP_N, CUBLAS_OP_N, n, nrhs, n, &mone, (cuDoubleComplex*)M, n,
+                     (cuDoubleComplex*)c->X.p, n, &one, (cuDoubleComplex*)c->R.p, n));
+    k_colnorm_ratio<<<nrhs, 256, 0, c->st>>>(c->R.p, rhs, n, n, c->colratio.p);
+    TRY(launch_check(c, 2));
+    // the relative residual is checked against the rhs column scale
+    CU(cudaMemcpyAsync(ratio.data(), c->colratio.p, nrhs * 8, cudaMemcpyDeviceToHost, c->st));
+    CU(cudaStreamSynchronize(c->st));
+    double worst = 0.0;
+    for (double r : ratio) worst = std::max(worst, r);
+    c->refine_sweeps = it;
+    if (!(worst == worst)) return fail(HAMS_ERR_NUMERIC, "non-finite residual in iterative refinement");
+    if (worst <= tol) break;
+    if (it > 4 && worst > 0.5 * prev) return fail(HAMS_ERR_NUMERIC, "iterative refinement stalled at %.3e", worst);
+    prev = worst;
+    k_z2c<<<592, 256, 0, c->st>>>(c->R.p, c->Xf.p, nx);
+    CUS(cusolverDnCgetrs(c->solver, CUBLAS_OP_N, n, nrhs, (cuComplex*)c->Af.p, n, c->ipiv.p, (cuComplex*)c->Xf.p, n, c->info.p));
+    k_c2z_add<<<592, 256, 0, c->st>>>(c->Xf.p, c->X.p, nx);
+    TRY(launch_check(c, 3));
+  }
+  return 0;
+}
+
+static int forces_dev(hams_ctx* c, const hams_wave* w, int nbeta) {
+  const int nb = c->nb, ndof = 6 * nb, nrhs = ndof + nbeta;
+  WaveDev wd = wave_dev(c, w);
+  IncWave q = inc_params(wd, c->opts.amp, c->opts.g, c->opts.xw[0], c->opts.xw[1]);
+  size_t tot = 2 * (size_t)ndof * ndof + 2 * (size_t)ndof * std::max(nbeta, 1);
+  TRY(c->outbuf.alloc(tot));
+  double* amas = c->outbuf.p;
+  double* bdmp = amas + (size_t)ndof * ndof;
+  double2* exfc = (double2*)(bdmp + (size_t)ndof * ndof);
+  k_forces<<<dim3(nb, 6, nrhs), 256, 0, c->st>>>(c->g, wd, q, c->beta.p, nbeta, c->opts.isol, c->opts.rho, c->X.p,
+                                                 c->n, amas, bdmp, exfc);
+  return launch_check(c);
+}
+
+static int solve_one(hams_ctx* c, const hams_wave* w, int nbeta, const double* beta, double* amas, double* bdmp,
+                     double* exfc) {
+  const int ndof = 6 * c->nb;
+  if (nbeta < 0) return fail(HAMS_ERR_ARG, "nbeta < 0");
+  TRY(c->beta.alloc(std::max(nbeta, 1)));
+  if (nbeta > 0) CU(cudaMemcpyAsync(c->beta.p, beta, (size_t)nbeta * 8, cudaMemcpyHostToDevice, c->st));
+  TRY(assemble_dev(c, w, nbeta));
+  int info = 0;
+  TRY(solve_dev(c, ndof + nbeta, &info));
+  CU(cudaEventRecord(c->ev[3], c->st));
+  TRY(forces_dev(c, w, nbeta));
+  CU(cudaEventRecord(c->ev[4], c->st));
+  double* o = c->outbuf.p;
+  if (amas) CU(cudaMemcpyAsync(amas, o, (size_t)ndof * ndof * 8, cudaMemcpyDeviceToHost, c->st));
+  if (bdmp) CU(cudaMemcpyAsync(bdmp, o + (size_t)ndof * ndof, (size_t)ndof * ndof * 8, cudaMemcpyDeviceToHost, c->st));
+  if (exfc && nbeta > 0)
+    CU(cudaMemcpyAsync(exfc, o + 2 * (size_t)ndof * ndof, (size_t)ndof * nbeta * 16, cudaMemcpyDeviceToHost, c->st));
+  int ovf = 0;
+  CU(cudaMemcpyAsync(&ovf, c->ovf.p, sizeof(int), cudaMemcpyDeviceToHost, c->st));
+  CU(cudaEventRecord(c->ev[5], c->st));
+  CU(cudaStreamSynchronize(c->st));
+  float ms;
+  cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]); c->last_ms[0] = ms;
+  cudaEventElapsedTime(&ms, c->ev[1], c->ev[2]); c->last_ms[1] = ms;
+  cudaEventElapsedTime(&ms, c->ev[2], c->ev[3]); c->last_ms[2] = ms;
+  cudaEventElapsedTime(&ms, c->ev[3], c->ev[4]); c->last_ms[3] = ms;
+  cudaEventElapsedTime(&ms, c->ev[0], c->ev[5]); c->last_ms[4] = ms;
+  for (int b = 0; b < 4; ++b) {
+    c->last_ms[5 + b] = 0.0;
+    c->last_ms[11 + b] = (double)(c->bin_off[b + 1] - c->bin_off[b]);
+    if (c->opts.depth >= 0.0 && cudaEventElapsedTime(&ms, c->evb[b], c->evb[b + 1]) == cudaSuccess) c->last_ms[5 + b] = ms;
+  }
+  if (cudaEventElapsedTime(&ms, c->ev[2], c->evf) == cudaSuccess) c->last_ms[9] = ms;
+  c->last_ms[10] = c->opts.precision == HAMS_PREC_MIXED ? (double)c->refine_sweeps : 0.0;
+  if (ovf) return fail(HAMS_ERR_NUMERIC, "adaptive quadrature stack overflow in the LINTON branch");
+  if (info > 0) return info;  // singular pivot, LAPACK style
+  return 0;
+}
+
+extern "C" int hams_solve_frequency(hams_ctx* c, const hams_wave* w, int32_t nbeta, const double* beta, double* amas,
+                                    double* bdmp, double* exfc) {
+  g_err.clear();
+  if (!c || !w || (nbeta > 0 && !beta)) return fail(HAMS_ERR_ARG, "null argument");
+  if (cudaSetDevice(c->dev) != cudaSuccess) return fail(HAMS_ERR_CUDA, "cudaSetDevice failed");
+  return solve_one(c, w, nbeta, beta, amas, bdmp, exfc);
+}
+
+extern "C" int hams_solve_batch(hams_ctx* c, int32_t nfreq, const hams_wave* waves, int32_t nbeta, const double* beta,
+                                double* amas, double* bdmp, double* exfc) {
+  g_err.clear();
+  if (!c || !waves || nfreq < 0 || (nbeta > 0 && !beta)) return fail(HAMS_ERR_ARG, "null argument");
+  if (cudaSetDevice(c->dev) != cudaSuccess) return fail(HAMS_ERR_CUDA, "cudaSetDevice failed");
+  const int ndof = 6 * c->nb;
+  std::vector<double> a((size_t)ndof * ndof), b((size_t)ndof * ndof), x(2 * (size_t)ndof * std::max(nbeta, 1));
+  int worst = 0;
+  for (int k = 0; k < nfreq; ++k) {
+    int rc = solve_one(c, &waves[k], nbeta, beta, a.data(), b.data(), x.data());
+    if (rc < 0) return rc;
+    if (rc > 0 && !worst) worst = rc;
+    // scatter into (nfreq, ...) column-major arrays with the frequency index leading
+    for (size_t e = 0; e < (size_t)ndof * ndof; ++e) {
+      if (amas) amas[k + e * nfreq] = a[e];
+      if (bdmp) bdmp[k + e * nfreq] = b[e];
+    }
+    if (exfc)
+      for (size_t e = 0; e < (size_t)ndof * nbeta; ++e) {
+        exfc[2 * (k + e * nfreq)] = x[2 * e];
+        exfc[2 * (k + e * nfreq) + 1] = x[2 * e + 1];
+      }
+  }
+  return worst;
+}
+
+extern "C" int hams_assemble(hams_ctx* c, const hams_wave* w, int32_t nbeta, const double* beta, double* amat,
+                             double* brmat, double* bdmat) {
+  g_err.clear();
+  if (!c || !w || (nbeta > 0 && !beta)) return fail(HAMS_ERR_ARG, "null argument");
+  if (cudaSetDevice(c->dev) != cudaSuccess) return fail(HAMS_ERR_CUDA, "cudaSetDevice failed");
+  const int n = c->n, tn = c->tn, ndof = 6 * c->nb, nrhs = ndof + nbeta;
+  TRY(c->beta.alloc(std::max(nbeta, 1)));
+  if (nbeta > 0) CU(cudaMemcpyAsync(c->beta.p, beta, (size_t)nbeta * 8, cudaMemcpyHostToDevice, c->st));
+  TRY(assemble_dev(c, w, nbeta));
+  const double2 *M = c->A.p, *R = c->B.p;
+  int ldm = tn;
+  if (c->nl > 0) {
+    const cuDoubleComplex one = make_cuDoubleComplex(1.0, 0.0), zero = make_cuDoubleComplex(0.0, 0.0);
+    TRY(c->C.alloc((size_t)n * n));
+    TRY(c->D.alloc((size_t)n * nrhs));
+    CUB_(cublasZgemm(c->blas, CUBLAS_OP_T, CUBLAS_OP_N, n, n, tn, &one, (cuDoubleComplex*)c->A.p, tn,
+                     (cuDoubleComplex*)c->A.p, tn, &zero, (cuDoubleComplex*)c->C.p, n));
+    CUB_(cublasZgemm(c->blas, CUBLAS_OP_T, CUBLAS_OP_N, n, nrhs, tn, &one, (cuDoubleComplex*)c->A.p, tn,
+                     (cuDoubleComplex*)c->B.p, tn, &zero, (cuDoubleComplex*)c->D.p, n));
+    M = c->C.p;
+    R = c->D.p;
+    ldm = n;
+  }
+  if (amat) CU(cudaMemcpy2DAsync(amat, (size_t)n * 16, M, (size_t)ldm * 16, (size_t)n * 16, n, cudaMemcpyDeviceToHost, c->st));
+  if (brmat)
+    CU(cudaMemcpy2DAsync(brmat, (size_t)n * 16, R, (size_t)ldm * 16, (size_t)n * 16, ndof, cudaMemcpyDeviceToHost, c->st));
+  if (bdmat && nbeta > 0)
+    CU(cudaMemcpy2DAsync(bdmat, (size_t)n * 16, R + (size_t)ndof * ldm, (size_t)ldm * 16, (size_t)n * 16, nbeta,
+                         cudaMemcpyDeviceToHost, c->st));
+  CU(cudaStreamSynchronize(c->st));
+  return 0;
+}
+
+extern "C" int hams_eval_green(hams_ctx* c, const hams_wave* w, int32_t npts, const double* pts, const int32_t* flag,
+                               double* grn) {
+  g_err.clear();
+  if (!c || !w || npts < 0 || (npts > 0 && (!pts || !flag || !grn))) return fail(HAMS_ERR_ARG, "null argument");
+  if (npts == 0) return 0;
+  if (cudaSetDevice(c->dev) != cudaSuccess) return fail(HAMS_ERR_CUDA, "cudaSetDevice failed");
+  DBuf<double> dp;
+  DBuf<int> df;
+  DBuf<double2> dout;
+  TRY(dp.alloc(6 * (size_t)npts));
+  TRY(df.alloc(npts));
+  TRY(dout.alloc(4 * (size_t)npts));
+  CU(cudaMemcpyAsync(dp.p, pts, 6 * (size_t)npts * 8, cudaMemcpyHostToDevice, c->st));
+  CU(cudaMemcpyAsync(df.p, flag, (size_t)npts * 4, cudaMemcpyHostToDevice, c->st));
+  WaveDev wd = wave_dev(c, w);
+  if (c->opts.depth >= 0.0 && !wd.limit) CU(cudaMemcpyAsync(c->wvn.p, w->wvn, HAMS_NK * 8, cudaMemcpyHostToDevice, c->st));
+  CU(cudaMemsetAsync(c->ovf.p, 0, sizeof(int), c->st));
+  k_eval_green<<<(npts + 127) / 128, 128, 0, c->st>>>(npts, dp.p, df.p, wd, c->wvn.p, dout.p, c->ovf.p);
+  TRY(launch_check(c));
+  CU(cudaMemcpyAsync(grn, dout.p, 4 * (size_t)npts * 16, cudaMemcpyDeviceToHost, c->st));
+  int ovf = 0;
+  CU(cudaMemcpyAsync(&ovf, c->ovf.p, sizeof(int), cudaMemcpyDeviceToHost, c->st));
+  CU(cudaStreamSynchronize(c->st));
+  dp.release();
+  df.release();
+  dout.release();
+  if (ovf) return fail(HAMS_ERR_NUMERIC, "adaptive quadrature stack overflow in the LINTON branch");
+  return 0;
+}
+
+extern "C" int hams_last_timings(hams_ctx* c, double* ms, int32_t n) {
+  if (!c || !ms) return 0;
+  int k = std::min<int>(n, hams_ctx::kTimings);
+  for (int i = 0; i < k; ++i) ms[i] = c->last_ms[i];
+  return k;
+}
+
+extern "C" int64_t hams_launch_count(hams_ctx* c) { return c ? (int64_t)c->launches.load() : 0; }

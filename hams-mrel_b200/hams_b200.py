@@ -1,0 +1,194 @@
+"""Python binding of the B200 per-frequency BEM library (libhams_b200.so).
+
+Mirrors the per-frequency operator calls of HAMS-MREL's frequency loop
+(src/HAMS_Prog.f90:613-733): CalWaveProperts -> ``wave_properties``;
+CALGREEN_MULTI + ASSB_* + *_SOLVER_MULTI + RFORCE/EFORCE_MULTI ->
+``Context.solve_frequency``.  Arrays follow the reference's Fortran module
+arrays (column-major, 1-based connectivity).  The CUDA library is required:
+importing this module on a machine without it raises, there is no CPU
+fallback.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libhams_b200.so")
+
+HAMS_NK = 200
+PREC_FP64 = 0
+PREC_MIXED = 1
+
+c_int = ctypes.c_int32
+c_dbl = ctypes.c_double
+P_dbl = ctypes.POINTER(ctypes.c_double)
+P_int = ctypes.POINTER(ctypes.c_int32)
+
+
+class HamsGeom(ctypes.Structure):
+    _fields_ = [("nelem", c_int), ("ntnd", c_int), ("nbody", c_int), ("isx", c_int), ("isy", c_int),
+                ("xyz", P_dbl), ("ncn", P_int), ("ncon", P_int), ("xyz_p", P_dbl), ("ds", P_dbl), ("pnsz", P_dbl),
+                ("dxyz", P_dbl), ("body_nelem", P_int), ("inelem", c_int), ("ixyz_p", P_dbl)]
+
+
+class HamsOpts(ctypes.Structure):
+    _fields_ = [("depth", c_dbl), ("rho", c_dbl), ("g", c_dbl), ("xw", c_dbl * 2), ("amp", c_dbl), ("isol", c_int),
+                ("irsp", c_int), ("precision", c_int), ("device", c_int), ("refine_tol", c_dbl),
+                ("refine_max", c_int), ("reserved", c_int * 7)]
+
+
+class HamsWave(ctypes.Structure):
+    _fields_ = [("v", c_dbl), ("wk", c_dbl), ("w1", c_dbl), ("tp", c_dbl), ("wl", c_dbl), ("wvn", c_dbl * HAMS_NK)]
+
+
+class HamsError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"hams error {code}: {msg}")
+        self.code = code
+
+
+_LIB = None
+
+
+def load_library(path=LIB_PATH):
+    """Load libhams_b200.so (raises OSError if it was not built)."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not os.path.exists(path):
+        raise OSError(f"{path} is missing: build it with `make -C {os.path.dirname(path)}`")
+    lib = ctypes.CDLL(path)
+    lib.hams_wave_properties.argtypes = [c_int, c_dbl, c_dbl, c_dbl, c_int, ctypes.POINTER(HamsWave)]
+    lib.hams_ctx_create.argtypes = [ctypes.POINTER(HamsGeom), ctypes.POINTER(HamsOpts), ctypes.POINTER(ctypes.c_void_p)]
+    lib.hams_ctx_destroy.argtypes = [ctypes.c_void_p]
+    lib.hams_solve_frequency.argtypes = [ctypes.c_void_p, ctypes.POINTER(HamsWave), c_int, P_dbl, P_dbl, P_dbl, P_dbl]
+    lib.hams_solve_batch.argtypes = [ctypes.c_void_p, c_int, ctypes.POINTER(HamsWave), c_int, P_dbl, P_dbl, P_dbl,
+                                     P_dbl]
+    lib.hams_assemble.argtypes = [ctypes.c_void_p, ctypes.POINTER(HamsWave), c_int, P_dbl, P_dbl, P_dbl, P_dbl]
+    lib.hams_eval_green.argtypes = [ctypes.c_void_p, ctypes.POINTER(HamsWave), c_int, P_dbl, P_int, P_dbl]
+    lib.hams_last_timings.argtypes = [ctypes.c_void_p, P_dbl, c_int]
+    lib.hams_launch_count.argtypes = [ctypes.c_void_p]
+    lib.hams_launch_count.restype = ctypes.c_int64
+    lib.hams_last_error.restype = ctypes.c_char_p
+    _LIB = lib
+    return lib
+
+
+def _check(rc, allow_pivot=False):
+    if rc < 0 or (rc > 0 and not allow_pivot):
+        msg = load_library().hams_last_error().decode()
+        raise HamsError(rc, msg or ("singular pivot %d" % rc))
+    return rc
+
+
+def _d(a):
+    return a.ctypes.data_as(P_dbl)
+
+
+def _i(a):
+    return a.ctypes.data_as(P_int)
+
+
+def wave_properties(value, depth, g=9.80665, inft=3, sybo_kk=0):
+    """CalWaveProperts for one input value (inft: 1 V, 2 k, 3 omega, 4 T, 5 lambda)."""
+    w = HamsWave()
+    _check(load_library().hams_wave_properties(inft, float(value), float(depth), float(g), sybo_kk, ctypes.byref(w)))
+    return w
+
+
+class Context:
+    """Device-resident geometry of one deck; solves frequencies on one GPU.
+
+    geom: dict with xyz (ntnd,3), ncn (n), ncon (n,4) 1-based, xyz_p (n,3),
+    ds (n), pnsz (n), dxyz (n,6), body_nelem (nb) and, for irsp=1, ixyz_p.
+    """
+
+    def __init__(self, geom, depth, rho=1000.0, g=9.80665, isol=1, irsp=0, precision=PREC_FP64, device=0,
+                 xw=(0.0, 0.0), amp=1.0, refine_tol=0.0, refine_max=0):
+        lib = load_library()
+        self._keep = {}
+        f = lambda k, dt: self._keep.setdefault(k, np.asfortranarray(geom[k], dtype=dt))
+        xyz, ncn, ncon = f("xyz", np.float64), f("ncn", np.int32), f("ncon", np.int32)
+        xyz_p, ds, pnsz, dxyz = f("xyz_p", np.float64), f("ds", np.float64), f("pnsz", np.float64), f("dxyz", np.float64)
+        bn = f("body_nelem", np.int32)
+        self.n = int(ncn.size)
+        self.nbody = int(bn.size)
+        self.ndof = 6 * self.nbody
+        g_ = HamsGeom(nelem=self.n, ntnd=xyz.shape[0], nbody=self.nbody, isx=int(geom.get("isx", 0)),
+                      isy=int(geom.get("isy", 0)), xyz=_d(xyz), ncn=_i(ncn), ncon=_i(ncon), xyz_p=_d(xyz_p), ds=_d(ds),
+                      pnsz=_d(pnsz), dxyz=_d(dxyz), body_nelem=_i(bn), inelem=0, ixyz_p=None)
+        if irsp == 1:
+            ixyz_p = f("ixyz_p", np.float64)
+            g_.inelem = ixyz_p.shape[0]
+            g_.ixyz_p = _d(ixyz_p)
+        o = HamsOpts(depth=float(depth), rho=float(rho), g=float(g), amp=float(amp), isol=int(isol), irsp=int(irsp),
+                     precision=int(precision), device=int(device), refine_tol=float(refine_tol),
+                     refine_max=int(refine_max))
+        o.xw[0], o.xw[1] = xw
+        self.depth, self.g = float(depth), float(g)
+        self._h = ctypes.c_void_p()
+        _check(lib.hams_ctx_create(ctypes.byref(g_), ctypes.byref(o), ctypes.byref(self._h)))
+
+    def close(self):
+        if self._h:
+            load_library().hams_ctx_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def wave(self, omega, inft=3):
+        return wave_properties(omega, self.depth, self.g, inft)
+
+    def solve_frequency(self, wave, betas):
+        betas = np.ascontiguousarray(betas, dtype=np.float64)
+        amas = np.zeros((self.ndof, self.ndof), order="F")
+        bdmp = np.zeros((self.ndof, self.ndof), order="F")
+        exfc = np.zeros((max(len(betas), 1), self.ndof), dtype=np.complex128, order="F")
+        _check(load_library().hams_solve_frequency(self._h, ctypes.byref(wave), len(betas), _d(betas), _d(amas),
+                                                   _d(bdmp), exfc.ctypes.data_as(P_dbl)))
+        return amas, bdmp, exfc[:len(betas)]
+
+    def solve_batch(self, waves, betas):
+        nf = len(waves)
+        arr = (HamsWave * nf)(*waves)
+        betas = np.ascontiguousarray(betas, dtype=np.float64)
+        amas = np.zeros((nf, self.ndof, self.ndof), order="F")
+        bdmp = np.zeros((nf, self.ndof, self.ndof), order="F")
+        exfc = np.zeros((nf, max(len(betas), 1), self.ndof), dtype=np.complex128, order="F")
+        _check(load_library().hams_solve_batch(self._h, nf, arr, len(betas), _d(betas), _d(amas), _d(bdmp),
+                                               exfc.ctypes.data_as(P_dbl)))
+        return amas, bdmp, exfc[:, :len(betas)]
+
+    def assemble(self, wave, betas):
+        betas = np.ascontiguousarray(betas, dtype=np.float64)
+        a = np.zeros((self.n, self.n), dtype=np.complex128, order="F")
+        b = np.zeros((self.n, self.ndof), dtype=np.complex128, order="F")
+        d = np.zeros((self.n, max(len(betas), 1)), dtype=np.complex128, order="F")
+        _check(load_library().hams_assemble(self._h, ctypes.byref(wave), len(betas), _d(betas),
+                                            a.ctypes.data_as(P_dbl), b.ctypes.data_as(P_dbl), d.ctypes.data_as(P_dbl)))
+        return a, b, d[:, :len(betas)]
+
+    def eval_green(self, wave, pts, flag):
+        pts = np.asfortranarray(pts, dtype=np.float64)
+        flag = np.ascontiguousarray(flag, dtype=np.int32)
+        out = np.zeros((pts.shape[0], 4), dtype=np.complex128, order="F")
+        _check(load_library().hams_eval_green(self._h, ctypes.byref(wave), pts.shape[0], _d(pts), _i(flag),
+                                              out.ctypes.data_as(P_dbl)))
+        return out
+
+    def timings(self):
+        """Stage times of the last solve (ms), per-branch Green kernel times and pair counts."""
+        ms = np.zeros(15)
+        load_library().hams_last_timings(self._h, _d(ms), 15)
+        return dict(green=ms[0], rhs=ms[1], solve=ms[2], forces=ms[3], total=ms[4], green_linton=ms[5],
+                    green_pidcock=ms[6], green_eigene=ms[7], green_eigen=ms[8], factor=ms[9], refine_sweeps=int(ms[10]),
+                    pairs_linton=int(ms[11]), pairs_pidcock=int(ms[12]), pairs_eigene=int(ms[13]),
+                    pairs_eigen=int(ms[14]))
+
+    def launch_count(self):
+        return int(load_library().hams_launch_count(self._h))

@@ -1,0 +1,157 @@
+/*
+ * hams_gpu.h -- C ABI of the B200 per-frequency BEM build-and-solve.
+ *
+ * Drop-in for the frequency-loop body of HAMS-MREL (src/HAMS_Prog.f90): the
+ * host (the reference's Fortran driver through iso_c_binding, the C++ driver
+ * hams_b200_run, or Python through ctypes) keeps reading ControlFile.in and
+ * the .pnl meshes and writing the HAMS/WAMIT files; everything from the
+ * Green-function tables to the force reductions runs on the GPU behind
+ * these calls.
+ *
+ * Conventions
+ *   - every call returns an int status: 0 ok; > 0 the 1-based index of a
+ *     zero pivot in the LU factorisation (LAPACK INFO style); < 0 an error
+ *     code below; hams_last_error() gives the message of the calling thread;
+ *   - arrays are host memory laid out as the reference's Fortran arrays:
+ *     column-major, mesh connectivity 1-based, complex values as
+ *     interleaved (re, im) doubles;
+ *   - a context owns one CUDA stream and its device buffers; use one context
+ *     per host thread.
+ */
+#ifndef HAMS_GPU_H
+#define HAMS_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define HAMS_NK 200 /* dispersion roots per frequency, WavDynMods.f90:59 (NK) */
+
+enum {
+  HAMS_OK = 0,
+  HAMS_ERR_ARG = -1,         /* invalid argument                      */
+  HAMS_ERR_CUDA = -2,        /* CUDA runtime / library failure         */
+  HAMS_ERR_UNSUPPORTED = -3, /* option not built (see message)         */
+  HAMS_ERR_NOMEM = -4,       /* device or host allocation failed       */
+  HAMS_ERR_NUMERIC = -5      /* non-finite result or refinement stalled*/
+};
+
+/* Numerical form of a solve. */
+enum {
+  HAMS_PREC_FP64 = 0,  /* plain FP64 drop-in: FP64 assembly, FP64 LU           */
+  HAMS_PREC_MIXED = 1  /* FP64 assembly, complex64 LU + FP64 iterative refinement */
+};
+
+/*
+ * Panel geometry after CalNormals[Multi] and BuildCombinedArrays
+ * (ReadPanelMeshMulti.f90:122, CalGreenFuncMulti.f90:53): the module arrays
+ * XYZ_GLOBAL_MULTI_COMB, NCN/NCON_MULTI_COMB, XYZ_GLOBAL_MULTI_COMB_P,
+ * DS/PNSZ/DXYZ_MULTI_COMB and the interior water-plane centres iXYZ_..._P.
+ */
+typedef struct hams_geom {
+  int32_t nelem;               /* hull panels of all bodies (N)                  */
+  int32_t ntnd;                /* hull nodes                                      */
+  int32_t nbody;               /* bodies                                          */
+  int32_t isx, isy;            /* symmetry flags of the .pnl header (0 0 only)    */
+  const double *xyz;           /* (ntnd,3)  node coordinates                      */
+  const int32_t *ncn;          /* (nelem)   vertices per panel, 3 or 4            */
+  const int32_t *ncon;         /* (nelem,4) vertex node ids, 1-based              */
+  const double *xyz_p;         /* (nelem,3) panel centres                         */
+  const double *ds;            /* (nelem)   panel areas                           */
+  const double *pnsz;          /* (nelem)   longest panel edge                    */
+  const double *dxyz;          /* (nelem,6) generalized normals n and r x n       */
+  const int32_t *body_nelem;   /* (nbody)   panels of each body, in order         */
+  int32_t inelem;              /* interior water-plane panels (0: none)           */
+  const double *ixyz_p;        /* (inelem,3) water-plane panel centres            */
+} hams_geom;
+
+typedef struct hams_opts {
+  double depth;     /* H: water depth, < 0 for infinite depth                    */
+  double rho, g;    /* density and gravity of the force and incident-wave terms  */
+  double xw[2];     /* incident-wave reference point (XW)                        */
+  double amp;       /* wave amplitude (AMP)                                      */
+  int32_t isol;     /* 1 total potential, 2 scattered (ISOL)                     */
+  int32_t irsp;     /* 1: remove irregular frequencies with water-plane lids     */
+  int32_t precision;/* HAMS_PREC_FP64 or HAMS_PREC_MIXED                         */
+  int32_t device;   /* CUDA device ordinal                                       */
+  double refine_tol;/* mixed: relative residual target of the refinement (<=0: 1e-12) */
+  int32_t refine_max;/* mixed: refinement sweeps (<=0: 30)                       */
+  int32_t reserved[7];
+} hams_opts;
+
+/* One frequency after CalWaveProperts (ImplementSubs.f90:40): V = w^2/g
+ * (0 and -1 for the zero / infinite frequency limits), wave number, angular
+ * frequency and the dispersion roots WVN (finite depth only). */
+typedef struct hams_wave {
+  double v, wk, w1, tp, wl;
+  double wvn[HAMS_NK];
+} hams_wave;
+
+typedef struct hams_ctx hams_ctx;
+
+/* Replaces CalWaveProperts + DISPERSION (ImplementSubs.f90:40,
+ * WavDynSubs.f90:40).  inft: 1 deep-water wave number, 2 wave number,
+ * 3 angular frequency, 4 period, 5 wave length; sybo_kk = 1 / 2 selects the
+ * zero / infinite frequency limit (SYBO = 1 decks), 0 a regular frequency. */
+int hams_wave_properties(int32_t inft, double value, double depth, double g, int32_t sybo_kk, hams_wave *out);
+
+/* Uploads the geometry, evaluates the frequency-independent Rankine panel
+ * integrals (SGLINTBD_*, SingularIntgr.f90:44,252) for every field/source
+ * pair and sorts the pairs by Green-function branch.  Replaces the setup of
+ * HAMS_Prog.f90:423-570 on the device side. */
+int hams_ctx_create(const hams_geom *geom, const hams_opts *opts, hams_ctx **out);
+void hams_ctx_destroy(hams_ctx *ctx);
+
+/*
+ * One frequency, all headings: the body of HAMS_Prog.f90:615-723 --
+ * CALGREEN_MULTI, ASSB_LEFT/RBC/DBC_MULTI, RADIATION/DIFFRACTION_SOLVER_MULTI,
+ * RFORCE_MULTI and EFORCE_MULTI (and their _IRR forms when opts.irsp = 1).
+ *   beta_rad (nbeta)      headings in radians
+ *   amas, bdmp (6nb,6nb)  AMAS/BDMP_MULTI_COMB(KK,:,:): added mass, damping
+ *   exfc (nbeta,6nb)      EXFC_MULTI_COMB(KK,:,:): complex excitation
+ * Any output pointer may be NULL.
+ */
+int hams_solve_frequency(hams_ctx *ctx, const hams_wave *wave, int32_t nbeta, const double *beta_rad, double *amas,
+                         double *bdmp, double *exfc);
+
+/* nfreq frequencies back to back, results stacked along a leading frequency
+ * index: amas/bdmp (nfreq,6nb,6nb), exfc (nfreq,nbeta,6nb), column-major as
+ * AMAS_MULTI_COMB / EXFC_MULTI_COMB. */
+int hams_solve_batch(hams_ctx *ctx, int32_t nfreq, const hams_wave *waves, int32_t nbeta, const double *beta_rad,
+                     double *amas, double *bdmp, double *exfc);
+
+/* The assembled systems of one frequency, before factorisation, for checks:
+ *   amat (n,n)        A of ASSB_LEFT_MULTI (or C = A^T A with lids)
+ *   brmat (n,6nb)     radiation right-hand sides (or A^T B)
+ *   bdmat (n,nbeta)   diffraction right-hand sides (or A^T B)
+ * Any output pointer may be NULL. */
+int hams_assemble(hams_ctx *ctx, const hams_wave *wave, int32_t nbeta, const double *beta_rad, double *amat,
+                  double *brmat, double *bdmat);
+
+/* Batch evaluation of FINGREEN3D (depth > 0) or INFGREEN3D (depth < 0) for
+ * npts source/field pairs: pts (npts,6) = (xq, yq, zq, xp, yp, zp) per row,
+ * flag (npts) the near/far flag, grn (npts,4) complex output (G, dG/dx,
+ * dG/dy, dG/dz at the source).  Runs on the context's device. */
+int hams_eval_green(hams_ctx *ctx, const hams_wave *wave, int32_t npts, const double *pts, const int32_t *flag,
+                    double *grn);
+
+/* Timing of the last solve in milliseconds: [0] Green/assembly kernels,
+ * [1] right-hand sides, [2] factorisation + solves, [3] reductions,
+ * [4] whole call, [5..8] Green kernels of the LINTON, PIDCOCK, EIGENE and
+ * EIGEN branches (finite depth), [9] LU factorisation, [10] refinement
+ * sweeps (mixed form), [11..14] pairs in each branch.  n is the capacity of
+ * ms (15 fills all). Returns the number written. */
+int hams_last_timings(hams_ctx *ctx, double *ms, int32_t n);
+
+/* Kernel launches issued by the library since the context was created. */
+int64_t hams_launch_count(hams_ctx *ctx);
+
+/* Message of the last failing call on this thread ("" if none). */
+const char *hams_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
