@@ -10,6 +10,11 @@
 // Infinite depth: the Wu/Noblesse/Liang global approximation of the
 // Havelock function (src/InfGreen_Appr.f90:104-872).
 //
+// The eigenfunction-series terms of EIGEN/EIGENE/PIDCOCK use the
+// bit-reproducible sin/cos/exp/log of detmath.h in the operation order of the
+// CPU checker: the epsilon extrapolation amplifies last-bit differences of a
+// math library to up to 1e-3 in single values.
+//
 // Every routine returns the wave part of G with 1/r and 1/r1 removed, plus
 // the point-source terms that FINGREEN3D / INFGREEN3D add back according to
 // the near/far flag (FinGreen3D.f90:124-150, InfGreen_Appr.f90:130-183).
@@ -111,11 +116,11 @@ __device__ inline void eigen(double r, double zf, double zp, double wk, const do
   prop_mode(r, zfh, zph, wk, h, g);
   for (int i = 2; i <= 10; ++i) {
     double km = wvn[i - 1], twokmh = 2.0 * km * h;
-    double pm = 4.0 / (1.0 + sin(twokmh) / twokmh) / h;
+    double pm = 4.0 / (1.0 + dm_sin(twokmh) / twokmh) / h;
     double k0, k1, skzf, ckzf;
     ik01a(km * r, k0, k1);
-    sincos(km * zfh, &skzf, &ckzf);
-    double ckzp = cos(km * zph);
+    dm_sincos(km * zfh, &skzf, &ckzf);
+    double ckzp = dm_cos(km * zph);
     double rm0 = pm * k0 * ckzf * ckzp, rm1 = -pm * km * k1 * ckzf * ckzp, rm2 = -pm * km * k0 * skzf * ckzp;
     g[0].re += rm0;
     g[1].re += rm1;
@@ -140,11 +145,11 @@ __device__ inline void eigene(double r, double zf, double zp, double wk, const d
   sc.s0[0] = sc.s1[0] = sc.s2[0] = 0.0;
   for (int i = 2; i <= nt; ++i) {
     double km = wvn[i - 1], twokmh = 2.0 * km * h;
-    double pm = 4.0 / (1.0 + sin(twokmh) / twokmh) / h;
+    double pm = 4.0 / (1.0 + dm_sin(twokmh) / twokmh) / h;
     double k0, k1, skzf, ckzf;
     ik01a(km * r, k0, k1);
-    sincos(km * zfh, &skzf, &ckzf);
-    double ckzp = cos(km * zph);
+    dm_sincos(km * zfh, &skzf, &ckzf);
+    double ckzp = dm_cos(km * zph);
     sc.s0[i - 1] = sc.s0[i - 2] + pm * k0 * ckzf * ckzp;
     sc.s1[i - 1] = sc.s1[i - 2] + -pm * km * k1 * ckzf * ckzp;
     sc.s2[i - 1] = sc.s2[i - 2] + -pm * km * k0 * skzf * ckzp;
@@ -156,7 +161,7 @@ __device__ inline void eigene(double r, double zf, double zp, double wk, const d
 }
 
 // Pidcock image sums IMGS/DGSR/DGSZ, FinGreen3D.f90:908-1113
-__constant__ double c_amn[25] = {
+static __constant__ double c_amn[25] = {
     0.0,        -0.02525711, 0.00086546,  -0.00004063, 0.00000193,  0.05051418,  -0.00692380,
     0.00073292, -0.00006636, 0.00000398,  0.00230838,  -0.00097875, 0.00020597,  -0.00003333,
     0.00000524, 0.00012934,  -0.00010879, 0.00003965,  -0.00000891, 0.0,         0.00000913,
@@ -218,9 +223,9 @@ __device__ inline void pidcock(double r, double zf, double zp, double v, double 
     ik01a(umt * r, k0t, k1t);
     double ac = (um * um + v * v) / ((um * um + v * v) * h - v);
     double su, cu, sut, cut;
-    sincos(um * zfh, &su, &cu);
-    sincos(umt * zfh, &sut, &cut);
-    double cup = cos(um * zph), cutp = cos(umt * zph);
+    dm_sincos(um * zfh, &su, &cu);
+    dm_sincos(umt * zfh, &sut, &cut);
+    double cup = dm_cos(um * zph), cutp = dm_cos(umt * zph);
     double am = ac * cu * cup, amt = cut * cutp / h;
     double dam = -um * ac * su * cup, damt = -umt * sut * cutp / h;
     sc.s0[i - 1] = sc.s0[i - 2] + (am * k0 - amt * k0t);
@@ -241,15 +246,15 @@ __device__ inline void pidcock(double r, double zf, double zp, double v, double 
 // ---------------------------------------------------------------------------
 // LINTON (R/h < 0.0005), FinGreen3D.f90:712-861 and its support routines
 // ---------------------------------------------------------------------------
-__constant__ double c_xgq[7] = {-0.949107912342759, -0.741531185599394, -0.405845151377397, 0.0,
+static __constant__ double c_xgq[7] = {-0.949107912342759, -0.741531185599394, -0.405845151377397, 0.0,
                                 0.405845151377397,  0.741531185599394,  0.949107912342759};
-__constant__ double c_wgq[7] = {0.129484966168870, 0.279705391489277, 0.381830050505119, 0.417959183673469,
+static __constant__ double c_wgq[7] = {0.129484966168870, 0.279705391489277, 0.381830050505119, 0.417959183673469,
                                 0.381830050505119, 0.279705391489277, 0.129484966168870};
-__constant__ double c_xkq[15] = {-0.991455371120813, -0.949107912342759, -0.864864423359769, -0.741531185599394,
+static __constant__ double c_xkq[15] = {-0.991455371120813, -0.949107912342759, -0.864864423359769, -0.741531185599394,
                                  -0.586087235467691, -0.405845151377397, -0.207784955007898, 0.0,
                                  0.207784955007898,  0.405845151377397,  0.586087235467691,  0.741531185599394,
                                  0.864864423359769,  0.949107912342759,  0.991455371120813};
-__constant__ double c_wkq[15] = {0.022935322010529, 0.063092092629979, 0.104790010322250, 0.140653259715525,
+static __constant__ double c_wkq[15] = {0.022935322010529, 0.063092092629979, 0.104790010322250, 0.140653259715525,
                                  0.169004726639267, 0.190350578064785, 0.204432940075298, 0.209482141084728,
                                  0.204432940075298, 0.190350578064785, 0.169004726639267, 0.140653259715525,
                                  0.104790010322250, 0.063092092629979, 0.022935322010529};
@@ -601,13 +606,13 @@ __device__ __forceinline__ double hpoly(const double* c, int deg, double t) {
   for (int k = deg - 2; k >= 1; --k) s = (c[k] + s) * t;
   return c[0] + s;
 }
-__constant__ double c_hA[10] = {+1.21, -13.328, +215.896, -1763.96, +8418.94, -24314.21, +42002.57, -41592.9, 21859.0, -4838.6};
-__constant__ double c_hB[10] = {+0.938, +5.373, -67.92, +796.534, -4780.77, +17137.74, -36618.81, +44894.06, -29030.24, +7671.22};
-__constant__ double c_hC[8] = {+1.268, -9.747, +209.653, -1397.89, +5155.67, -9844.35, +9136.4, -3272.62};
-__constant__ double c_hD[10] = {+0.632, -40.97, +667.16, -6072.07, +31127.39, -96293.05, +181856.75, -205690.43, +128170.2, -33744.6};
-__constant__ double c_hdA[10] = {+2.948, -24.53, +249.69, -754.85, -1187.71, +16370.75, -48811.41, +68220.87, -46688.0, +12622.25};
-__constant__ double c_hdB[10] = {+1.11, +2.894, -76.765, +1565.35, -11336.19, +44270.15, -97014.11, +118879.26, -76209.82, +19923.28};
-__constant__ double c_hdC[6] = {+14.19, -148.24, +847.8, -2318.58, +3168.35, -1590.27};
+static __constant__ double c_hA[10] = {+1.21, -13.328, +215.896, -1763.96, +8418.94, -24314.21, +42002.57, -41592.9, 21859.0, -4838.6};
+static __constant__ double c_hB[10] = {+0.938, +5.373, -67.92, +796.534, -4780.77, +17137.74, -36618.81, +44894.06, -29030.24, +7671.22};
+static __constant__ double c_hC[8] = {+1.268, -9.747, +209.653, -1397.89, +5155.67, -9844.35, +9136.4, -3272.62};
+static __constant__ double c_hD[10] = {+0.632, -40.97, +667.16, -6072.07, +31127.39, -96293.05, +181856.75, -205690.43, +128170.2, -33744.6};
+static __constant__ double c_hdA[10] = {+2.948, -24.53, +249.69, -754.85, -1187.71, +16370.75, -48811.41, +68220.87, -46688.0, +12622.25};
+static __constant__ double c_hdB[10] = {+1.11, +2.894, -76.765, +1565.35, -11336.19, +44270.15, -97014.11, +118879.26, -76209.82, +19923.28};
+static __constant__ double c_hdC[6] = {+14.19, -148.24, +847.8, -2318.58, +3168.35, -1590.27};
 
 __device__ inline double hv_j0(double xx) {
   const double pi = 3.141592653589793;

@@ -1,0 +1,75 @@
+// green_series.cu -- the epsilon-accelerated finite-depth Green kernels.
+//
+// EIGENE and PIDCOCK (FinGreen3D.f90:413-660) sum up to 100 eigenfunction
+// terms and extrapolate them with the Wynn epsilon algorithm (Limes), which
+// divides by differences of nearly equal partial sums and stops on exact
+// equalities.  This file is compiled with --fmad=false so that every product
+// and sum of those series is rounded exactly as in the CPU checker; the
+// transcendental functions inside them come from detmath.h.  The remaining
+// kernels (hams_gpu.cu) keep fused multiply-adds.
+#include "kernels.cuh"
+
+template <int BR>
+__global__ void __launch_bounds__(128) k_green_series(DevGeom g, WaveDev w, const double* __restrict__ wvn,
+                                                      const uint32_t* __restrict__ pairs, long long count,
+                                                      const double* __restrict__ rs, const double* __restrict__ rd,
+                                                      double2* __restrict__ A, double2* __restrict__ S, int* ovf) {
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= count) return;
+  size_t p = pairs[t];
+  int i = (int)(p % (size_t)g.tn), j = (int)(p / (size_t)g.tn);
+  int flag = near_flag(g, i, j);
+  double xp = g.fxyz[i], yp = g.fxyz[i + g.tn], zp = g.fxyz[i + 2 * g.tn];
+  double xq = g.xq[j], yq = g.xq[j + g.n], zq = g.xq[j + 2 * g.n];
+  grn4 G;
+  if (w.limit) {
+    G = hams::green_limit(w.limit == 2, xq, xp, yq, yp, zq, zp, flag);
+  } else {
+    hams::SeriesScratch sc;
+    int o = 0;
+    G = hams::fingreen3d<BR>(xq, xp, yq, yp, zq, zp, w.v, wvn, w.h, flag, &sc, &o);
+  }
+  store_pair(g, p, i, j, G, rs, rd, A, S);
+}
+
+void launch_green_series(int br, unsigned blocks, cudaStream_t st, DevGeom g, WaveDev w, const double* wvn,
+                         const uint32_t* pairs, long long count, const double* rs, const double* rd, double2* A,
+                         double2* S, int* ovf) {
+  if (br == hams::kPidcock)
+    k_green_series<hams::kPidcock><<<blocks, 128, 0, st>>>(g, w, wvn, pairs, count, rs, rd, A, S, ovf);
+  else
+    k_green_series<hams::kEigenE><<<blocks, 128, 0, st>>>(g, w, wvn, pairs, count, rs, rd, A, S, ovf);
+}
+
+// Batch Green evaluation of hams_eval_green: any branch, one pair per thread.
+__global__ void k_eval_green(int npts, const double* __restrict__ pts, const int* __restrict__ flag, WaveDev w,
+                             const double* __restrict__ wvn, double2* __restrict__ out, int* ovf) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= npts) return;
+  double xq = pts[t], yq = pts[t + npts], zq = pts[t + 2 * (size_t)npts];
+  double xp = pts[t + 3 * (size_t)npts], yp = pts[t + 4 * (size_t)npts], zp = pts[t + 5 * (size_t)npts];
+  grn4 G;
+  if (w.limit) {
+    G = hams::green_limit(w.limit == 2, xq, xp, yq, yp, zq, zp, flag[t]);
+  } else if (w.h < 0.0) {
+    G = hams::infgreen3d(xq, xp, yq, yp, zq, zp, w.v, flag[t]);
+  } else {
+    hams::SeriesScratch sc;
+    int o = 0;
+    double rr = sqrt((xq - xp) * (xq - xp) + (yq - yp) * (yq - yp));
+    switch (hams::fin_branch(rr, w.h)) {
+      case hams::kLinton: G = hams::fingreen3d<hams::kLinton>(xq, xp, yq, yp, zq, zp, w.v, wvn, w.h, flag[t], &sc, &o); break;
+      case hams::kPidcock: G = hams::fingreen3d<hams::kPidcock>(xq, xp, yq, yp, zq, zp, w.v, wvn, w.h, flag[t], &sc, &o); break;
+      case hams::kEigenE: G = hams::fingreen3d<hams::kEigenE>(xq, xp, yq, yp, zq, zp, w.v, wvn, w.h, flag[t], &sc, &o); break;
+      default: G = hams::fingreen3d<hams::kEigen>(xq, xp, yq, yp, zq, zp, w.v, wvn, w.h, flag[t], &sc, &o); break;
+    }
+    if (o) atomicOr(ovf, 1);
+  }
+  for (int k = 0; k < 4; ++k) out[t + (size_t)k * npts] = make_double2(G.g[k].re, G.g[k].im);
+}
+
+
+void launch_eval_green(unsigned blocks, cudaStream_t st, int npts, const double* pts, const int* flag, WaveDev w,
+                       const double* wvn, double2* out, int* ovf) {
+  k_eval_green<<<blocks, 128, 0, st>>>(npts, pts, flag, w, wvn, out, ovf);
+}

@@ -80,31 +80,7 @@ static int fail(int code, const char* fmt, ...) {
     if (rc_ < 0) return rc_; \
   } while (0)
 
-// ---------------------------------------------------------------------------
-// geometry as the kernels see it
-// ---------------------------------------------------------------------------
-struct DevGeom {
-  int n, tn, nb;
-  const double* xq;    // source centres (n,3)
-  const double* fxyz;  // field points (tn,3): hull centres then lid centres
-  const double* ds;    // (n)
-  const double* pnsz;  // (n)
-  const double* nrm;   // (n,6)
-  const double* vtx;   // (n,4,3): vertices of each source panel (v = 0..3)
-  const int* ncn;      // (n)
-  const int* body;     // (n) body of each source panel
-  const int* bstart;   // (nb+1)
-};
-
-struct WaveDev {
-  double v, wk, w1, h;
-  int limit;  // 0 regular, 1 zero frequency, 2 infinite frequency
-};
-
-__device__ __forceinline__ int near_flag(const DevGeom& g, int i, int j) {
-  double dx = g.fxyz[i] - g.xq[j], dy = g.fxyz[i + g.tn] - g.xq[j + g.n], dz = g.fxyz[i + 2 * g.tn] - g.xq[j + 2 * g.n];
-  return sqrt(dx * dx + dy * dy + dz * dz) <= 50.0 * g.pnsz[j] ? 1 : 0;
-}
+#include "kernels.cuh"
 
 // ---------------------------------------------------------------------------
 // setup kernels
@@ -155,17 +131,8 @@ __global__ void k_pair_keys(DevGeom g, double h, uint32_t* __restrict__ keys, ui
 // ---------------------------------------------------------------------------
 // per-frequency assembly: Green function fused with the pair algebra
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ void store_pair(const DevGeom& g, size_t p, int i, int j, const grn4& G,
-                                           const double* __restrict__ rs, const double* __restrict__ rd,
-                                           double2* __restrict__ A, double2* __restrict__ S) {
-  double ds = g.ds[j], n1 = g.nrm[j], n2 = g.nrm[j + g.n], n3 = g.nrm[j + 2 * g.n];
-  double are = rd[p] + ds * (G.g[1].re * n1 + G.g[2].re * n2 + G.g[3].re * n3);
-  double aim = ds * (G.g[1].im * n1 + G.g[2].im * n2 + G.g[3].im * n3);
-  if (i == j) are += 2.0 * 3.141592653589793;  // A(I,I) = 2 pi on hull rows (AssbMatxMulti.f90:75)
-  A[p] = make_double2(are, aim);
-  S[p] = make_double2(rs[p] + G.g[0].re * ds, G.g[0].im * ds);
-}
-
+// LINTON (BR = 0) and EIGEN (BR = 3) pairs; the epsilon-series branches are
+// in green_series.cu.
 template <int BR>
 __global__ void __launch_bounds__(128) k_green_fin(DevGeom g, WaveDev w, const double* __restrict__ wvn,
                                                    const uint32_t* __restrict__ pairs, long long count,
@@ -183,12 +150,7 @@ __global__ void __launch_bounds__(128) k_green_fin(DevGeom g, WaveDev w, const d
     G = hams::green_limit(w.limit == 2, xq, xp, yq, yp, zq, zp, flag);
   } else {
     int o = 0;
-    if (BR == hams::kPidcock || BR == hams::kEigenE) {
-      hams::SeriesScratch sc;
-      G = hams::fingreen3d<BR>(xq, xp, yq, yp, zq, zp, w.v, wvn, w.h, flag, &sc, &o);
-    } else {
-      G = hams::fingreen3d<BR>(xq, xp, yq, yp, zq, zp, w.v, wvn, w.h, flag, nullptr, &o);
-    }
+    G = hams::fingreen3d<BR>(xq, xp, yq, yp, zq, zp, w.v, wvn, w.h, flag, nullptr, &o);
     if (o) atomicOr(ovf, 1);
   }
   store_pair(g, p, i, j, G, rs, rd, A, S);
@@ -440,35 +402,6 @@ __global__ void k_colnorm_ratio(const double2* __restrict__ r, const double2* __
     __syncthreads();
   }
   if (threadIdx.x == 0) out[col] = s2[0] > 0.0 ? s1[0] / s2[0] : s1[0];
-}
-
-// ---------------------------------------------------------------------------
-// batch Green evaluation (hams_eval_green)
-// ---------------------------------------------------------------------------
-__global__ void k_eval_green(int npts, const double* __restrict__ pts, const int* __restrict__ flag, WaveDev w,
-                             const double* __restrict__ wvn, double2* __restrict__ out, int* ovf) {
-  int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= npts) return;
-  double xq = pts[t], yq = pts[t + npts], zq = pts[t + 2 * (size_t)npts];
-  double xp = pts[t + 3 * (size_t)npts], yp = pts[t + 4 * (size_t)npts], zp = pts[t + 5 * (size_t)npts];
-  grn4 G;
-  if (w.limit) {
-    G = hams::green_limit(w.limit == 2, xq, xp, yq, yp, zq, zp, flag[t]);
-  } else if (w.h < 0.0) {
-    G = hams::infgreen3d(xq, xp, yq, yp, zq, zp, w.v, flag[t]);
-  } else {
-    hams::SeriesScratch sc;
-    int o = 0;
-    double rr = sqrt((xq - xp) * (xq - xp) + (yq - yp) * (yq - yp));
-    switch (hams::fin_branch(rr, w.h)) {
-      case hams::kLinton: G = hams::fingreen3d<hams::kLinton>(xq, xp, yq, yp, zq, zp, w.v, wvn, w.h, flag[t], &sc, &o); break;
-      case hams::kPidcock: G = hams::fingreen3d<hams::kPidcock>(xq, xp, yq, yp, zq, zp, w.v, wvn, w.h, flag[t], &sc, &o); break;
-      case hams::kEigenE: G = hams::fingreen3d<hams::kEigenE>(xq, xp, yq, yp, zq, zp, w.v, wvn, w.h, flag[t], &sc, &o); break;
-      default: G = hams::fingreen3d<hams::kEigen>(xq, xp, yq, yp, zq, zp, w.v, wvn, w.h, flag[t], &sc, &o); break;
-    }
-    if (o) atomicOr(ovf, 1);
-  }
-  for (int k = 0; k < 4; ++k) out[t + (size_t)k * npts] = make_double2(G.g[k].re, G.g[k].im);
 }
 
 // ---------------------------------------------------------------------------
@@ -744,8 +677,8 @@ static int assemble_dev(hams_ctx* c, const hams_wave* w, int nbeta) {
       unsigned blocks = (unsigned)((cnt + 127) / 128);
       switch (br) {
         case 0: k_green_fin<0><<<blocks, 128, 0, c->st>>>(c->g, wd, c->wvn.p, lst, cnt, c->rs.p, c->rd.p, c->A.p, c->S.p, c->ovf.p); break;
-        case 1: k_green_fin<1><<<blocks, 128, 0, c->st>>>(c->g, wd, c->wvn.p, lst, cnt, c->rs.p, c->rd.p, c->A.p, c->S.p, c->ovf.p); break;
-        case 2: k_green_fin<2><<<blocks, 128, 0, c->st>>>(c->g, wd, c->wvn.p, lst, cnt, c->rs.p, c->rd.p, c->A.p, c->S.p, c->ovf.p); break;
+        case 1:
+        case 2: launch_green_series(br, blocks, c->st, c->g, wd, c->wvn.p, lst, cnt, c->rs.p, c->rd.p, c->A.p, c->S.p, c->ovf.p); break;
         default: k_green_fin<3><<<blocks, 128, 0, c->st>>>(c->g, wd, c->wvn.p, lst, cnt, c->rs.p, c->rd.p, c->A.p, c->S.p, c->ovf.p); break;
       }
       TRY(launch_check(c));
@@ -994,7 +927,7 @@ extern "C" int hams_eval_green(hams_ctx* c, const hams_wave* w, int32_t npts, co
   WaveDev wd = wave_dev(c, w);
   if (c->opts.depth >= 0.0 && !wd.limit) CU(cudaMemcpyAsync(c->wvn.p, w->wvn, HAMS_NK * 8, cudaMemcpyHostToDevice, c->st));
   CU(cudaMemsetAsync(c->ovf.p, 0, sizeof(int), c->st));
-  k_eval_green<<<(npts + 127) / 128, 128, 0, c->st>>>(npts, dp.p, df.p, wd, c->wvn.p, dout.p, c->ovf.p);
+  launch_eval_green((npts + 127) / 128, c->st, npts, dp.p, df.p, wd, c->wvn.p, dout.p, c->ovf.p);
   TRY(launch_check(c));
   CU(cudaMemcpyAsync(grn, dout.p, 4 * (size_t)npts * 16, cudaMemcpyDeviceToHost, c->st));
   int ovf = 0;

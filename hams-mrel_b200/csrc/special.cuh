@@ -12,6 +12,8 @@
 #include <cuda_runtime.h>
 #include <math.h>
 
+#include "detmath.h"
+
 #define HAMS_F4(x) ((double)(x##f))
 
 namespace hams {
@@ -96,9 +98,13 @@ __device__ inline double eix(double x) {
   return exp(x) / x * ei;
 }
 
-// K0(x), K1(x), IK01A (FinGrnExtSubs.f90:538-635).  The reference compares
-// the K0 series against a value it never initialised on the first pass;
-// zero is used, which cannot stop the series at its first term.
+// K0(x), K1(x), IK01A (FinGrnExtSubs.f90:538-635).  K0/K1 feed the
+// epsilon-accelerated series, whose result moves with the last bit of its
+// inputs, so this routine uses the bit-reproducible exp/log of detmath.h and
+// the operation order of the CPU checker; the kernels that call it for the
+// EIGENE/PIDCOCK series are compiled without implicit fused multiply-adds.
+// The reference compares the K0 series against a value it never initialised
+// on the first pass; zero is used, which cannot stop the series early.
 __device__ inline void ik01a(double x, double& bk0, double& bk1) {
   const double pi = 3.141592653589793, el = 0.5772156649015329;
   if (x == 0.0) {
@@ -106,10 +112,10 @@ __device__ inline void ik01a(double x, double& bk0, double& bk1) {
     bk1 = 1.0e300;
     return;
   }
-  double x2 = x * x, bi0, bi1;
+  double x2 = x * x, bi0, bi1, r;
   if (x <= 18.0) {
     bi0 = 1.0;
-    double r = 1.0;
+    r = 1.0;
     for (int k = 1; k <= 50; ++k) {
       r = 0.25 * r * x2 / (double)(k * k);
       bi0 = bi0 + r;
@@ -133,19 +139,17 @@ __device__ inline void ik01a(double x, double& bk0, double& bk1) {
     int k0 = 12;
     if (x >= 35.0) k0 = 9;
     if (x >= 50.0) k0 = 7;
-    double ca = exp(x) / sqrt(2.0 * pi * x), xr = 1.0 / x, p = 1.0;
+    double ca = dm_exp(x) / sqrt(2.0 * pi * x), xr = 1.0 / x;
     bi0 = 1.0;
-    bi1 = 1.0;
-    for (int k = 1; k <= k0; ++k) {
-      p *= xr;
-      bi0 = bi0 + A[k - 1] * p;
-      bi1 = bi1 + B[k - 1] * p;
-    }
+    for (int k = 1; k <= k0; ++k) bi0 = bi0 + A[k - 1] * powi(xr, k);
     bi0 = ca * bi0;
+    bi1 = 1.0;
+    for (int k = 1; k <= k0; ++k) bi1 = bi1 + B[k - 1] * powi(xr, k);
     bi1 = ca * bi1;
   }
   if (x <= 9.0) {
-    double ct = -(log(x / 2.0) + el), w0 = 0.0, r = 1.0, ww = 0.0;
+    double ct = -(dm_log(x / 2.0) + el), w0 = 0.0, ww = 0.0;
+    r = 1.0;
     bk0 = 0.0;
     for (int k = 1; k <= 50; ++k) {
       w0 = w0 + 1.0 / k;
@@ -158,12 +162,9 @@ __device__ inline void ik01a(double x, double& bk0, double& bk1) {
   } else {
     const double A1[8] = {0.125, 0.2109375, 1.0986328125, 1.1775970458984e01, 2.1461706161499e02,
                           5.9511522710323e03, 2.3347645606175e05, 1.2312234987631e07};
-    double cb = 0.5 / x, xr2 = 1.0 / x2, p = 1.0;
+    double cb = 0.5 / x, xr2 = 1.0 / x2;
     bk0 = 1.0;
-    for (int k = 1; k <= 8; ++k) {
-      p *= xr2;
-      bk0 = bk0 + A1[k - 1] * p;
-    }
+    for (int k = 1; k <= 8; ++k) bk0 = bk0 + A1[k - 1] * powi(xr2, k);
     bk0 = cb * bk0 / bi0;
   }
   bk1 = (1.0 / x - bi1 * bk0) / bi0;

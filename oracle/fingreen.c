@@ -10,8 +10,14 @@
  * sums of Pidcock, and Linton's Ewald-type representation with its adaptive
  * Gauss-Kronrod (7/15) quadratures.  Recursion is kept recursive here, in
  * the order of the reference (left half, then right half).
+ * The sin/cos of the eigenfunction series terms (EIGEN, EIGENE, PIDCOCK) are
+ * the bit-reproducible ones of detmath.h: the epsilon extrapolation of those
+ * series turns one-ulp differences between math libraries into differences
+ * of up to 1e-3 in single values, so the checker and the GPU code share one
+ * implementation of them.
  */
 #include "oracle_internal.h"
+#include "detmath.h"
 
 static double powi(double x, int n)
 {
@@ -53,13 +59,13 @@ static void eigen(double r, double zf, double zp, double wk, const double *wvn, 
     for (i = 2; i <= nt; ++i) {
         km = wvn[i - 1];
         twokmh = 2.0 * km * h;
-        pm = 4.0 / (1.0 + sin(twokmh) / twokmh) / h;
+        pm = 4.0 / (1.0 + dm_sin(twokmh) / twokmh) / h;
         orc_ik01a(km * r, &k0, &k1);
         kzf = km * zfh;
         kzp = km * zph;
-        ckzf = cos(kzf);
-        ckzp = cos(kzp);
-        skzf = sin(kzf);
+        ckzf = dm_cos(kzf);
+        ckzp = dm_cos(kzp);
+        skzf = dm_sin(kzf);
         rm[0] = pm * k0 * ckzf * ckzp;
         rm[1] = -pm * km * k1 * ckzf * ckzp;
         rm[2] = -pm * km * k0 * skzf * ckzp;
@@ -113,13 +119,13 @@ static void eigene(double r, double zf, double zp, double wk, const double *wvn,
     for (i = 2; i <= nt; ++i) {
         km = wvn[i - 1];
         twokmh = 2.0 * km * h;
-        pm = 4.0 / (1.0 + sin(twokmh) / twokmh) / h;
+        pm = 4.0 / (1.0 + dm_sin(twokmh) / twokmh) / h;
         orc_ik01a(km * r, &k0, &k1);
         kzf = km * zfh;
         kzp = km * zph;
-        ckzf = cos(kzf);
-        ckzp = cos(kzp);
-        skzf = sin(kzf);
+        ckzf = dm_cos(kzf);
+        ckzp = dm_cos(kzp);
+        skzf = dm_sin(kzf);
         rm[0] = pm * k0 * ckzf * ckzp;
         rm[1] = -pm * km * k1 * ckzf * ckzp;
         rm[2] = -pm * km * k0 * skzf * ckzp;
@@ -234,10 +240,10 @@ static void pidcock(double r, double zf, double zp, double v, double wk, const d
         orc_ik01a(x, &k0, &k1);
         orc_ik01a(umt * r, &k0t, &k1t);
         ac = (um * um + v * v) / ((um * um + v * v) * h - v);
-        am = ac * cos(um * (zf + h)) * cos(um * (zp + h));
-        amt = cos(umt * (zf + h)) * cos(umt * (zp + h)) / h;
-        dam = -um * ac * sin(um * (zf + h)) * cos(um * (zp + h));
-        damt = -umt * sin(umt * (zf + h)) * cos(umt * (zp + h)) / h;
+        am = ac * dm_cos(um * (zf + h)) * dm_cos(um * (zp + h));
+        amt = dm_cos(umt * (zf + h)) * dm_cos(umt * (zp + h)) / h;
+        dam = -um * ac * dm_sin(um * (zf + h)) * dm_cos(um * (zp + h));
+        damt = -umt * dm_sin(umt * (zf + h)) * dm_cos(umt * (zp + h)) / h;
         rm[0] = am * k0 - amt * k0t;
         rm[1] = -um * am * k1 + umt * amt * k1t;
         rm[2] = dam * k0 - damt * k0t;

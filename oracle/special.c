@@ -11,6 +11,7 @@
  * S. Zhang & J. Jin, "Computation of Special Functions", Wiley 1996.
  */
 #include "oracle_internal.h"
+#include "detmath.h"
 
 /* Fortran x**n for an integer exponent (binary powering). */
 static double powi(double x, int n)
@@ -155,7 +156,10 @@ void orc_limes(int n, double *s, double *rlimes, int *ipade, int *kpade, double 
 }
 
 /*
- * IK01A, FinGrnExtSubs.f90:538-635: K0(x), K1(x) for x >= 0.
+ * IK01A, FinGrnExtSubs.f90:538-635: K0(x), K1(x) for x >= 0.  Its exp and
+ * log are the bit-reproducible ones of detmath.h, shared with the GPU code:
+ * K0/K1 feed the epsilon-accelerated series, which amplifies last-bit
+ * differences of the math library.
  * The reference reads WW before assigning it on the first pass of the K0
  * series (FinGrnExtSubs.f90:608); it is taken as 0 here, which cannot stop
  * the series on its first term.
@@ -200,7 +204,7 @@ void orc_ik01a(double x, double *bk0, double *bk1)
         k0 = 12;
         if (x >= 35.0) k0 = 9;
         if (x >= 50.0) k0 = 7;
-        ca = exp(x) / sqrt(2.0 * pi * x);
+        ca = dm_exp(x) / sqrt(2.0 * pi * x);
         bi0 = 1.0;
         xr = 1.0 / x;
         for (k = 1; k <= k0; ++k) bi0 = bi0 + A[k - 1] * powi(xr, k);
@@ -210,7 +214,7 @@ void orc_ik01a(double x, double *bk0, double *bk1)
         bi1 = ca * bi1;
     }
     if (x <= 9.0) {
-        ct = -(log(x / 2.0) + el);
+        ct = -(dm_log(x / 2.0) + el);
         *bk0 = 0.0;
         w0 = 0.0;
         r = 1.0;

@@ -62,7 +62,7 @@ def synthetic(case, precision=hams_b200.PREC_FP64, rho=1025.0, g=9.81):
 @pytest.mark.parametrize("omega,h", [(0.05, 70.0), (0.8, 50.0), (2.5, 50.0), (1.2, 14.5)])
 def test_fingreen_pairs_all_branches(omega, h):
     rng = np.random.default_rng(7)
-    d, ctx = deck_context("config1")
+    _, ctx = synthetic(dict(bodies=[meshgen.cylinder(4.0, 8.0, 8, 2, 2)], centres=[(0.0, 0.0, 0.0)], depth=h))
     w = hams_b200.wave_properties(omega, h, 9.80665)
     ow = oracle_lib.OrcWave()
     oracle_lib.load().orc_wave_props(3, omega, h, 9.80665, 0, oracle_lib.ctypes.byref(ow))

@@ -11,9 +11,13 @@ relative Frobenius norms per file, in the style of the reference's own
 count of entries printed identically.
 
 Observed with the oracle (relative Frobenius, worst of the six files):
-  config1  (3 x 234 panels, h=70 m, omega 0.05-0.07):  A 3.4e-7, B 2.1e-4, X 5.9e-8
+  config1  (3 x 234 panels, h=70 m, omega 0.05-0.07):  A 3.4e-7, B 1.3e-4, X 3.0e-8
   example2 (10 x 234 panels, h=14.5 m, T=0.5, 1 s):   A 4.9e-6, B 2.4e-5, X 3.3e-6
   example5 (1 x 234 + 383 lid panels, h=70 m):        A 1.9e-5, B 9.0e-3, X 3.0e-6
+The Wynn-epsilon extrapolation of the EIGENE/PIDCOCK series turns a one-ulp
+difference of sin/cos/exp/log into up to 1e-3 in single Green values; the
+oracle evaluates those with correctly rounded functions, as the reference's
+compiler library does, which is what brings config1 to these numbers.
 Damping at these long waves is ~1e-6 of the added mass, and the lid path
 squares the condition number (A^T A), so its last digits are FP noise of the
 reference build; the tolerances carry that.
@@ -29,9 +33,11 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 GOLDEN = os.path.join(HERE, "golden")
 
 # (deck, tol A, tol B, tol X, minimum fraction of significant entries printed identically per A/B/X)
-# Observed fractions: config1 0.92/0.79/0.90, example2 0.73/0.67/0.63, example5 0.80/0.64/0.72.
+# Observed fractions: config1 0.977/0.912/0.968, example2 0.73/0.67/0.63, example5 0.79/0.63/0.71.
+# The epsilon-accelerated series use correctly rounded sin/cos/exp/log (detmath.h); with
+# glibc's versions config1 prints identically for 0.92/0.79/0.90 only.
 CASES = [
-    ("config1", 1e-6, 1e-3, 1e-6, (0.88, 0.75, 0.87)),
+    ("config1", 1e-6, 5e-4, 2e-7, (0.95, 0.88, 0.94)),
     ("example2", 2e-5, 1e-4, 1e-5, (0.70, 0.63, 0.60)),
     ("example5", 1e-4, 3e-2, 1e-5, (0.76, 0.60, 0.68)),
 ]
