@@ -468,7 +468,9 @@ struct hams_ctx {
   cudaEvent_t evf = nullptr;
   static constexpr int kTimings = 15;
   double last_ms[kTimings] = {};
-  std::atomic<long long> launches{0};
+  std::atomic<long long> launches{0};   // kernels of this library
+  std::atomic<long long> lib_calls{0};  // cuBLAS / cuSOLVER / CUB calls
+  cudaEvent_t marks[8] = {};
   int refine_sweeps = 0;
 };
 
@@ -497,6 +499,8 @@ extern "C" void hams_ctx_destroy(hams_ctx* c) {
   for (auto& e : c->ev)
     if (e) cudaEventDestroy(e);
   for (auto& e : c->evb)
+    if (e) cudaEventDestroy(e);
+  for (auto& e : c->marks)
     if (e) cudaEventDestroy(e);
   if (c->evf) cudaEventDestroy(c->evf);
   if (c->solver) cusolverDnDestroy(c->solver);
@@ -568,7 +572,7 @@ static int ctx_setup(hams_ctx* c, const hams_geom* geo) {
     DBuf<char> tbuf;
     TRY(tbuf.alloc(tmp));
     CU(cub::DeviceRadixSort::SortPairs(tbuf.p, tmp, keys.p, keys2.p, idx.p, c->pairs.p, np, 0, 10, c->st));
-    c->launches += 4;
+    c->lib_calls += 1;
     // bin boundaries: first index of each branch in the sorted keys
     std::vector<uint32_t> hk(np);
     CU(cudaMemcpyAsync(hk.data(), keys2.p, np * 4, cudaMemcpyDeviceToHost, c->st));
@@ -632,6 +636,7 @@ extern "C" int hams_ctx_create(const hams_geom* geo, const hams_opts* opts, hams
     cusolverDnSetStream(c->solver, c->st);
     for (auto& e : c->ev) cudaEventCreate(&e);
     for (auto& e : c->evb) cudaEventCreate(&e);
+    for (auto& e : c->marks) cudaEventCreate(&e);
     cudaEventCreate(&c->evf);
     rc = ctx_setup(c, geo);
   }
@@ -718,7 +723,7 @@ static int solve_dev(hams_ctx* c, int nrhs, int* info_host) {
                      (cuDoubleComplex*)c->A.p, tn, &zero, (cuDoubleComplex*)c->C.p, n));
     CUB_(cublasZgemm(c->blas, CUBLAS_OP_T, CUBLAS_OP_N, n, nrhs, tn, &one, (cuDoubleComplex*)c->A.p, tn,
                      (cuDoubleComplex*)c->B.p, tn, &zero, (cuDoubleComplex*)c->D.p, n));
-    c->launches += 2;
+    c->lib_calls += 2;
     M = c->C.p;
     rhs = c->D.p;
     ldr = n;
@@ -734,7 +739,7 @@ static int solve_dev(hams_ctx* c, int nrhs, int* info_host) {
     CUS(cusolverDnZgetrf(c->solver, n, n, (cuDoubleComplex*)M, n, (cuDoubleComplex*)c->work.p, c->ipiv.p, c->info.p));
     CU(cudaEventRecord(c->evf, c->st));
     CUS(cusolverDnZgetrs(c->solver, CUBLAS_OP_N, n, nrhs, (cuDoubleComplex*)M, n, c->ipiv.p, (cuDoubleComplex*)c->X.p, n, c->info.p));
-    c->launches += 2;
+    c->lib_calls += 2;
     CU(cudaMemcpyAsync(info_host, c->info.p, sizeof(int), cudaMemcpyDeviceToHost, c->st));
     return 0;
   }
@@ -751,12 +756,13 @@ static int solve_dev(hams_ctx* c, int nrhs, int* info_host) {
   TRY(c->work32.alloc((size_t)lw * sizeof(cuComplex)));
   CUS(cusolverDnCgetrf(c->solver, n, n, (cuComplex*)c->Af.p, n, (cuComplex*)c->work32.p, c->ipiv.p, c->info.p));
   CU(cudaEventRecord(c->evf, c->st));
-  c->launches += 1;
+  c->lib_calls += 1;
   CU(cudaMemcpyAsync(info_host, c->info.p, sizeof(int), cudaMemcpyDeviceToHost, c->st));
   // x0 = LU^-1 b (in complex64), then refine
   k_z2c<<<592, 256, 0, c->st>>>(c->X.p, c->Xf.p, nx);
   TRY(launch_check(c));
   CUS(cusolverDnCgetrs(c->solver, CUBLAS_OP_N, n, nrhs, (cuComplex*)c->Af.p, n, c->ipiv.p, (cuComplex*)c->Xf.p, n, c->info.p));
+  c->lib_calls += 1;
   k_c2z<<<592, 256, 0, c->st>>>(c->Xf.p, c->X.p, nx);
   TRY(launch_check(c, 2));
   const double tol = c->opts.refine_tol > 0.0 ? c->opts.refine_tol : 1e-12;
@@ -770,8 +776,9 @@ static int solve_dev(hams_ctx* c, int nrhs, int* info_host) {
     CU(cudaMemcpy2DAsync(c->R.p, (size_t)n * 16, rhs, (size_t)ldr * 16, (size_t)n * 16, nrhs, cudaMemcpyDeviceToDevice, c->st));
     CUB_(cublasZgemm(c->blas, CUBLAS_OP_N, CUBLAS_OP_N, n, nrhs, n, &mone, (cuDoubleComplex*)M, n,
                      (cuDoubleComplex*)c->X.p, n, &one, (cuDoubleComplex*)c->R.p, n));
+    c->lib_calls += 1;
     k_colnorm_ratio<<<nrhs, 256, 0, c->st>>>(c->R.p, rhs, n, n, c->colratio.p);
-    TRY(launch_check(c, 2));
+    TRY(launch_check(c));
     // the relative residual is checked against the rhs column scale
     CU(cudaMemcpyAsync(ratio.data(), c->colratio.p, nrhs * 8, cudaMemcpyDeviceToHost, c->st));
     CU(cudaStreamSynchronize(c->st));
@@ -784,8 +791,9 @@ static int solve_dev(hams_ctx* c, int nrhs, int* info_host) {
     prev = worst;
     k_z2c<<<592, 256, 0, c->st>>>(c->R.p, c->Xf.p, nx);
     CUS(cusolverDnCgetrs(c->solver, CUBLAS_OP_N, n, nrhs, (cuComplex*)c->Af.p, n, c->ipiv.p, (cuComplex*)c->Xf.p, n, c->info.p));
+    c->lib_calls += 1;
     k_c2z_add<<<592, 256, 0, c->st>>>(c->Xf.p, c->X.p, nx);
-    TRY(launch_check(c, 3));
+    TRY(launch_check(c, 2));
   }
   return 0;
 }
@@ -948,3 +956,58 @@ extern "C" int hams_last_timings(hams_ctx* c, double* ms, int32_t n) {
 }
 
 extern "C" int64_t hams_launch_count(hams_ctx* c) { return c ? (int64_t)c->launches.load() : 0; }
+
+extern "C" int64_t hams_library_call_count(hams_ctx* c) { return c ? (int64_t)c->lib_calls.load() : 0; }
+
+extern "C" int hams_mark(hams_ctx* c, int32_t slot) {
+  if (!c || slot < 0 || slot >= 8) return fail(HAMS_ERR_ARG, "bad mark slot");
+  CU(cudaEventRecord(c->marks[slot], c->st));
+  return 0;
+}
+
+extern "C" int hams_mark_elapsed(hams_ctx* c, int32_t a, int32_t b, double* ms) {
+  if (!c || !ms || a < 0 || a >= 8 || b < 0 || b >= 8) return fail(HAMS_ERR_ARG, "bad mark slot");
+  CU(cudaEventSynchronize(c->marks[b]));
+  float f = 0.0f;
+  CU(cudaEventElapsedTime(&f, c->marks[a], c->marks[b]));
+  *ms = f;
+  return 0;
+}
+
+// Dependent-chain FP64 FMA throughput: each thread runs 8 independent chains.
+__global__ void k_fp64_peak(double* out, int iters) {
+  double a0 = threadIdx.x * 1e-9, a1 = a0 + 1e-9, a2 = a0 + 2e-9, a3 = a0 + 3e-9;
+  double a4 = a0 + 4e-9, a5 = a0 + 5e-9, a6 = a0 + 6e-9, a7 = a0 + 7e-9;
+  const double m = 0.999999999, c = 1e-12;
+  for (int i = 0; i < iters; ++i) {
+    a0 = fma(a0, m, c); a1 = fma(a1, m, c); a2 = fma(a2, m, c); a3 = fma(a3, m, c);
+    a4 = fma(a4, m, c); a5 = fma(a5, m, c); a6 = fma(a6, m, c); a7 = fma(a7, m, c);
+  }
+  double s = a0 + a1 + a2 + a3 + a4 + a5 + a6 + a7;
+  if (s == 12345.0) out[0] = s;  // keeps the chains live
+}
+
+extern "C" int hams_measure_fp64_peak(int32_t device, double* tflops) {
+  g_err.clear();
+  if (!tflops) return fail(HAMS_ERR_ARG, "null argument");
+  CU(cudaSetDevice(device));
+  int sms = 0;
+  CU(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+  DBuf<double> out;
+  TRY(out.alloc(1));
+  cudaEvent_t e0, e1;
+  CU(cudaEventCreate(&e0));
+  CU(cudaEventCreate(&e1));
+  const int iters = 1 << 16, threads = 256, blocks = sms * 8;
+  k_fp64_peak<<<blocks, threads>>>(out.p, 1024);  // warm-up
+  CU(cudaEventRecord(e0));
+  k_fp64_peak<<<blocks, threads>>>(out.p, iters);
+  CU(cudaEventRecord(e1));
+  CU(cudaEventSynchronize(e1));
+  float ms = 0.0f;
+  CU(cudaEventElapsedTime(&ms, e0, e1));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  *tflops = 2.0 * 8.0 * iters * (double)threads * blocks / (ms * 1e-3) / 1e12;
+  return 0;
+}

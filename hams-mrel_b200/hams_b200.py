@@ -71,6 +71,13 @@ def load_library(path=LIB_PATH):
     lib.hams_launch_count.argtypes = [ctypes.c_void_p]
     lib.hams_launch_count.restype = ctypes.c_int64
     lib.hams_last_error.restype = ctypes.c_char_p
+    lib.hams_library_call_count.argtypes = [ctypes.c_void_p]
+    lib.hams_library_call_count.restype = ctypes.c_int64
+    lib.hams_mark.argtypes = [ctypes.c_void_p, c_int]
+    lib.hams_mark_elapsed.argtypes = [ctypes.c_void_p, c_int, c_int, P_dbl]
+    lib.hams_measure_fp64_peak.argtypes = [c_int, P_dbl]
+    lib.hams_prepare_geometry.argtypes = [c_int, P_dbl, c_int, P_int, P_int, c_int, P_int, P_dbl, P_dbl, P_dbl, P_dbl,
+                                          P_dbl]
     _LIB = lib
     return lib
 
@@ -95,6 +102,23 @@ def wave_properties(value, depth, g=9.80665, inft=3, sybo_kk=0):
     w = HamsWave()
     _check(load_library().hams_wave_properties(inft, float(value), float(depth), float(g), sybo_kk, ctypes.byref(w)))
     return w
+
+
+def prepare_geometry(xyz, ncn, ncon, body_nelem, xr):
+    """CalNormals[Multi]: panel centres, areas, sizes and generalized normals from the nodes.
+
+    Returns a geometry dict ready for Context (arrays in Fortran order).
+    """
+    xyz = np.asfortranarray(xyz, dtype=np.float64)
+    ncn = np.ascontiguousarray(ncn, dtype=np.int32)
+    ncon = np.asfortranarray(ncon, dtype=np.int32)
+    bn = np.ascontiguousarray(body_nelem, dtype=np.int32)
+    xr = np.asfortranarray(np.asarray(xr, dtype=np.float64).reshape(len(bn), 3))
+    n = ncn.size
+    xyz_p, ds, pnsz, dxyz = np.zeros((n, 3), order="F"), np.zeros(n), np.zeros(n), np.zeros((n, 6), order="F")
+    _check(load_library().hams_prepare_geometry(xyz.shape[0], _d(xyz), n, _i(ncn), _i(ncon), bn.size, _i(bn), _d(xr),
+                                                _d(xyz_p), _d(ds), _d(pnsz), _d(dxyz)))
+    return dict(xyz=xyz, ncn=ncn, ncon=ncon, xyz_p=xyz_p, ds=ds, pnsz=pnsz, dxyz=dxyz, body_nelem=bn)
 
 
 class Context:
@@ -191,4 +215,24 @@ class Context:
                     pairs_eigen=int(ms[14]))
 
     def launch_count(self):
+        """Kernels of this library launched so far on this context."""
         return int(load_library().hams_launch_count(self._h))
+
+    def library_call_count(self):
+        """cuBLAS / cuSOLVER / CUB calls issued so far on this context."""
+        return int(load_library().hams_library_call_count(self._h))
+
+    def mark(self, slot):
+        _check(load_library().hams_mark(self._h, slot))
+
+    def elapsed_ms(self, a, b):
+        ms = ctypes.c_double()
+        _check(load_library().hams_mark_elapsed(self._h, a, b, ctypes.byref(ms)))
+        return ms.value
+
+
+def measure_fp64_peak(device=0):
+    """FP64 FMA throughput of the device, TFLOP/s."""
+    t = ctypes.c_double()
+    _check(load_library().hams_measure_fp64_peak(device, ctypes.byref(t)))
+    return t.value

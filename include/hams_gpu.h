@@ -97,6 +97,14 @@ typedef struct hams_ctx hams_ctx;
  * zero / infinite frequency limit (SYBO = 1 decks), 0 a regular frequency. */
 int hams_wave_properties(int32_t inft, double value, double depth, double g, int32_t sybo_kk, hams_wave *out);
 
+/* Panel centres, areas, longest edges and generalized normals (n, r x n
+ * about each body's reference point xr (nbody,3)) from the nodes: CalNormals
+ * / CalNormalsMulti (ReadPanelMesh.f90:110, ReadPanelMeshMulti.f90:122) with
+ * the routines of NormalProcess.f90.  Host-only; outputs as in hams_geom. */
+int hams_prepare_geometry(int32_t ntnd, const double *xyz, int32_t nelem, const int32_t *ncn, const int32_t *ncon,
+                          int32_t nbody, const int32_t *body_nelem, const double *xr, double *xyz_p, double *ds,
+                          double *pnsz, double *dxyz);
+
 /* Uploads the geometry, evaluates the frequency-independent Rankine panel
  * integrals (SGLINTBD_*, SingularIntgr.f90:44,252) for every field/source
  * pair and sorts the pairs by Green-function branch.  Replaces the setup of
@@ -145,8 +153,21 @@ int hams_eval_green(hams_ctx *ctx, const hams_wave *wave, int32_t npts, const do
  * ms (15 fills all). Returns the number written. */
 int hams_last_timings(hams_ctx *ctx, double *ms, int32_t n);
 
-/* Kernel launches issued by the library since the context was created. */
+/* Kernels of this library launched since the context was created (library
+ * calls into cuBLAS / cuSOLVER / CUB are counted by hams_library_call_count). */
 int64_t hams_launch_count(hams_ctx *ctx);
+int64_t hams_library_call_count(hams_ctx *ctx);
+
+/* Device-time marks on the context's stream: hams_mark records event `slot`
+ * (0..7); hams_mark_elapsed waits for mark b and returns the milliseconds
+ * between marks a and b. */
+int hams_mark(hams_ctx *ctx, int32_t slot);
+int hams_mark_elapsed(hams_ctx *ctx, int32_t a, int32_t b, double *ms);
+
+/* FP64 fused multiply-add throughput of the device in TFLOP/s (2 flops per
+ * FMA), measured with independent dependency chains on every SM: the
+ * denominator of the Green-function kernels' roofline. */
+int hams_measure_fp64_peak(int32_t device, double *tflops);
 
 /* Message of the last failing call on this thread ("" if none). */
 const char *hams_last_error(void);

@@ -55,3 +55,19 @@ def test_wave_properties_limits_and_errors():
         hams_b200.wave_properties(-1.0, 50.0)
     with pytest.raises(hams_b200.HamsError):
         hams_b200.wave_properties(1.0, 50.0, inft=9)
+
+
+@pytest.mark.parametrize("deck", ["config1", "example5"])
+def test_prepare_geometry_matches_checker(deck):
+    d = oracle_lib.load_deck(os.path.join(REPO, "tests", "golden", deck, "input"))
+    g = hams_b200.prepare_geometry(d["xyz"], d["ncn"], d["ncon"], d["body_nelem"], d["xr"])
+    for k in ("xyz_p", "ds", "pnsz"):
+        assert np.array_equal(g[k], d[k]), k
+    # generalized-mode files would override dxyz; these decks have none
+    assert np.array_equal(g["dxyz"], d["dxyz"])
+
+
+def test_prepare_geometry_rejects_bad_connectivity():
+    xyz = np.zeros((4, 3))
+    with pytest.raises(hams_b200.HamsError):
+        hams_b200.prepare_geometry(xyz, [4], [[1, 2, 3, 9]], [1], [[0, 0, 0]])
