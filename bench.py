@@ -1,0 +1,368 @@
+"""Throughput of the per-frequency BEM build-and-solve on B200.
+
+Workload: the 3 x 3 array of truncated cylinders (radius 4 m, draft 8 m,
+20 m spacing, 600 quad panels each, 5,400 panels) in 50 m of water,
+rho = 1025, g = 9.81, frequencies 0.2-2.5 rad/s (40), headings 0/30/60/90 deg
+(54 radiation + 4 diffraction right-hand sides).  A step is one frequency:
+Green functions and assembly of the 5,400 x 5,400 complex system, the LU
+factorisation and solve, and the added-mass / damping / excitation
+reductions.  Synthetic parametric mesh (no external data).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--form mixed|fp64]
+  python bench.py --impl reference ...   # the CPU implementation on the host cores
+
+Each rank solves its own K frequencies (weak scaling, no data-path
+collective); the timed region is the max over ranks of the device time
+between two events on the library's stream.  Rank 0 prints one JSON line.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(REPO, "hams-mrel_b200"))
+
+import meshgen  # noqa: E402
+
+METRIC = "freq-solves/s @5.4k panels: surrogate+mixed vs plain FP64 GPU @≤1e-4 rel err"
+UNIT = "freq-solves/s"
+RHO, G = 1025.0, 9.81
+WORKLOAD = "3x3 cylinder array R=4 T=8 spacing 20 m, 5400 quad panels, depth 50 m, 40 freq 0.2-2.5 rad/s, " \
+           "headings 0/30/60/90 deg (54 rad + 4 dif RHS)"
+
+# FP64 operations per EIGENE panel pair of the series Green kernel, from the
+# executed-instruction counters of one ncu capture of that kernel on this
+# workload: dadd + dmul + 2 dfma (smsp__sass_thread_inst_executed_op_d*), and
+# its DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum).
+EIGENE_FP64_FLOPS_PER_PAIR = None
+EIGENE_DRAM_BYTES_PER_LAUNCH = None
+
+
+def build_case():
+    case = meshgen.case_c2()
+    xyz, ncn, ncon, cnt = meshgen.combine(case["bodies"])
+    return case, xyz, ncn, ncon, cnt, np.array(case["centres"], dtype=np.float64)
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+# ---------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi clock / throttle-reason samples during the timed region."""
+
+    FIELDS = "index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active," \
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown," \
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap"
+
+    def __init__(self, device):
+        self.proc = None
+        self.out = None
+        try:
+            import torch
+
+            uuid = str(torch.cuda.get_device_properties(device).uuid)
+            self.sel = uuid if uuid.startswith("GPU-") else "GPU-" + uuid
+        except Exception:
+            self.sel = str(device)
+
+    def start(self):
+        try:
+            self.out = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", self.sel, f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.out,
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.out.flush()
+        self.out.seek(0)
+        rows = [r.split(",") for r in self.out.read().strip().splitlines() if r.count(",") >= 8]
+        self.out.close()
+        os.unlink(self.out.name)
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        sm, smax, reasons = [], None, set()
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                smax = float(r[2])
+            except ValueError:
+                continue
+            for k, name in enumerate(names):
+                if r[5 + k].strip().lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ------------------------------------------------------- CPU (oracle) timing
+def cpu_sample_time(case, xyz, ncn, ncon, cnt, xr, omega, target_s=8.0, threads=None):
+    """Seconds per frequency of the CPU implementation, from a bounded sample.
+
+    Assembly: the oracle's OpenMP row assembly (every `stride`-th hull row,
+    all host threads), scaled by n / rows.  LU and solve: LAPACK zgetrf /
+    zgetrs (the reference calls the same routines through MKL) on the
+    n x n system, or on a leading m x m block scaled by (n/m)^3 and (n/m)^2
+    when the full factorisation would take longer than a few seconds.
+    Force reductions (O(n * modes)) are left out; they are < 0.1 % of a step.
+    """
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import oracle_lib
+    import scipy.linalg.lapack as lapack
+
+    threads = threads or len(os.sched_getaffinity(0))
+    oc = oracle_lib.Case(xyz, ncn, ncon, cnt, xr, case["depth"], rho=RHO, g=G)
+    oc.opts.nthread = threads
+    n = oc.n
+    betas = np.radians(case["betas_deg"])
+    w = oc.wave(omega)
+    # calibrate the stride on a handful of rows, then time the sample
+    stride = max(1, n // max(threads, 8))
+    t = time.perf_counter()
+    oc.assemble_rows(w, betas, stride, 0)
+    t_probe = time.perf_counter() - t
+    rows_probe = (n + stride - 1) // stride
+    per_row = t_probe / rows_probe
+    want = max(rows_probe, min(n, int(0.6 * target_s / max(per_row, 1e-9))))
+    stride = max(1, n // want)
+    t = time.perf_counter()
+    a, _, _ = oc.assemble_rows(w, betas, stride, 1 % stride if stride > 1 else 0)
+    t_rows = time.perf_counter() - t
+    nr = a.shape[0]
+    t_asm = t_rows * n / nr
+    # LU + solve on a diagonally dominant complex matrix of the same size
+    rng = np.random.default_rng(0)
+    m = min(n, 1350)
+    while True:
+        mat = (rng.standard_normal((m, m)) + 1j * rng.standard_normal((m, m))).astype(np.complex128)
+        mat[np.diag_indices(m)] += 4.0 * np.sqrt(m)
+        rhs = np.asfortranarray(rng.standard_normal((m, 58)) + 0j)
+        mat = np.asfortranarray(mat)
+        t = time.perf_counter()
+        lu, piv, info = lapack.zgetrf(mat, overwrite_a=True)
+        lapack.zgetrs(lu, piv, rhs, overwrite_b=True)
+        t_lu = time.perf_counter() - t
+        if m == n or t_lu * (n / m) ** 3 > 0.4 * target_s:
+            break
+        m = n if (n / m) ** 3 * t_lu < 0.25 * target_s else min(n, 2 * m)
+    t_lin = t_lu * (n / m) ** 3
+    sample = f"oracle assembly of {nr}/{n} rows (stride {stride}) x {n / nr:.1f}; LAPACK zgetrf+zgetrs " \
+             f"(58 RHS) {m}x{m}" + (f" x (n/m)^3 = {(n / m) ** 3:.1f}" if m < n else "") + f"; omega={omega:.3f}"
+    return t_asm + t_lin, threads, sample, dict(assembly_s=t_asm, lu_s=t_lin)
+
+
+def reference_arm(args):
+    """The CPU implementation of the path on the host cores (rank 0 only)."""
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return
+    case, xyz, ncn, ncon, cnt, xr = build_case()
+    omegas = case["omegas"]
+    per = []
+    cores, sample = None, None
+    for s in range(args.warmup + args.steps):
+        om = omegas[s % len(omegas)]
+        sec, cores, sample, _ = cpu_sample_time(case, xyz, ncn, ncon, cnt, xr, om,
+                                                target_s=args.cpu_seconds or 3.0)
+        if s >= args.warmup:
+            per.append(sec)
+    total = sum(per)
+    value = len(per) / total
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / len(per),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "form": "cpu"},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                             "sample": "per step: " + sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------ GPU arm
+def rel(a, b):
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def run_form(hb, dev, geom, case, prec, omegas, betas, warmup, steps, barrier, want_results, sampler=None):
+    ctx = hb.Context(geom, case["depth"], rho=RHO, g=G, precision=prec, device=dev)
+    waves = [hb.wave_properties(om, case["depth"], G) for om in omegas]
+    for s in range(warmup):
+        ctx.solve_frequency(waves[s % len(waves)], betas)
+    results, eig_ms, eig_pairs, sweeps = [], [], 0, []
+    barrier()
+    if sampler:
+        sampler.start()
+    l0, lib0 = ctx.launch_count(), ctx.library_call_count()
+    ctx.mark(0)
+    for s in range(steps):
+        r = ctx.solve_frequency(waves[s % len(waves)], betas)
+        tm = ctx.timings()
+        eig_ms.append(tm["green_eigene"])
+        eig_pairs = tm["pairs_eigene"]
+        sweeps.append(tm["refine_sweeps"])
+        if want_results:
+            results.append(r)
+    ctx.mark(1)
+    ms = ctx.elapsed_ms(0, 1)
+    launches, libcalls = ctx.launch_count() - l0, ctx.library_call_count() - lib0
+    clocks = sampler.stop() if sampler else None
+    barrier()
+    ctx.close()
+    return dict(ms=ms, launches=launches, lib_calls=libcalls, eig_ms=eig_ms, eig_pairs=eig_pairs, results=results,
+                clocks=clocks, sweeps=sweeps)
+
+
+def e2e_form(hb, dev, case, xyz, ncn, ncon, cnt, xr, prec, omegas, betas, steps, barrier):
+    """Deck through the C ABI from host buffers: geometry, context, K frequencies."""
+    import torch
+
+    torch.cuda.synchronize()
+    barrier()
+    t = time.perf_counter()
+    geom = hb.prepare_geometry(xyz, ncn, ncon, cnt, xr)
+    ctx = hb.Context(geom, case["depth"], rho=RHO, g=G, precision=prec, device=dev)
+    for s in range(steps):
+        ctx.solve_frequency(hb.wave_properties(omegas[s % len(omegas)], case["depth"], G), betas)
+    ctx.close()
+    torch.cuda.synchronize()
+    el = time.perf_counter() - t
+    n, nb, ndof = ncn.size, cnt.size, 6 * cnt.size
+    geom_bytes = xyz.nbytes + ncn.astype(np.int32).nbytes + 4 * 4 * n + 8 * (3 + 1 + 1 + 6) * n + 4 * nb
+    wave_bytes = 8 * 205 + 8 * len(betas)
+    h2d = geom_bytes / steps + wave_bytes
+    d2h = 8 * 2 * ndof * ndof + 16 * len(betas) * ndof
+    return el, int(round(h2d)), int(d2h)
+
+
+def gpu_arm(args):
+    import torch
+    import torch.distributed as dist
+
+    ws, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    if ws > 1:
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
+
+    def barrier():
+        torch.cuda.synchronize()
+        if ws > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        if ws == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    import hams_b200 as hb
+
+    case, xyz, ncn, ncon, cnt, xr = build_case()
+    geom = hb.prepare_geometry(xyz, ncn, ncon, cnt, xr)
+    betas = np.radians(case["betas_deg"])
+    allom = case["omegas"]
+    # weak scaling: rank r takes frequencies r*K, r*K+1, ... of the repeated sweep
+    om_rank = np.array([allom[(rank * args.steps + s) % len(allom)] for s in range(args.steps)])
+    om_warm = np.array([allom[(s * 7 + 3) % len(allom)] for s in range(args.warmup)])
+    prec_main = hb.PREC_MIXED if args.form == "mixed" else hb.PREC_FP64
+    want_cmp = args.form == "mixed"
+
+    sampler = ClockSampler(local)
+    main = run_form(hb, local, geom, case, prec_main, np.concatenate([om_warm, om_rank]), betas, args.warmup, 0,
+                    barrier, False)  # warm the library and caches on this deck
+    main = run_form(hb, local, geom, case, prec_main, om_rank, betas, args.warmup, args.steps, barrier, want_cmp, sampler)
+    fp64 = None
+    if want_cmp:
+        fp64 = run_form(hb, local, geom, case, hb.PREC_FP64, om_rank, betas, args.warmup, args.steps, barrier, True)
+    ms = max_over_ranks(main["ms"])
+    ms_fp64 = max_over_ranks(fp64["ms"]) if fp64 else None
+    err = None
+    if fp64:
+        e = [max(rel(a[0], b[0]), rel(a[1], b[1]), rel(a[2], b[2])) for a, b in zip(main["results"], fp64["results"])]
+        err = max_over_ranks(max(e))
+    e2e_s, h2d, d2h = e2e_form(hb, local, case, xyz, ncn, ncon, cnt, xr, prec_main, om_rank, betas, args.steps, barrier)
+    e2e_s = max_over_ranks(e2e_s)
+
+    value = ws * args.steps / (ms * 1e-3)
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64+c64-lu" if args.form == "mixed" else "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "form": args.form, "panels": int(ncn.size),
+                       "rhs_per_step": 6 * int(cnt.size) + len(betas),
+                       "l2": "no flush: the 5400x5400 complex system (0.47 GB) and pair tables exceed the 126 MB L2",
+                       "parallelism": f"frequency shards x{ws}"},
+            "clocks": main["clocks"], "gpu_launches": main["launches"], "library_calls": main["lib_calls"],
+            "e2e": {"value": ws * args.steps / e2e_s, "unit": UNIT, "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h,
+                    "includes": "host geometry prep, context set-up (upload, Rankine tables, pair sort) and K "
+                                "frequency solves through the C ABI from host buffers"}}
+    if fp64:
+        line["fp64_value"] = ws * args.steps / (ms_fp64 * 1e-3)
+        line["rel_err_vs_fp64"] = err
+        line["refine_sweeps_mean"] = float(np.mean(main["sweeps"]))
+    # roofline of the dominant kernel: the EIGENE-branch series Green kernel
+    eig_ms = float(np.mean(main["eig_ms"]))
+    peak = hb.measure_fp64_peak(local) if rank == 0 else None
+    roof = {"kernel": "k_green_series<EIGENE>", "bound": "fp64", "unit": "TFLOP/s", "launch_ms": eig_ms,
+            "pairs_per_launch": main["eig_pairs"], "peak": peak,
+            "peak_source": "measured in this run: FP64 FMA loop on all SMs (no FP64 figure in MEASURED_PEAKS.json)",
+            "achieved": None, "frac": None, "traffic": None}
+    if EIGENE_FP64_FLOPS_PER_PAIR and peak:
+        ach = EIGENE_FP64_FLOPS_PER_PAIR * main["eig_pairs"] / (eig_ms * 1e-3) / 1e12
+        roof.update(achieved=ach, frac=ach / peak, flops_per_pair=EIGENE_FP64_FLOPS_PER_PAIR)
+    if EIGENE_DRAM_BYTES_PER_LAUNCH:
+        roof["traffic"] = EIGENE_DRAM_BYTES_PER_LAUNCH
+    line["roofline"] = roof
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        sec, cores, sample, parts = cpu_sample_time(case, xyz, ncn, ncon, cnt, xr, float(allom[len(allom) // 2]),
+                                                    target_s=args.cpu_seconds or 8.0)
+        line["cpu_baseline"] = {"value": 1.0 / sec, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample,
+                                **{k: round(v, 3) for k, v in parts.items()}}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=40)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    ap.add_argument("--form", choices=["mixed", "fp64"], default="mixed")
+    ap.add_argument("--cpu-seconds", type=float, default=None,
+                    help="CPU work per baseline sample (default 8 s; 3 s per step of --impl reference)")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        reference_arm(args)
+    else:
+        gpu_arm(args)
+
+
+if __name__ == "__main__":
+    main()

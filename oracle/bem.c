@@ -539,6 +539,43 @@ int32_t orc_assemble(const orc_geom *g, const orc_opts *o, const orc_wave *w, in
     return 0;
 }
 
+/* Rows offset, offset+stride, ... of the hull system only (no lids, no
+ * normal equations): the bounded sample the CPU-baseline timing uses.
+ * Outputs have leading dimension nr = number of rows assembled (returned). */
+int32_t orc_assemble_rows(const orc_geom *g, const orc_opts *o, const orc_wave *w, int32_t nbeta, const double *beta,
+                          int32_t stride, int32_t offset, double *amat_d, double *brmat_d, double *bdmat_d)
+{
+    const int n = g->nelem, nsys = g->nsys, nb = g->nbody;
+    int nr = 0, r;
+    if (stride < 1 || offset < 0 || offset >= n) return 0;
+    nr = (n - offset + stride - 1) / stride;
+    zdouble *amat = (zdouble *)amat_d, *brmat = (zdouble *)brmat_d, *bdmat = (zdouble *)bdmat_d;
+    zdouble *wdbc = (zdouble *)calloc((size_t)nbeta * n * 4, sizeof(zdouble));
+    int ib, jel, is, ip;
+    int nthread = o->nthread > 0 ? o->nthread : 0;
+    for (ib = 0; ib < nbeta; ++ib)
+        for (jel = 0; jel < n; ++jel)
+            for (is = 1; is <= nsys; ++is)
+                for (ip = 1; ip <= nsys; ++ip)
+                    wdbc[(((long)ib * n + jel) * 2 + (is - 1)) * 2 + (ip - 1)] = dbc_weight(g, o, w, jel, is, ip, beta[ib]);
+    memset(amat, 0, sizeof(zdouble) * (size_t)nr * n * nsys);
+    memset(brmat, 0, sizeof(zdouble) * (size_t)nr * 6 * nb * nsys);
+    memset(bdmat, 0, sizeof(zdouble) * (size_t)nr * nsys * nbeta);
+#pragma omp parallel num_threads(nthread > 0 ? nthread : omp_get_max_threads())
+    {
+        double *rknbuf = (double *)malloc(sizeof(double) * 4 * (size_t)n * nsys);
+        zdouble *grnbuf = (zdouble *)malloc(sizeof(zdouble) * 4 * (size_t)n * nsys);
+#pragma omp for schedule(dynamic, 1)
+        for (r = 0; r < nr; ++r)
+            assemble_row(g, o, w, g->xyz_p, n, offset + r * stride, 0, nbeta, wdbc, amat + r, nr, brmat + r, nr,
+                         bdmat + r, nr, rknbuf, grnbuf);
+        free(rknbuf);
+        free(grnbuf);
+    }
+    free(wdbc);
+    return nr;
+}
+
 /* ------------------------------------------------------------------ */
 /* Dense complex LU, ZGETRF/ZGETRS semantics                            */
 /* ------------------------------------------------------------------ */

@@ -97,6 +97,11 @@ void orc_special_c(int32_t which, double x, double *out);
 int32_t orc_assemble(const orc_geom *g, const orc_opts *o, const orc_wave *w, int32_t nbeta,
                      const double *beta, double *amat, double *brmat, double *bdmat);
 
+/* Hull rows offset, offset+stride, ... only (no lids): a bounded sample of
+ * orc_assemble for CPU timing. Leading dimension = returned row count. */
+int32_t orc_assemble_rows(const orc_geom *g, const orc_opts *o, const orc_wave *w, int32_t nbeta,
+                          const double *beta, int32_t stride, int32_t offset, double *amat,
+                          double *brmat, double *bdmat);
 /* Partial-pivot complex LU (ZGETRF semantics, 1-based ipiv) and solve. */
 int32_t orc_zgetrf(int32_t n, double *a, int32_t *ipiv, int32_t nthread);
 void orc_zgetrs(int32_t n, int32_t nrhs, const double *a, const int32_t *ipiv, double *b);

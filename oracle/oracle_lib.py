@@ -70,6 +70,9 @@ def load():
     lib.orc_sglint_c.argtypes = [ctypes.POINTER(OrcGeom), c_int, P_dbl, P_dbl]
     lib.orc_assemble.argtypes = [ctypes.POINTER(OrcGeom), ctypes.POINTER(OrcOpts), ctypes.POINTER(OrcWave), c_int,
                                  P_dbl, P_dbl, P_dbl, P_dbl]
+    lib.orc_assemble_rows.argtypes = [ctypes.POINTER(OrcGeom), ctypes.POINTER(OrcOpts), ctypes.POINTER(OrcWave),
+                                      c_int, P_dbl, c_int, c_int, P_dbl, P_dbl, P_dbl]
+    lib.orc_assemble_rows.restype = c_int
     lib.orc_zgetrf.argtypes = [c_int, P_dbl, P_int, c_int]
     lib.orc_zgetrs.argtypes = [c_int, c_int, P_dbl, P_int, P_dbl]
     lib.orc_forces.argtypes = [ctypes.POINTER(OrcGeom), ctypes.POINTER(OrcOpts), ctypes.POINTER(OrcWave), c_int,
@@ -160,6 +163,21 @@ class Case:
         d = np.zeros((n, nsys, max(len(betas), 1)), dtype=np.complex128, order="F")
         lib.orc_assemble(ctypes.byref(self.geom), ctypes.byref(self.opts), ctypes.byref(w), len(betas), dptr(betas),
                          a.ctypes.data_as(P_dbl), b.ctypes.data_as(P_dbl), d.ctypes.data_as(P_dbl))
+        return a, b, d
+
+    def assemble_rows(self, w, betas, stride, offset=0):
+        """Hull rows offset, offset+stride, ... of the system (the timed CPU sample)."""
+        lib = load()
+        n, nsys, ndof = self.n, self.geom.nsys, 6 * self.nbody
+        nr = (n - offset + stride - 1) // stride
+        betas = np.ascontiguousarray(betas, dtype=np.float64)
+        a = np.zeros((nr, n, nsys), dtype=np.complex128, order="F")
+        b = np.zeros((nr, ndof, nsys), dtype=np.complex128, order="F")
+        d = np.zeros((nr, nsys, max(len(betas), 1)), dtype=np.complex128, order="F")
+        got = lib.orc_assemble_rows(ctypes.byref(self.geom), ctypes.byref(self.opts), ctypes.byref(w), len(betas),
+                                    dptr(betas), stride, offset, a.ctypes.data_as(P_dbl), b.ctypes.data_as(P_dbl),
+                                    d.ctypes.data_as(P_dbl))
+        assert got == nr
         return a, b, d
 
     def forces(self, w, betas, xrad, xdif):

@@ -12,8 +12,9 @@ import pytest
 
 REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 GOLDEN = os.path.join(REPO, "tests", "golden")
-if os.path.join(REPO, "tests") not in sys.path:
-    sys.path.insert(0, os.path.join(REPO, "tests"))
+for _d in (os.path.join(REPO, "tests"), os.path.join(REPO, "oracle"), os.path.join(REPO, "hams-mrel_b200")):
+    if _d not in sys.path:
+        sys.path.insert(0, _d)
 
 
 def pytest_configure(config):
