@@ -40,9 +40,11 @@ WORKLOAD = "3x3 cylinder array R=4 T=8 spacing 20 m, 5400 quad panels, depth 50 
 # FP64 operations per EIGENE panel pair of the series Green kernel, from the
 # executed-instruction counters of one ncu capture of that kernel on this
 # workload: dadd + dmul + 2 dfma (smsp__sass_thread_inst_executed_op_d*), and
-# its DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum).
-EIGENE_FP64_FLOPS_PER_PAIR = None
-EIGENE_DRAM_BYTES_PER_LAUNCH = None
+# its DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum).
+# Both belong to the kernel version they were captured from
+# (profiles/k_green_series_eigene_c2_array.md).
+EIGENE_FP64_FLOPS_PER_PAIR = 71716
+EIGENE_DRAM_BYTES_PER_LAUNCH = 10.19e9
 
 
 def build_case():
