@@ -31,6 +31,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -944,6 +945,67 @@ extern "C" int hams_eval_green(hams_ctx* c, const hams_wave* w, int32_t npts, co
   dp.release();
   df.release();
   dout.release();
+  if (ovf) return fail(HAMS_ERR_NUMERIC, "adaptive quadrature stack overflow in the LINTON branch");
+  return 0;
+}
+
+// ---------------------------------------------------------------------------
+// hams_eval_green_static: hams_eval_green without device allocation.  Its
+// staging lives in one fixed reservation per device: the results (4 complex
+// per point), the points (6 doubles), the flags and the overflow word.
+// ---------------------------------------------------------------------------
+constexpr size_t kStaticPts = HAMS_EVAL_STATIC_MAX_POINTS;
+constexpr size_t kStaticOutOff = 0;                                   // double2 (4 * kStaticPts)
+constexpr size_t kStaticPtsOff = kStaticOutOff + 4 * kStaticPts * 16;  // double (6 * kStaticPts)
+constexpr size_t kStaticFlagOff = kStaticPtsOff + 6 * kStaticPts * 8;  // int (kStaticPts)
+constexpr size_t kStaticOvfOff = kStaticFlagOff + kStaticPts * 4;      // int
+constexpr size_t kStaticBytes = (kStaticOvfOff + 4 + 255) / 256 * 256;
+static __device__ __align__(256) unsigned char g_eval_static[kStaticBytes];
+
+constexpr int kStaticMaxDevices = 64;
+static std::mutex g_static_mu;
+static unsigned char* g_static_addr[kStaticMaxDevices] = {};
+
+// Address of the reservation on device `dev` (which must be current): looked
+// up with cudaGetSymbolAddress on the first call for that device, then cached.
+static int static_scratch(int dev, unsigned char** out) {
+  if (dev < 0 || dev >= kStaticMaxDevices) return fail(HAMS_ERR_UNSUPPORTED, "device ordinal %d >= %d", dev, kStaticMaxDevices);
+  std::lock_guard<std::mutex> lock(g_static_mu);
+  if (!g_static_addr[dev]) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_eval_static);
+    if (e != cudaSuccess || !p) return fail(HAMS_ERR_CUDA, "cudaGetSymbolAddress: %s", cudaGetErrorString(e));
+    g_static_addr[dev] = (unsigned char*)p;
+  }
+  *out = g_static_addr[dev];
+  return 0;
+}
+
+extern "C" int hams_eval_green_static(hams_ctx* c, const hams_wave* w, int32_t npts, const double* pts,
+                                      const int32_t* flag, double* grn) {
+  g_err.clear();
+  if (!c || !w || npts < 0 || (npts > 0 && (!pts || !flag || !grn))) return fail(HAMS_ERR_ARG, "null argument");
+  if (npts > HAMS_EVAL_STATIC_MAX_POINTS)
+    return fail(HAMS_ERR_ARG, "npts %d exceeds the static reservation of %d points", npts, HAMS_EVAL_STATIC_MAX_POINTS);
+  if (npts == 0) return 0;
+  if (cudaSetDevice(c->dev) != cudaSuccess) return fail(HAMS_ERR_CUDA, "cudaSetDevice failed");
+  unsigned char* base = nullptr;
+  TRY(static_scratch(c->dev, &base));
+  double2* dout = (double2*)(base + kStaticOutOff);
+  double* dp = (double*)(base + kStaticPtsOff);
+  int* df = (int*)(base + kStaticFlagOff);
+  int* dovf = (int*)(base + kStaticOvfOff);
+  CU(cudaMemcpyAsync(dp, pts, 6 * (size_t)npts * 8, cudaMemcpyHostToDevice, c->st));
+  CU(cudaMemcpyAsync(df, flag, (size_t)npts * 4, cudaMemcpyHostToDevice, c->st));
+  WaveDev wd = wave_dev(c, w);
+  if (c->opts.depth >= 0.0 && !wd.limit) CU(cudaMemcpyAsync(c->wvn.p, w->wvn, HAMS_NK * 8, cudaMemcpyHostToDevice, c->st));
+  CU(cudaMemsetAsync(dovf, 0, sizeof(int), c->st));  // the overflow word must start at zero
+  launch_eval_green((npts + 127) / 128, c->st, npts, dp, df, wd, c->wvn.p, dout, dovf);
+  TRY(launch_check(c));
+  CU(cudaMemcpyAsync(grn, dout, 4 * (size_t)npts * 16, cudaMemcpyDeviceToHost, c->st));
+  int ovf = 0;
+  CU(cudaMemcpyAsync(&ovf, dovf, sizeof(int), cudaMemcpyDeviceToHost, c->st));
+  CU(cudaStreamSynchronize(c->st));
   if (ovf) return fail(HAMS_ERR_NUMERIC, "adaptive quadrature stack overflow in the LINTON branch");
   return 0;
 }

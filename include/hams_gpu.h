@@ -145,6 +145,24 @@ int hams_assemble(hams_ctx *ctx, const hams_wave *wave, int32_t nbeta, const dou
 int hams_eval_green(hams_ctx *ctx, const hams_wave *wave, int32_t npts, const double *pts, const int32_t *flag,
                     double *grn);
 
+/* hams_eval_green without any device allocation (no counterpart in the
+ * reference).  For callers that cannot allocate device memory: a host loop
+ * that evaluates Green functions while solves run on other streams of the
+ * same device (cudaFree inside hams_eval_green synchronizes the whole device
+ * and stalls them), or a process whose device memory is fully committed to
+ * the per-frequency systems.  The staging lives in one fixed reservation per
+ * device of HAMS_EVAL_STATIC_MAX_POINTS points (about 464 KiB of device
+ * memory); larger npts is rejected with HAMS_ERR_ARG.  The first call on a
+ * device looks the reservation up (cudaGetSymbolAddress) and caches it; make
+ * that first call before any stream capture on the device.  Calls on one
+ * device share the reservation: each call waits for its own stream before it
+ * returns, so calls one after another are safe, but calls that overlap in
+ * time on one device (from several host threads) race and must be
+ * serialised by the caller.  Same arguments and results as hams_eval_green. */
+#define HAMS_EVAL_STATIC_MAX_POINTS 4096
+int hams_eval_green_static(hams_ctx *ctx, const hams_wave *wave, int32_t npts, const double *pts,
+                           const int32_t *flag, double *grn);
+
 /* Timing of the last solve in milliseconds: [0] Green/assembly kernels,
  * [1] right-hand sides, [2] factorisation + solves, [3] reductions,
  * [4] whole call, [5..8] Green kernels of the LINTON, PIDCOCK, EIGENE and
