@@ -69,19 +69,34 @@ constexpr int kMaxSeries = 100; // longest PIDCOCK series (NT <= 100)
 // FinGrnExtSubs.f90:370-470); s is overwritten, as in the reference.
 // ---------------------------------------------------------------------------
 __device__ inline double limes(int n, double* s, double* a) {
+  // Each column k of the reference's table is one pass over i.  Its two
+  // loops (the odd column a, then the even column s with the running
+  // maximum of |a|) are fused here: step i produces a(i+1) and then s(i)
+  // from the same operands in the same order, so every entry and the
+  // returned value are bit-identical; old s(i+1) and new a(i) are carried
+  // in registers.  When the s loop of a column would be empty the a loop's
+  // values are never read again, so that column is skipped.
   double rl = s[n], amax = 0.0;
   for (int i = 0; i <= n; ++i) a[i] = 0.0;
   for (int k = 1;; ++k) {
-    if (n - 2 * k + 1 < 0) break;
-    for (int i = 0; i <= n - 2 * k + 1; ++i) a[i] = (s[i + 1] != s[i]) ? a[i + 1] + 1.0 / (s[i + 1] - s[i]) : a[i + 1];
-    if (n - 2 * k < 0) break;
-    for (int i = 0; i <= n - 2 * k; ++i) {
-      s[i] = (a[i + 1] != a[i]) ? s[i + 1] + 1.0 / (a[i + 1] - a[i]) : s[i + 1];
-      if (fabs(a[i]) > amax) {
-        amax = fabs(a[i]);
-        rl = s[i];
-        if (s[i + 1] == s[i]) return rl;
+    const int m = n - 2 * k;  // last i of the s loop
+    if (m < 0) break;
+    double s_i = s[0], s_i1 = s[1];
+    double an_i = (s_i1 != s_i) ? a[1] + 1.0 / (s_i1 - s_i) : a[1];
+    a[0] = an_i;
+    for (int i = 0; i <= m; ++i) {
+      double s_i2 = s[i + 2], a_i2 = a[i + 2];
+      double an_i1 = (s_i2 != s_i1) ? a_i2 + 1.0 / (s_i2 - s_i1) : a_i2;
+      a[i + 1] = an_i1;
+      double sn_i = (an_i1 != an_i) ? s_i1 + 1.0 / (an_i1 - an_i) : s_i1;
+      s[i] = sn_i;
+      if (fabs(an_i) > amax) {
+        amax = fabs(an_i);
+        rl = sn_i;
+        if (s_i1 == sn_i) return rl;
       }
+      s_i1 = s_i2;
+      an_i = an_i1;
     }
   }
   return rl;
@@ -109,18 +124,78 @@ __device__ __forceinline__ void prop_mode(double r, double zfh, double zph, doub
   g[2] = cmk(-wk * dp0 * y0, wk * dp0 * j0);
 }
 
+// Per-mode factors of the eigenfunction series (mode number i >= 2, root
+// wvn[i-1]): pm of EIGEN/EIGENE, ac of PIDCOCK, and the sin/cos of the
+// vertical eigenfunctions at the source (zf + h) and field (zp + h) depths.
+// Each depends on one mode and one panel only.  InlineModes evaluates them
+// for one pair as FinGreen3D does; TableModes reads them from the
+// per-frequency tables that k_mode_tables fills with the same expressions in
+// the same rounding, so both give the same bits.
+struct InlineModes {
+  const double* __restrict__ wvn;
+  double h, v, zfh, zph;
+  __device__ __forceinline__ double umt(int i) const { return (i - 1) * 3.141592653589793 / h; }
+  __device__ __forceinline__ double pm(int i) const {
+    double km = wvn[i - 1], twokmh = 2.0 * km * h;
+    return 4.0 / (1.0 + dm_sin(twokmh) / twokmh) / h;
+  }
+  __device__ __forceinline__ double ac(int i) const {
+    double um = wvn[i - 1];
+    return (um * um + v * v) / ((um * um + v * v) * h - v);
+  }
+  __device__ __forceinline__ void src(int i, double& s, double& c) const { dm_sincos(wvn[i - 1] * zfh, &s, &c); }
+  __device__ __forceinline__ void srct(int i, double& s, double& c) const { dm_sincos(umt(i) * zfh, &s, &c); }
+  __device__ __forceinline__ double fld(int i) const { return dm_cos(wvn[i - 1] * zph); }
+  __device__ __forceinline__ double fldt(int i) const { return dm_cos(umt(i) * zph); }
+};
+
+constexpr int kModeMax = 100;  // mode numbers 0..99 (PIDCOCK uses up to 99)
+
+// Per-frequency mode tables, laid out mode-major so that a warp of pairs with
+// consecutive field points reads consecutive entries.
+struct ModeTab {
+  int n, tn;              // source panels, field points
+  int nmode;              // modes 2..nmode-1 are filled
+  const double* pm;       // (kModeMax)
+  const double* ac;       // (kModeMax)
+  const double2* src;     // (kModeMax, n): sin, cos of wvn[i-1] (zq + h)
+  const double2* srct;    // (kModeMax, n): sin, cos of (i-1) pi/h (zq + h)
+  const double* fld;      // (kModeMax, tn): cos of wvn[i-1] (zp + h)
+  const double* fldt;     // (kModeMax, tn): cos of (i-1) pi/h (zp + h)
+};
+
+struct TableModes {
+  const ModeTab& t;
+  int j, f;  // source panel, field point
+  __device__ __forceinline__ double pm(int i) const { return t.pm[i]; }
+  __device__ __forceinline__ double ac(int i) const { return t.ac[i]; }
+  __device__ __forceinline__ void src(int i, double& s, double& c) const {
+    double2 q = t.src[(size_t)i * t.n + j];
+    s = q.x;
+    c = q.y;
+  }
+  __device__ __forceinline__ void srct(int i, double& s, double& c) const {
+    double2 q = t.srct[(size_t)i * t.n + j];
+    s = q.x;
+    c = q.y;
+  }
+  __device__ __forceinline__ double fld(int i) const { return t.fld[(size_t)i * t.tn + f]; }
+  __device__ __forceinline__ double fldt(int i) const { return t.fldt[(size_t)i * t.tn + f]; }
+};
+
 // EIGEN, FinGreen3D.f90:281-362 (R/h >= 0.5)
+template <class MD>
 __device__ inline void eigen(double r, double zf, double zp, double wk, const double* __restrict__ wvn, double h,
-                             cplx g[3]) {
+                             cplx g[3], const MD& md) {
   double zfh = zf + h, zph = zp + h;
   prop_mode(r, zfh, zph, wk, h, g);
   for (int i = 2; i <= 10; ++i) {
-    double km = wvn[i - 1], twokmh = 2.0 * km * h;
-    double pm = 4.0 / (1.0 + dm_sin(twokmh) / twokmh) / h;
+    double km = wvn[i - 1];
+    double pm = md.pm(i);
     double k0, k1, skzf, ckzf;
     ik01a(km * r, k0, k1);
-    dm_sincos(km * zfh, &skzf, &ckzf);
-    double ckzp = dm_cos(km * zph);
+    md.src(i, skzf, ckzf);
+    double ckzp = md.fld(i);
     double rm0 = pm * k0 * ckzf * ckzp, rm1 = -pm * km * k1 * ckzf * ckzp, rm2 = -pm * km * k0 * skzf * ckzp;
     g[0].re += rm0;
     g[1].re += rm1;
@@ -130,26 +205,35 @@ __device__ inline void eigen(double r, double zf, double zp, double wk, const do
   remove_rankine(r, zf, zp, g);
 }
 
-// Scratch for the epsilon tables of one thread.
-struct SeriesScratch {
-  double s0[kMaxSeries], s1[kMaxSeries], s2[kMaxSeries], a[kMaxSeries + 1];
+// Scratch for the epsilon tables of one thread: N >= the longest series.
+template <int N>
+struct SeriesScratchN {
+  double s0[N], s1[N], s2[N], a[N];
 };
+constexpr int kEigenEMax = 50;   // EIGENE: NT = int(-88.89 R/h + 54.45) <= 50 for R/h >= 0.05
+constexpr int kPidcockMax = 99;  // PIDCOCK: NT = int(-1010.10 R/h + 100.50) <= 99 for R/h >= 0.0005
+using SeriesScratch = SeriesScratchN<kMaxSeries>;
 
 // EIGENE, FinGreen3D.f90:413-506 (0.05 <= R/h < 0.5)
+template <class MD, int N>
 __device__ inline void eigene(double r, double zf, double zp, double wk, const double* __restrict__ wvn, double h,
-                              cplx g[3], SeriesScratch& sc) {
+                              cplx g[3], SeriesScratchN<N>& sc, const MD& md, int* overflow) {
   double rhp = fabs(r / h);
   int nt = (int)(HAMS_F4(-88.89) * rhp + HAMS_F4(54.45));
+  if (nt > N) {  // outside the branch's range of R/h
+    *overflow = 1;
+    nt = N;
+  }
   double zfh = zf + h, zph = zp + h;
   prop_mode(r, zfh, zph, wk, h, g);
   sc.s0[0] = sc.s1[0] = sc.s2[0] = 0.0;
   for (int i = 2; i <= nt; ++i) {
-    double km = wvn[i - 1], twokmh = 2.0 * km * h;
-    double pm = 4.0 / (1.0 + dm_sin(twokmh) / twokmh) / h;
+    double km = wvn[i - 1];
+    double pm = md.pm(i);
     double k0, k1, skzf, ckzf;
     ik01a(km * r, k0, k1);
-    dm_sincos(km * zfh, &skzf, &ckzf);
-    double ckzp = dm_cos(km * zph);
+    md.src(i, skzf, ckzf);
+    double ckzp = md.fld(i);
     sc.s0[i - 1] = sc.s0[i - 2] + pm * k0 * ckzf * ckzp;
     sc.s1[i - 1] = sc.s1[i - 2] + -pm * km * k1 * ckzf * ckzp;
     sc.s2[i - 1] = sc.s2[i - 2] + -pm * km * k0 * skzf * ckzp;
@@ -198,8 +282,9 @@ __device__ inline void pidcock_images(double r, double zf, double zp, double h, 
 }
 
 // PIDCOCK, FinGreen3D.f90:558-660 (0.0005 <= R/h < 0.05)
+template <class MD, int N>
 __device__ inline void pidcock(double r, double zf, double zp, double v, double wk, const double* __restrict__ wvn,
-                               double h, cplx g[3], SeriesScratch& sc) {
+                               double h, cplx g[3], SeriesScratchN<N>& sc, const MD& md, int* overflow) {
   const double pi = 3.141592653589793, ga = 0.5772156649015328;
   double zfh = zf + h, zph = zp + h;
   {
@@ -215,17 +300,21 @@ __device__ inline void pidcock(double r, double zf, double zp, double v, double 
   }
   double rhp = fabs(r / h);
   int nt = (int)(HAMS_F4(-1010.10) * rhp + HAMS_F4(100.50));
+  if (nt > N) {  // outside the branch's range of R/h
+    *overflow = 1;
+    nt = N;
+  }
   sc.s0[0] = sc.s1[0] = sc.s2[0] = 0.0;
   for (int i = 2; i <= nt; ++i) {
     double umt = (i - 1) * pi / h, um = wvn[i - 1];
     double k0, k1, k0t, k1t;
     ik01a(um * r, k0, k1);
     ik01a(umt * r, k0t, k1t);
-    double ac = (um * um + v * v) / ((um * um + v * v) * h - v);
+    double ac = md.ac(i);
     double su, cu, sut, cut;
-    dm_sincos(um * zfh, &su, &cu);
-    dm_sincos(umt * zfh, &sut, &cut);
-    double cup = dm_cos(um * zph), cutp = dm_cos(umt * zph);
+    md.src(i, su, cu);
+    md.srct(i, sut, cut);
+    double cup = md.fld(i), cutp = md.fldt(i);
     double am = ac * cu * cup, amt = cut * cutp / h;
     double dam = -um * ac * su * cup, damt = -umt * sut * cutp / h;
     sc.s0[i - 1] = sc.s0[i - 2] + (am * k0 - amt * k0t);
@@ -534,21 +623,26 @@ __host__ __device__ __forceinline__ int fin_terms(double rr, double h) {
 
 // FINGREEN3D (FinGreen3D.f90:81-155) for one source (xq..) / field (xp..) pair
 // of branch BR (compile-time, so each branch kernel carries only its own
-// scratch).  v = omega^2/g, wk = wvn[0].
-template <int BR>
+// scratch SC, unused by LINTON and EIGEN).  v = omega^2/g, wk = wvn[0]; md
+// supplies the per-mode factors (InlineModes or TableModes).
+// Convenience form with inline mode factors.
+template <int BR, class SC>
 __device__ inline grn4 fingreen3d(double xq, double xp, double yq, double yp, double zq, double zp, double v,
-                                  const double* __restrict__ wvn, double h, int flag, SeriesScratch* sc,
-                                  int* overflow) {
+                                  const double* __restrict__ wvn, double h, int flag, SC* sc, int* overflow);
+template <int BR, class MD, class SC>
+__device__ inline grn4 fingreen3d(double xq, double xp, double yq, double yp, double zq, double zp, double v,
+                                  const double* __restrict__ wvn, double h, int flag, SC* sc, int* overflow,
+                                  const MD& md) {
   double xpq = xq - xp, ypq = yq - yp, zpq = zq + zp;
   double rr = sqrt(xpq * xpq + ypq * ypq);
   double r = sqrt(rr * rr + (zp - zq) * (zp - zq)), r1 = sqrt(rr * rr + zpq * zpq);
   grn4 o;
   cplx fg[3];
   double wk = wvn[0];
-  if (BR == kLinton) linton(rr, zq, zp, v, wk, wvn, h, fg, overflow);
-  else if (BR == kPidcock) pidcock(rr, zq, zp, v, wk, wvn, h, fg, *sc);
-  else if (BR == kEigenE) eigene(rr, zq, zp, wk, wvn, h, fg, *sc);
-  else eigen(rr, zq, zp, wk, wvn, h, fg);
+  if constexpr (BR == kLinton) linton(rr, zq, zp, v, wk, wvn, h, fg, overflow);
+  else if constexpr (BR == kPidcock) pidcock(rr, zq, zp, v, wk, wvn, h, fg, *sc, md, overflow);
+  else if constexpr (BR == kEigenE) eigene(rr, zq, zp, wk, wvn, h, fg, *sc, md, overflow);
+  else eigen(rr, zq, zp, wk, wvn, h, fg, md);
   if (rr == 0.0) fg[1] = cmk(0.0, 0.0);
   o.g[0] = fg[0];
   o.g[3] = fg[2];
@@ -572,6 +666,13 @@ __device__ inline grn4 fingreen3d(double xq, double xp, double yq, double yp, do
     o.g[3].re -= (zpq * ir13 + (zq - zp) * ir3);
   }
   return o;
+}
+
+template <int BR, class SC>
+__device__ inline grn4 fingreen3d(double xq, double xp, double yq, double yp, double zq, double zp, double v,
+                                  const double* __restrict__ wvn, double h, int flag, SC* sc, int* overflow) {
+  InlineModes md{wvn, h, v, zq + h, zp + h};
+  return fingreen3d<BR>(xq, xp, yq, yp, zq, zp, v, wvn, h, flag, sc, overflow, md);
 }
 
 // Zero- and infinite-frequency limits of both Green functions

@@ -9,11 +9,16 @@
 // kernels (hams_gpu.cu) keep fused multiply-adds.
 #include "kernels.cuh"
 
-template <int BR>
-__global__ void __launch_bounds__(128) k_green_series(DevGeom g, WaveDev w, const double* __restrict__ wvn,
-                                                      const uint32_t* __restrict__ pairs, long long count,
-                                                      const double* __restrict__ rs, const double* __restrict__ rd,
-                                                      double2* __restrict__ A, double2* __restrict__ S, int* ovf) {
+// 128 threads and at most 64 registers per thread (8 blocks per SM): the
+// series are latency-bound, and the extra resident warps outweigh the few
+// spills (measured on the 5,400-panel array: EIGENE 54 ms at 116 registers,
+// 38 ms at 64).
+template <int BR, int N>
+__global__ void __launch_bounds__(128, 8) k_green_series(DevGeom g, WaveDev w, const double* __restrict__ wvn,
+                                                      hams::ModeTab mt, const uint32_t* __restrict__ pairs,
+                                                      long long count, const double* __restrict__ rs,
+                                                      const double* __restrict__ rd, double2* __restrict__ A,
+                                                      double2* __restrict__ S, int* ovf) {
   long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= count) return;
   size_t p = pairs[t];
@@ -25,20 +30,59 @@ __global__ void __launch_bounds__(128) k_green_series(DevGeom g, WaveDev w, cons
   if (w.limit) {
     G = hams::green_limit(w.limit == 2, xq, xp, yq, yp, zq, zp, flag);
   } else {
-    hams::SeriesScratch sc;
+    hams::SeriesScratchN<N> sc;
+    hams::TableModes md{mt, j, i};
     int o = 0;
-    G = hams::fingreen3d<BR>(xq, xp, yq, yp, zq, zp, w.v, wvn, w.h, flag, &sc, &o);
+    G = hams::fingreen3d<BR>(xq, xp, yq, yp, zq, zp, w.v, wvn, w.h, flag, &sc, &o, md);
+    if (o) atomicOr(ovf, 1);
   }
   store_pair(g, p, i, j, G, rs, rd, A, S);
 }
 
 void launch_green_series(int br, unsigned blocks, cudaStream_t st, DevGeom g, WaveDev w, const double* wvn,
-                         const uint32_t* pairs, long long count, const double* rs, const double* rd, double2* A,
-                         double2* S, int* ovf) {
+                         const hams::ModeTab& mt, const uint32_t* pairs, long long count, const double* rs,
+                         const double* rd, double2* A, double2* S, int* ovf) {
   if (br == hams::kPidcock)
-    k_green_series<hams::kPidcock><<<blocks, 128, 0, st>>>(g, w, wvn, pairs, count, rs, rd, A, S, ovf);
+    k_green_series<hams::kPidcock, hams::kPidcockMax>
+        <<<blocks, 128, 0, st>>>(g, w, wvn, mt, pairs, count, rs, rd, A, S, ovf);
   else
-    k_green_series<hams::kEigenE><<<blocks, 128, 0, st>>>(g, w, wvn, pairs, count, rs, rd, A, S, ovf);
+    k_green_series<hams::kEigenE, hams::kEigenEMax>
+        <<<blocks, 128, 0, st>>>(g, w, wvn, mt, pairs, count, rs, rd, A, S, ovf);
+}
+
+// Per-frequency mode tables (ModeTab) for modes 2..nmode-1: one thread per
+// (mode, panel) entry, the expressions of InlineModes (green.cuh), compiled
+// here without fused multiply-adds like the series that read them.
+__global__ void k_mode_tables(DevGeom g, WaveDev w, const double* __restrict__ wvn, int nmode, double* pm, double* ac,
+                              double2* src, double2* srct, double* fld, double* fldt) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  int i = blockIdx.y + 2;  // mode number
+  if (i >= nmode) return;
+  const double h = w.h;
+  if (k < g.n) {
+    hams::InlineModes md{wvn, h, w.v, g.xq[k + 2 * g.n] + h, 0.0};
+    double s, c;
+    md.src(i, s, c);
+    src[(size_t)i * g.n + k] = make_double2(s, c);
+    md.srct(i, s, c);
+    srct[(size_t)i * g.n + k] = make_double2(s, c);
+  }
+  if (k < g.tn) {
+    hams::InlineModes md{wvn, h, w.v, 0.0, g.fxyz[k + 2 * g.tn] + h};
+    fld[(size_t)i * g.tn + k] = md.fld(i);
+    fldt[(size_t)i * g.tn + k] = md.fldt(i);
+  }
+  if (k == 0) {
+    hams::InlineModes md{wvn, h, w.v, 0.0, 0.0};
+    pm[i] = md.pm(i);
+    ac[i] = md.ac(i);
+  }
+}
+
+void launch_mode_tables(cudaStream_t st, DevGeom g, WaveDev w, const double* wvn, int nmode, double* pm, double* ac,
+                        double2* src, double2* srct, double* fld, double* fldt) {
+  dim3 grid((g.tn + 127) / 128, nmode - 2);
+  k_mode_tables<<<grid, 128, 0, st>>>(g, w, wvn, nmode, pm, ac, src, srct, fld, fldt);
 }
 
 // Batch Green evaluation of hams_eval_green: any branch, one pair per thread.
@@ -54,14 +98,21 @@ __global__ void k_eval_green(int npts, const double* __restrict__ pts, const int
   } else if (w.h < 0.0) {
     G = hams::infgreen3d(xq, xp, yq, yp, zq, zp, w.v, flag[t]);
   } else {
-    hams::SeriesScratch sc;
     int o = 0;
     double rr = sqrt((xq - xp) * (xq - xp) + (yq - yp) * (yq - yp));
     switch (hams::fin_branch(rr, w.h)) {
-      case hams::kLinton: G = hams::fingreen3d<hams::kLinton>(xq, xp, yq, yp, zq, zp, w.v, wvn, w.h, flag[t], &sc, &o); break;
-      case hams::kPidcock: G = hams::fingreen3d<hams::kPidcock>(xq, xp, yq, yp, zq, zp, w.v, wvn, w.h, flag[t], &sc, &o); break;
-      case hams::kEigenE: G = hams::fingreen3d<hams::kEigenE>(xq, xp, yq, yp, zq, zp, w.v, wvn, w.h, flag[t], &sc, &o); break;
-      default: G = hams::fingreen3d<hams::kEigen>(xq, xp, yq, yp, zq, zp, w.v, wvn, w.h, flag[t], &sc, &o); break;
+      case hams::kLinton: G = hams::fingreen3d<hams::kLinton>(xq, xp, yq, yp, zq, zp, w.v, wvn, w.h, flag[t], (void*)nullptr, &o); break;
+      case hams::kPidcock: {
+        hams::SeriesScratchN<hams::kPidcockMax> sc;
+        G = hams::fingreen3d<hams::kPidcock>(xq, xp, yq, yp, zq, zp, w.v, wvn, w.h, flag[t], &sc, &o);
+        break;
+      }
+      case hams::kEigenE: {
+        hams::SeriesScratchN<hams::kEigenEMax> sc;
+        G = hams::fingreen3d<hams::kEigenE>(xq, xp, yq, yp, zq, zp, w.v, wvn, w.h, flag[t], &sc, &o);
+        break;
+      }
+      default: G = hams::fingreen3d<hams::kEigen>(xq, xp, yq, yp, zq, zp, w.v, wvn, w.h, flag[t], (void*)nullptr, &o); break;
     }
     if (o) atomicOr(ovf, 1);
   }

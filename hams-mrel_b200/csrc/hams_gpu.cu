@@ -134,11 +134,14 @@ __global__ void k_pair_keys(DevGeom g, double h, uint32_t* __restrict__ keys, ui
 // ---------------------------------------------------------------------------
 // LINTON (BR = 0) and EIGEN (BR = 3) pairs; the epsilon-series branches are
 // in green_series.cu.
+// EIGEN runs at 8 blocks per SM like the series kernels; LINTON's adaptive
+// quadrature keeps its registers.
 template <int BR>
-__global__ void __launch_bounds__(128) k_green_fin(DevGeom g, WaveDev w, const double* __restrict__ wvn,
-                                                   const uint32_t* __restrict__ pairs, long long count,
-                                                   const double* __restrict__ rs, const double* __restrict__ rd,
-                                                   double2* __restrict__ A, double2* __restrict__ S, int* ovf) {
+__global__ void __launch_bounds__(128, BR == hams::kEigen ? 8 : 1) k_green_fin(DevGeom g, WaveDev w, const double* __restrict__ wvn,
+                                                   hams::ModeTab mt, const uint32_t* __restrict__ pairs,
+                                                   long long count, const double* __restrict__ rs,
+                                                   const double* __restrict__ rd, double2* __restrict__ A,
+                                                   double2* __restrict__ S, int* ovf) {
   long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= count) return;
   size_t p = pairs[t];
@@ -151,7 +154,8 @@ __global__ void __launch_bounds__(128) k_green_fin(DevGeom g, WaveDev w, const d
     G = hams::green_limit(w.limit == 2, xq, xp, yq, yp, zq, zp, flag);
   } else {
     int o = 0;
-    G = hams::fingreen3d<BR>(xq, xp, yq, yp, zq, zp, w.v, wvn, w.h, flag, nullptr, &o);
+    hams::TableModes md{mt, j, i};
+    G = hams::fingreen3d<BR>(xq, xp, yq, yp, zq, zp, w.v, wvn, w.h, flag, (void*)nullptr, &o, md);
     if (o) atomicOr(ovf, 1);
   }
   store_pair(g, p, i, j, G, rs, rd, A, S);
@@ -460,6 +464,9 @@ struct hams_ctx {
   DBuf<double2> A, S, B, part, wd, C, D, X, R;
   DBuf<float2> Af, Xf;
   DBuf<double> wvn, beta, outbuf, colratio;
+  DBuf<double> mt_pm, mt_ac, mt_fld, mt_fldt;  // per-frequency mode tables (finite depth)
+  DBuf<double2> mt_src, mt_srct;
+  hams::ModeTab mt{};
   DBuf<int> ipiv, info, ovf;
   DBuf<char> work;
   DBuf<char> work32;
@@ -596,6 +603,17 @@ static int ctx_setup(hams_ctx* c, const hams_geom* geo) {
   CU(cudaMemcpyAsync(c->chunks.p, c->chunks_h.data(), c->chunks_h.size() * sizeof(int2), cudaMemcpyHostToDevice, c->st));
   CU(cudaMemcpyAsync(c->chunk_body.p, cb.data(), cb.size() * sizeof(int), cudaMemcpyHostToDevice, c->st));
 
+  if (c->opts.depth >= 0.0) {
+    const size_t km = hams::kModeMax;
+    TRY(c->mt_pm.alloc(km)); TRY(c->mt_ac.alloc(km));
+    TRY(c->mt_src.alloc(km * n)); TRY(c->mt_srct.alloc(km * n));
+    TRY(c->mt_fld.alloc(km * tn)); TRY(c->mt_fldt.alloc(km * tn));
+    // modes needed by the longest series present: PIDCOCK 99, EIGENE 50, EIGEN 10
+    int nmode = 11;
+    if (c->bin_off[3] > c->bin_off[2]) nmode = hams::kEigenEMax + 1;
+    if (c->bin_off[2] > c->bin_off[1]) nmode = hams::kPidcockMax + 1;
+    c->mt = hams::ModeTab{n, tn, nmode, c->mt_pm.p, c->mt_ac.p, c->mt_src.p, c->mt_srct.p, c->mt_fld.p, c->mt_fldt.p};
+  }
   TRY(c->A.alloc(np));
   TRY(c->S.alloc(np));
   TRY(c->wvn.alloc(HAMS_NK));
@@ -675,6 +693,11 @@ static int assemble_dev(hams_ctx* c, const hams_wave* w, int nbeta) {
     k_green_inf<<<grid, 128, 0, c->st>>>(c->g, wd, c->rs.p, c->rd.p, c->A.p, c->S.p);
     TRY(launch_check(c));
   } else {
+    if (!wd.limit) {
+      launch_mode_tables(c->st, c->g, wd, c->wvn.p, c->mt.nmode, c->mt_pm.p, c->mt_ac.p, c->mt_src.p, c->mt_srct.p,
+                         c->mt_fld.p, c->mt_fldt.p);
+      TRY(launch_check(c));
+    }
     for (int br = 0; br < 4; ++br) {
       long long cnt = c->bin_off[br + 1] - c->bin_off[br];
       CU(cudaEventRecord(c->evb[br], c->st));
@@ -682,10 +705,10 @@ static int assemble_dev(hams_ctx* c, const hams_wave* w, int nbeta) {
       const uint32_t* lst = c->pairs.p + c->bin_off[br];
       unsigned blocks = (unsigned)((cnt + 127) / 128);
       switch (br) {
-        case 0: k_green_fin<0><<<blocks, 128, 0, c->st>>>(c->g, wd, c->wvn.p, lst, cnt, c->rs.p, c->rd.p, c->A.p, c->S.p, c->ovf.p); break;
+        case 0: k_green_fin<0><<<blocks, 128, 0, c->st>>>(c->g, wd, c->wvn.p, c->mt, lst, cnt, c->rs.p, c->rd.p, c->A.p, c->S.p, c->ovf.p); break;
         case 1:
-        case 2: launch_green_series(br, blocks, c->st, c->g, wd, c->wvn.p, lst, cnt, c->rs.p, c->rd.p, c->A.p, c->S.p, c->ovf.p); break;
-        default: k_green_fin<3><<<blocks, 128, 0, c->st>>>(c->g, wd, c->wvn.p, lst, cnt, c->rs.p, c->rd.p, c->A.p, c->S.p, c->ovf.p); break;
+        case 2: launch_green_series(br, blocks, c->st, c->g, wd, c->wvn.p, c->mt, lst, cnt, c->rs.p, c->rd.p, c->A.p, c->S.p, c->ovf.p); break;
+        default: k_green_fin<3><<<blocks, 128, 0, c->st>>>(c->g, wd, c->wvn.p, c->mt, lst, cnt, c->rs.p, c->rd.p, c->A.p, c->S.p, c->ovf.p); break;
       }
       TRY(launch_check(c));
     }

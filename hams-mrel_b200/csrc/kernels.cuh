@@ -51,9 +51,12 @@ __device__ __forceinline__ void store_pair(const DevGeom& g, size_t p, int i, in
 // Launchers of the kernels compiled without implicit fused multiply-adds
 // (green_series.cu): the EIGENE (br = 2) and PIDCOCK (br = 1) branches, whose
 // epsilon-extrapolated series must see the same operation sequence as the
-// CPU checker, and the batch evaluator.
+// CPU checker, the per-frequency mode tables they read, and the batch
+// evaluator.
 void launch_green_series(int br, unsigned blocks, cudaStream_t st, DevGeom g, WaveDev w, const double* wvn,
-                         const uint32_t* pairs, long long count, const double* rs, const double* rd, double2* A,
-                         double2* S, int* ovf);
+                         const hams::ModeTab& mt, const uint32_t* pairs, long long count, const double* rs,
+                         const double* rd, double2* A, double2* S, int* ovf);
+void launch_mode_tables(cudaStream_t st, DevGeom g, WaveDev w, const double* wvn, int nmode, double* pm, double* ac,
+                        double2* src, double2* srct, double* fld, double* fldt);
 void launch_eval_green(unsigned blocks, cudaStream_t st, int npts, const double* pts, const int* flag, WaveDev w,
                        const double* wvn, double2* out, int* ovf);

@@ -98,6 +98,44 @@ __device__ inline double eix(double x) {
   return exp(x) / x * ei;
 }
 
+// fl(|num / den|) < 1e-15, the convergence test of the IK01A series, with
+// the IEEE division taken only when the quotient lies within 1e-9 (relative)
+// of the threshold.  Outside that band the product of |den| with the widened
+// threshold, rounded once (relative error 2^-53), decides the same way the
+// correctly rounded quotient would.  NaN, zero or extreme |den| fall back to
+// the division.
+__device__ __forceinline__ bool quot_below_1em15(double num, double den) {
+  double an = fabs(num), ad = fabs(den);
+  if (ad > 1e-280 && ad < 1e280) {
+    if (an < (1.0e-15 * (1.0 - 1e-9)) * ad) return true;
+    if (an > (1.0e-15 * (1.0 + 1e-9)) * ad) return false;
+  }
+  return fabs(num / den) < 1.0e-15;
+}
+
+// The same test for a positive partial sum den >= 1 and a positive term num
+// (the I0 and I1 series): no range checks, and the common "not yet" outcome
+// costs one product and one comparison.
+__device__ __forceinline__ bool term_below_1em15(double num, double den) {
+  if (num > (1.0e-15 * (1.0 + 1e-9)) * den) return false;
+  if (num < (1.0e-15 * (1.0 - 1e-9)) * den) return true;
+  return fabs(num / den) < 1.0e-15;
+}
+
+// 1.0 / k, k*k and k*(k+1) for k = 0..50 as doubles, rounded at compile time
+// exactly as the run-time division and integer conversion.
+struct SeriesConsts {
+  double recip[51], kk[51], kk1[51];
+  constexpr SeriesConsts() : recip{}, kk{}, kk1{} {
+    for (int k = 1; k <= 50; ++k) {
+      recip[k] = 1.0 / k;
+      kk[k] = (double)(k * k);
+      kk1[k] = (double)(k * (k + 1));
+    }
+  }
+};
+static __constant__ SeriesConsts c_series = SeriesConsts();
+
 // K0(x), K1(x), IK01A (FinGrnExtSubs.f90:538-635).  K0/K1 feed the
 // epsilon-accelerated series, whose result moves with the last bit of its
 // inputs, so this routine uses the bit-reproducible exp/log of detmath.h and
@@ -116,17 +154,19 @@ __device__ inline void ik01a(double x, double& bk0, double& bk1) {
   if (x <= 18.0) {
     bi0 = 1.0;
     r = 1.0;
+    // r > 0 and bi0, bi1 >= 1 for x > 0 (a NaN x fails every comparison and
+    // reaches the division, as in the reference)
     for (int k = 1; k <= 50; ++k) {
-      r = 0.25 * r * x2 / (double)(k * k);
+      r = 0.25 * r * x2 / c_series.kk[k];
       bi0 = bi0 + r;
-      if (fabs(r / bi0) < 1.0e-15) break;
+      if (term_below_1em15(r, bi0)) break;
     }
     bi1 = 1.0;
     r = 1.0;
     for (int k = 1; k <= 50; ++k) {
-      r = 0.25 * r * x2 / (double)(k * (k + 1));
+      r = 0.25 * r * x2 / c_series.kk1[k];
       bi1 = bi1 + r;
-      if (fabs(r / bi1) < 1.0e-15) break;
+      if (term_below_1em15(r, bi1)) break;
     }
     bi1 = 0.5 * x * bi1;
   } else {
@@ -152,10 +192,10 @@ __device__ inline void ik01a(double x, double& bk0, double& bk1) {
     r = 1.0;
     bk0 = 0.0;
     for (int k = 1; k <= 50; ++k) {
-      w0 = w0 + 1.0 / k;
-      r = 0.25 * r / (double)(k * k) * x2;
+      w0 = w0 + c_series.recip[k];
+      r = 0.25 * r / c_series.kk[k] * x2;
       bk0 = bk0 + r * (w0 + ct);
-      if (fabs((bk0 - ww) / bk0) < 1.0e-15) break;
+      if (quot_below_1em15(bk0 - ww, bk0)) break;
       ww = bk0;
     }
     bk0 = bk0 + ct;
