@@ -82,6 +82,7 @@ static int fail(int code, const char* fmt, ...) {
   } while (0)
 
 #include "kernels.cuh"
+#include "lu_mixed.h"
 
 // ---------------------------------------------------------------------------
 // setup kernels
@@ -462,7 +463,9 @@ struct hams_ctx {
   DBuf<int> chunk_body;
   // per-frequency buffers
   DBuf<double2> A, S, B, part, wd, C, D, X, R;
-  DBuf<float2> Af, Xf;
+  DBuf<float2> Af, Xf, luw;
+  DBuf<int> perm;
+  int lu_used = -1;  // mixed form: factorisation used by the last solve (HAMS_LU_*)
   DBuf<double> wvn, beta, outbuf, colratio;
   DBuf<double> mt_pm, mt_ac, mt_fld, mt_fldt;  // per-frequency mode tables (finite depth)
   DBuf<double2> mt_src, mt_srct;
@@ -474,7 +477,7 @@ struct hams_ctx {
   cudaEvent_t ev[6] = {};
   cudaEvent_t evb[5] = {};
   cudaEvent_t evf = nullptr;
-  static constexpr int kTimings = 15;
+  static constexpr int kTimings = 16;
   double last_ms[kTimings] = {};
   std::atomic<long long> launches{0};   // kernels of this library
   std::atomic<long long> lib_calls{0};  // cuBLAS / cuSOLVER / CUB calls
@@ -733,6 +736,102 @@ static int assemble_dev(hams_ctx* c, const hams_wave* w, int nbeta) {
   return 0;
 }
 
+// Mixed form: X (n x nrhs, FP64) from the FP64 matrix M (n x n) and the
+// right-hand sides rhs (ld ldr = n): complex64 factorisation of M (block LU
+// of lu_mixed.cu, or the library's Cgetrf), then FP64 iterative refinement
+// R = rhs - M X, X += LU^-1 R until the residual of every column is below
+// refine_tol of that column's scale.  Returns HAMS_ERR_NUMERIC when the
+// factorisation breaks down or the refinement stalls.
+static int mixed_solve(hams_ctx* c, double2* M, const double2* rhs, int ldr, int nrhs, int kind, int* info_host) {
+  const int n = c->n;
+  const cuDoubleComplex one = make_cuDoubleComplex(1.0, 0.0), mone = make_cuDoubleComplex(-1.0, 0.0);
+  size_t nn = (size_t)n * n, nx = (size_t)n * nrhs;
+  TRY(c->Af.alloc(nn));
+  TRY(c->Xf.alloc(nx));
+  TRY(c->R.alloc(nx));
+  TRY(c->colratio.alloc(nrhs));
+  CU(cudaMemcpy2DAsync(c->X.p, (size_t)n * 16, rhs, (size_t)ldr * 16, (size_t)n * 16, nrhs, cudaMemcpyDeviceToDevice, c->st));
+  k_z2c<<<1184, 256, 0, c->st>>>(M, c->Af.p, nn);
+  TRY(launch_check(c));
+  const bool block = kind != HAMS_LU_LIBRARY;
+  c->lu_used = kind;
+  if (block) {
+    TRY(c->luw.alloc(mixed_lu_workspace_elems(n) + nx));
+    TRY(c->perm.alloc(n));
+    long long la = 0, lb = 0;
+    cublasComputeType_t ct = kind == HAMS_LU_BLOCK_TF32 ? CUBLAS_COMPUTE_32F_FAST_TF32 : CUBLAS_COMPUTE_32F_EMULATED_16BFX9;
+    int rc = mixed_lu_factor(c->st, c->blas, ct, n, c->Af.p, c->perm.p, c->luw.p, c->info.p, &la, &lb);
+    c->launches += la;
+    c->lib_calls += lb;
+    if (rc) return fail(HAMS_ERR_NUMERIC, "block LU: %s failed", rc == 1 ? "CUDA" : "cuBLAS");
+    int zp = 0;
+    CU(cudaMemcpyAsync(&zp, c->info.p, sizeof(int), cudaMemcpyDeviceToHost, c->st));
+    CU(cudaStreamSynchronize(c->st));
+    if (zp <= n) return fail(HAMS_ERR_NUMERIC, "block LU: zero pivot in column %d", zp);
+    *info_host = 0;
+  } else {
+    int lw = 0;
+    CUS(cusolverDnCgetrf_bufferSize(c->solver, n, n, (cuComplex*)c->Af.p, n, &lw));
+    TRY(c->work32.alloc((size_t)lw * sizeof(cuComplex)));
+    CUS(cusolverDnCgetrf(c->solver, n, n, (cuComplex*)c->Af.p, n, (cuComplex*)c->work32.p, c->ipiv.p, c->info.p));
+    c->lib_calls += 1;
+    CU(cudaMemcpyAsync(info_host, c->info.p, sizeof(int), cudaMemcpyDeviceToHost, c->st));
+  }
+  CU(cudaEventRecord(c->evf, c->st));
+  // Xf <- LU^-1 Xf
+  auto lu_solve = [&]() -> int {
+    if (block) {
+      long long la = 0, lb = 0;
+      int rc = mixed_lu_solve(c->st, c->blas, n, nrhs, c->Af.p, c->perm.p, c->Xf.p,
+                              c->luw.p + mixed_lu_workspace_elems(n), &la, &lb);
+      c->launches += la;
+      c->lib_calls += lb;
+      if (rc) return fail(HAMS_ERR_CUDA, "block LU solve failed");
+      return 0;
+    }
+    CUS(cusolverDnCgetrs(c->solver, CUBLAS_OP_N, n, nrhs, (cuComplex*)c->Af.p, n, c->ipiv.p, (cuComplex*)c->Xf.p, n,
+                         c->info.p));
+    c->lib_calls += 1;
+    return 0;
+  };
+  k_z2c<<<592, 256, 0, c->st>>>(c->X.p, c->Xf.p, nx);
+  TRY(launch_check(c));
+  TRY(lu_solve());
+  k_c2z<<<592, 256, 0, c->st>>>(c->Xf.p, c->X.p, nx);
+  TRY(launch_check(c));
+  const double tol = c->opts.refine_tol > 0.0 ? c->opts.refine_tol : 1e-12;
+  const int maxit = c->opts.refine_max > 0 ? c->opts.refine_max : 30;
+  std::vector<double> ratio(nrhs);
+  double prev = 1e300;
+  c->refine_sweeps = 0;
+  for (int it = 0;; ++it) {
+    // R = rhs - M_fp64 X   (M still holds the FP64 matrix)
+    CU(cudaMemcpy2DAsync(c->R.p, (size_t)n * 16, rhs, (size_t)ldr * 16, (size_t)n * 16, nrhs, cudaMemcpyDeviceToDevice, c->st));
+    CUB_(cublasZgemm(c->blas, CUBLAS_OP_N, CUBLAS_OP_N, n, nrhs, n, &mone, (cuDoubleComplex*)M, n,
+                     (cuDoubleComplex*)c->X.p, n, &one, (cuDoubleComplex*)c->R.p, n));
+    c->lib_calls += 1;
+    k_colnorm_ratio<<<nrhs, 256, 0, c->st>>>(c->R.p, rhs, n, n, c->colratio.p);  // ldr == n here
+    TRY(launch_check(c));
+    // the relative residual is checked against the rhs column scale
+    CU(cudaMemcpyAsync(ratio.data(), c->colratio.p, nrhs * 8, cudaMemcpyDeviceToHost, c->st));
+    CU(cudaStreamSynchronize(c->st));
+    double worst = 0.0;
+    for (double r : ratio) worst = std::max(worst, r);
+    c->refine_sweeps = it;
+    if (!(worst == worst)) return fail(HAMS_ERR_NUMERIC, "non-finite residual in iterative refinement");
+    if (worst <= tol) break;
+    if (it >= maxit) return fail(HAMS_ERR_NUMERIC, "iterative refinement: %.3e after %d sweeps", worst, it);
+    if (it > 4 && worst > 0.5 * prev) return fail(HAMS_ERR_NUMERIC, "iterative refinement stalled at %.3e", worst);
+    prev = worst;
+    k_z2c<<<592, 256, 0, c->st>>>(c->R.p, c->Xf.p, nx);
+    TRY(launch_check(c));
+    TRY(lu_solve());
+    k_c2z_add<<<592, 256, 0, c->st>>>(c->Xf.p, c->X.p, nx);
+    TRY(launch_check(c));
+  }
+  return 0;
+}
+
 // Solve on the device: X (n x nrhs) from A, B (or normal equations with lids).
 static int solve_dev(hams_ctx* c, int nrhs, int* info_host) {
   const int n = c->n, tn = c->tn;
@@ -767,59 +866,17 @@ static int solve_dev(hams_ctx* c, int nrhs, int* info_host) {
     CU(cudaMemcpyAsync(info_host, c->info.p, sizeof(int), cudaMemcpyDeviceToHost, c->st));
     return 0;
   }
-  // mixed: complex64 LU of a rounded copy + FP64 iterative refinement
-  size_t nn = (size_t)n * n, nx = (size_t)n * nrhs;
-  TRY(c->Af.alloc(nn));
-  TRY(c->Xf.alloc(nx));
-  TRY(c->R.alloc(nx));
-  TRY(c->colratio.alloc(nrhs));
-  k_z2c<<<1184, 256, 0, c->st>>>(M, c->Af.p, nn);
-  TRY(launch_check(c));
-  int lw = 0;
-  CUS(cusolverDnCgetrf_bufferSize(c->solver, n, n, (cuComplex*)c->Af.p, n, &lw));
-  TRY(c->work32.alloc((size_t)lw * sizeof(cuComplex)));
-  CUS(cusolverDnCgetrf(c->solver, n, n, (cuComplex*)c->Af.p, n, (cuComplex*)c->work32.p, c->ipiv.p, c->info.p));
-  CU(cudaEventRecord(c->evf, c->st));
-  c->lib_calls += 1;
-  CU(cudaMemcpyAsync(info_host, c->info.p, sizeof(int), cudaMemcpyDeviceToHost, c->st));
-  // x0 = LU^-1 b (in complex64), then refine
-  k_z2c<<<592, 256, 0, c->st>>>(c->X.p, c->Xf.p, nx);
-  TRY(launch_check(c));
-  CUS(cusolverDnCgetrs(c->solver, CUBLAS_OP_N, n, nrhs, (cuComplex*)c->Af.p, n, c->ipiv.p, (cuComplex*)c->Xf.p, n, c->info.p));
-  c->lib_calls += 1;
-  k_c2z<<<592, 256, 0, c->st>>>(c->Xf.p, c->X.p, nx);
-  TRY(launch_check(c, 2));
-  const double tol = c->opts.refine_tol > 0.0 ? c->opts.refine_tol : 1e-12;
-  const int maxit = c->opts.refine_max > 0 ? c->opts.refine_max : 30;
-  const cuDoubleComplex mone = make_cuDoubleComplex(-1.0, 0.0);
-  std::vector<double> ratio(nrhs);
-  double prev = 1e300;
-  c->refine_sweeps = 0;
-  for (int it = 0; it < maxit; ++it) {
-    // R = rhs - M_fp64 X   (M still holds the FP64 matrix)
-    CU(cudaMemcpy2DAsync(c->R.p, (size_t)n * 16, rhs, (size_t)ldr * 16, (size_t)n * 16, nrhs, cudaMemcpyDeviceToDevice, c->st));
-    CUB_(cublasZgemm(c->blas, CUBLAS_OP_N, CUBLAS_OP_N, n, nrhs, n, &mone, (cuDoubleComplex*)M, n,
-                     (cuDoubleComplex*)c->X.p, n, &one, (cuDoubleComplex*)c->R.p, n));
-    c->lib_calls += 1;
-    k_colnorm_ratio<<<nrhs, 256, 0, c->st>>>(c->R.p, rhs, n, n, c->colratio.p);
-    TRY(launch_check(c));
-    // the relative residual is checked against the rhs column scale
-    CU(cudaMemcpyAsync(ratio.data(), c->colratio.p, nrhs * 8, cudaMemcpyDeviceToHost, c->st));
-    CU(cudaStreamSynchronize(c->st));
-    double worst = 0.0;
-    for (double r : ratio) worst = std::max(worst, r);
-    c->refine_sweeps = it;
-    if (!(worst == worst)) return fail(HAMS_ERR_NUMERIC, "non-finite residual in iterative refinement");
-    if (worst <= tol) break;
-    if (it > 4 && worst > 0.5 * prev) return fail(HAMS_ERR_NUMERIC, "iterative refinement stalled at %.3e", worst);
-    prev = worst;
-    k_z2c<<<592, 256, 0, c->st>>>(c->R.p, c->Xf.p, nx);
-    CUS(cusolverDnCgetrs(c->solver, CUBLAS_OP_N, n, nrhs, (cuComplex*)c->Af.p, n, c->ipiv.p, (cuComplex*)c->Xf.p, n, c->info.p));
-    c->lib_calls += 1;
-    k_c2z_add<<<592, 256, 0, c->st>>>(c->Xf.p, c->X.p, nx);
-    TRY(launch_check(c, 2));
+  // mixed: complex64 LU of a rounded copy + FP64 iterative refinement; the
+  // block LU falls back to the library's partially pivoted LU when its
+  // refinement does not converge
+  const int kind = c->opts.lu_kind;
+  if (kind == HAMS_LU_BLOCK_EMU || kind == HAMS_LU_BLOCK_TF32) {
+    int rc = mixed_solve(c, M, rhs, ldr, nrhs, kind, info_host);
+    if (rc == 0) return 0;
+    if (rc != HAMS_ERR_NUMERIC) return rc;
+    g_err.clear();
   }
-  return 0;
+  return mixed_solve(c, M, rhs, ldr, nrhs, HAMS_LU_LIBRARY, info_host);
 }
 
 static int forces_dev(hams_ctx* c, const hams_wave* w, int nbeta) {
@@ -870,6 +927,7 @@ static int solve_one(hams_ctx* c, const hams_wave* w, int nbeta, const double* b
   }
   if (cudaEventElapsedTime(&ms, c->ev[2], c->evf) == cudaSuccess) c->last_ms[9] = ms;
   c->last_ms[10] = c->opts.precision == HAMS_PREC_MIXED ? (double)c->refine_sweeps : 0.0;
+  c->last_ms[15] = c->opts.precision == HAMS_PREC_MIXED ? (double)c->lu_used : -1.0;
   if (ovf) return fail(HAMS_ERR_NUMERIC, "adaptive quadrature stack overflow in the LINTON branch");
   if (info > 0) return info;  // singular pivot, LAPACK style
   return 0;

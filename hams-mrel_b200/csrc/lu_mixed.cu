@@ -1,0 +1,290 @@
+// lu_mixed.cu -- complex64 LU of the influence matrix for the mixed form.
+//
+// The mixed form factors a complex64 copy of A and recovers FP64 accuracy
+// by iterative refinement against the FP64 matrix (hams_gpu.cu: mixed_solve),
+// which replaces ZGETRF/ZGETRS of RADIATION_SOLVER_MULTI /
+// DIFFRACTION_SOLVER_MULTI (AssbMatxMulti.f90:112,279,346) there.  The
+// factorisation only has to be a good preconditioner, so it is organised for
+// the tensor cores instead of following LAPACK's pivot order:
+//
+//   for each diagonal block k (kNB = 64 rows):
+//     k_diag_lu      one CTA factors A_kk = P_k^T L_kk U_kk in shared memory
+//                    with partial pivoting inside the block, and forms
+//                    L_kk^-1 and U_kk^-1;
+//     k_apply_perm   applies P_k to the rest of block row k;
+//     GEMM           U_kj = L_kk^-1 A_kj, L_ik = A_ik U_kk^-1;
+//     GEMM           A_ij -= L_ik U_kj, the rank-64 trailing update.
+//
+// The complex products run as real GEMMs on the real expansions of the
+// complex matrices (cuBLAS, tensor cores, FP32 accumulation; inputs rounded
+// to TF32, or FP32 emulated on BF16 tensor cores).  Pivoting is local to
+// each diagonal block (P is block diagonal); the FP64 refinement checks the
+// result, and the caller falls back to a partially pivoted LU if the
+// refinement does not converge.
+#include <cublas_v2.h>
+#include <cuda_runtime.h>
+
+#include "lu_mixed.h"
+
+namespace {
+
+constexpr int kNB = 64;
+constexpr int kLd = kNB + 1;  // padded shared-memory leading dimension
+
+// Real expansion of complex matrices.  A complex p x q matrix X becomes the
+// real 2p x 2q matrix X^ with the 2 x 2 block [[xr, -xi], [xi, xr]] in place
+// of each entry; a complex q x r matrix B stored interleaved (column-major
+// float2) is, viewed as floats, the real 2q x r matrix with rows re, im.
+// Then (X B) viewed as floats = X^ B_real and (X Y)^ = X^ Y^, so every
+// complex product of the factorisation is one real GEMM on tensor cores.
+__device__ __forceinline__ void put_expanded(float* E, int lde, int i, int k, float2 x) {
+  E[(size_t)(2 * k) * lde + 2 * i] = x.x;
+  E[(size_t)(2 * k) * lde + 2 * i + 1] = x.y;
+  E[(size_t)(2 * k + 1) * lde + 2 * i] = -x.y;
+  E[(size_t)(2 * k + 1) * lde + 2 * i + 1] = x.x;
+}
+
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+  return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+
+// One CTA of 256 threads: LU with partial pivoting of the nbk x nbk
+// diagonal block at (k0, k0), written back in place (unit L below, U on and
+// above the diagonal); the block's row permutation as global source rows in
+// perm; the expansions of L^-1 and U^-1 (2nbk x 2nbk, ld 2 kNB) in invL,
+// invU.  info gets 1 + the first global column whose pivot is zero.
+__global__ void __launch_bounds__(256) k_diag_lu(float2* A, int lda, int k0, int nbk, int* perm, float* invL,
+                                                 float* invU, int* info) {
+  extern __shared__ float2 sm[];
+  float2* T = sm;                 // [col * kLd + row]
+  float2* X = sm + kNB * kLd;     // L^-1
+  float2* Y = sm + 2 * kNB * kLd; // U^-1
+  __shared__ int piv[kNB];
+  __shared__ int prm[kNB];
+  const int tid = threadIdx.x, tx = tid % 16, ty = tid / 16;
+  for (int e = tid; e < nbk * nbk; e += 256) {
+    int r = e % nbk, c = e / nbk;
+    T[c * kLd + r] = A[(size_t)(k0 + c) * lda + k0 + r];
+  }
+  __syncthreads();
+  for (int j = 0; j < nbk; ++j) {
+    if (tid < 32) {
+      float best = -1.0f;
+      int bi = j;
+      for (int r = j + tid; r < nbk; r += 32) {
+        float2 v = T[j * kLd + r];
+        float a = fabsf(v.x) + fabsf(v.y);
+        if (a > best) {
+          best = a;
+          bi = r;
+        }
+      }
+      for (int o = 16; o; o >>= 1) {
+        float ob = __shfl_xor_sync(0xffffffffu, best, o);
+        int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+        if (ob > best || (ob == best && oi < bi)) {
+          best = ob;
+          bi = oi;
+        }
+      }
+      if (tid == 0) {
+        piv[j] = bi;
+        if (!(best > 0.0f)) atomicMin(info, k0 + j + 1);
+      }
+    }
+    __syncthreads();
+    const int p = piv[j];
+    if (p != j && tid < nbk) {
+      float2 t = T[tid * kLd + j];
+      T[tid * kLd + j] = T[tid * kLd + p];
+      T[tid * kLd + p] = t;
+    }
+    __syncthreads();
+    float2 d = T[j * kLd + j];
+    float dd = d.x * d.x + d.y * d.y;
+    if (dd > 0.0f && tid > j && tid < nbk) {
+      float2 rcp = make_float2(d.x / dd, -d.y / dd);
+      T[j * kLd + tid] = cmul(T[j * kLd + tid], rcp);
+    }
+    __syncthreads();
+    // rank-1 update: tx walks rows (consecutive in shared memory), ty columns
+    for (int c = j + 1 + ty; c < nbk; c += 16) {
+      float2 u = T[c * kLd + j];
+      for (int r = j + 1 + tx; r < nbk; r += 16) {
+        float2 l = T[j * kLd + r], t = T[c * kLd + r];
+        T[c * kLd + r] = make_float2(t.x - (l.x * u.x - l.y * u.y), t.y - (l.x * u.y + l.y * u.x));
+      }
+    }
+    __syncthreads();
+  }
+  if (tid == 0) {  // the block permutation: the same swaps applied to row indices
+    for (int i = 0; i < nbk; ++i) prm[i] = i;
+    for (int j = 0; j < nbk; ++j) {
+      int t = prm[j];
+      prm[j] = prm[piv[j]];
+      prm[piv[j]] = t;
+    }
+  }
+  // inverses by columns, four lanes per column sharing each inner product
+  {
+    const int c = tid / 4, q = tid % 4;
+    const bool live = c < nbk;
+    // L^-1 (unit lower): X(i,c) = -sum_{k=c}^{i-1} L(i,k) X(k,c)
+    if (live)
+      for (int i = q; i < nbk; i += 4) X[c * kLd + i] = make_float2(i == c ? 1.0f : 0.0f, 0.0f);
+    __syncwarp();
+    for (int i = 1; i < nbk; ++i) {
+      float2 s = make_float2(0.0f, 0.0f);
+      if (live && i > c)
+        for (int k = c + q; k < i; k += 4) {
+          float2 l = T[k * kLd + i], x = X[c * kLd + k];
+          s.x += l.x * x.x - l.y * x.y;
+          s.y += l.x * x.y + l.y * x.x;
+        }
+      s.x += __shfl_xor_sync(0xffffffffu, s.x, 1);
+      s.y += __shfl_xor_sync(0xffffffffu, s.y, 1);
+      s.x += __shfl_xor_sync(0xffffffffu, s.x, 2);
+      s.y += __shfl_xor_sync(0xffffffffu, s.y, 2);
+      if (live && i > c && q == 0) X[c * kLd + i] = make_float2(-s.x, -s.y);
+      __syncwarp();
+    }
+    // U^-1 (upper): Y(i,c) = (delta_ic - sum_{k=i+1}^{c} U(i,k) Y(k,c)) / U(i,i)
+    if (live)
+      for (int i = q; i < nbk; i += 4) Y[c * kLd + i] = make_float2(0.0f, 0.0f);
+    __syncwarp();
+    for (int i = nbk - 1; i >= 0; --i) {
+      float2 s = make_float2(0.0f, 0.0f);
+      if (live && i <= c)
+        for (int k = i + 1 + q; k <= c; k += 4) {
+          float2 u = T[k * kLd + i], y = Y[c * kLd + k];
+          s.x += u.x * y.x - u.y * y.y;
+          s.y += u.x * y.y + u.y * y.x;
+        }
+      s.x += __shfl_xor_sync(0xffffffffu, s.x, 1);
+      s.y += __shfl_xor_sync(0xffffffffu, s.y, 1);
+      s.x += __shfl_xor_sync(0xffffffffu, s.x, 2);
+      s.y += __shfl_xor_sync(0xffffffffu, s.y, 2);
+      if (live && i <= c && q == 0) {
+        float2 d = T[i * kLd + i];
+        float dd = d.x * d.x + d.y * d.y;
+        float nx = (i == c ? 1.0f : 0.0f) - s.x, ny = -s.y;
+        Y[c * kLd + i] = dd > 0.0f ? make_float2((nx * d.x + ny * d.y) / dd, (ny * d.x - nx * d.y) / dd)
+                                   : make_float2(0.0f, 0.0f);
+      }
+      __syncwarp();
+    }
+  }
+  __syncthreads();
+  for (int e = tid; e < nbk * nbk; e += 256) {
+    int r = e % nbk, c = e / nbk;
+    A[(size_t)(k0 + c) * lda + k0 + r] = T[c * kLd + r];
+    put_expanded(invL, 2 * kNB, r, c, X[c * kLd + r]);
+    put_expanded(invU, 2 * kNB, r, c, Y[c * kLd + r]);
+  }
+  for (int i = tid; i < nbk; i += 256) perm[k0 + i] = k0 + prm[i];
+}
+
+// E (2w x 2nbk, ld 2w) <- expansion of the w x nbk column panel at (k1, k0).
+__global__ void k_expand_panel(const float2* __restrict__ A, int lda, int k1, int k0, int w, int nbk, float* E) {
+  size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= (size_t)w * nbk) return;
+  int i = (int)(e % w), k = (int)(e / w);
+  put_expanded(E, 2 * w, i, k, A[(size_t)(k0 + k) * lda + k1 + i]);
+}
+
+// Rows k0..k0+nbk-1 of every column outside the diagonal block take the
+// block's permutation: row k0+i receives old row perm[k0+i].
+__global__ void k_apply_perm(float2* A, int lda, int n, int k0, int nbk, const int* __restrict__ perm) {
+  __shared__ float2 tile[kNB][33];
+  const int c0 = blockIdx.x * 32, tx = threadIdx.x % 32, ty = threadIdx.x / 32;  // 256 threads: 8 x 32
+  const int c = c0 + tx;
+  const bool live = c < n && (c < k0 || c >= k0 + nbk);
+  for (int i = ty; i < nbk; i += 8)
+    if (live) tile[i][tx] = A[(size_t)c * lda + perm[k0 + i]];
+  __syncthreads();
+  for (int i = ty; i < nbk; i += 8)
+    if (live) A[(size_t)c * lda + k0 + i] = tile[i][tx];
+}
+
+// X (n x nrhs, ld n) <- rows gathered by perm.
+__global__ void k_gather_rows(const float2* __restrict__ src, float2* __restrict__ dst, int n, int nrhs,
+                              const int* __restrict__ perm) {
+  size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= (size_t)n * nrhs) return;
+  int r = (int)(e % n);
+  size_t c = e / n;
+  dst[e] = src[c * n + perm[r]];
+}
+
+cublasStatus_t sgemm(cublasHandle_t h, cublasComputeType_t ct, int m, int n, int k, float alpha, const float* A,
+                     int lda, const float* B, int ldb, float beta, float* C, int ldc) {
+  return cublasGemmEx(h, CUBLAS_OP_N, CUBLAS_OP_N, m, n, k, &alpha, A, CUDA_R_32F, lda, B, CUDA_R_32F, ldb, &beta, C,
+                      CUDA_R_32F, ldc, ct, CUBLAS_GEMM_DEFAULT);
+}
+
+}  // namespace
+
+// U panel (2kNB x n floats), expanded L panel and its source (2 x 2n x 2kNB),
+// expanded inverses of the diagonal block (2 x 2kNB x 2kNB).
+size_t mixed_lu_workspace_elems(int n) {
+  return (2 * (size_t)kNB * n + 2 * (2 * (size_t)n * 2 * kNB) + 2 * (size_t)(2 * kNB) * (2 * kNB)) / 2 + 1;
+}
+
+int mixed_lu_factor(cudaStream_t st, cublasHandle_t blas, cublasComputeType_t ct, int n, float2* A, int* perm,
+                    float2* work, int* dinfo, long long* launches, long long* lib_calls) {
+  const int smem = 3 * kNB * kLd * (int)sizeof(float2);
+  if (cudaFuncSetAttribute(k_diag_lu, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess) return 1;
+  const int nblk = (n + kNB - 1) / kNB, K2 = 2 * kNB;
+  float* W1 = (float*)work;                     // U panel, real 2nbk x w (ld 2kNB)
+  float* Ehat = W1 + (size_t)K2 * n;            // expanded A_ik, 2w x 2nbk (ld 2w)
+  float* Lhat = Ehat + (size_t)2 * n * K2;      // expanded L_ik, 2w x 2nbk (ld 2w)
+  float* invL = Lhat + (size_t)2 * n * K2;      // 2nbk x 2nbk (ld 2kNB)
+  float* invU = invL + (size_t)K2 * K2;
+  if (cudaMemsetAsync(dinfo, 0x7f, sizeof(int), st) != cudaSuccess) return 1;  // large positive: no zero pivot
+  if (cudaMemsetAsync(invL, 0, 2 * (size_t)K2 * K2 * sizeof(float), st) != cudaSuccess) return 1;
+  float* Ar = (float*)A;  // A viewed as floats: 2n x n, ld 2n
+  for (int b = 0; b < nblk; ++b) {
+    const int k0 = b * kNB, nbk = (n - k0 < kNB) ? n - k0 : kNB, k1 = k0 + nbk, w = n - k1, k2 = 2 * nbk;
+    k_diag_lu<<<1, 256, smem, st>>>(A, n, k0, nbk, perm, invL, invU, dinfo);
+    k_apply_perm<<<(n + 31) / 32, 256, 0, st>>>(A, n, n, k0, nbk, perm);
+    *launches += 2;
+    if (cudaGetLastError() != cudaSuccess) return 1;
+    if (w <= 0) break;
+    k_expand_panel<<<(unsigned)(((size_t)w * nbk + 255) / 256), 256, 0, st>>>(A, n, k1, k0, w, nbk, Ehat);
+    *launches += 1;
+    if (cudaGetLastError() != cudaSuccess) return 1;
+    float* Akj = Ar + (size_t)k1 * 2 * n + 2 * k0;  // real 2nbk x w, ld 2n
+    float* Aij = Ar + (size_t)k1 * 2 * n + 2 * k1;  // real 2w x w, ld 2n
+    // U_kj = L_kk^-1 A_kj;  L_ik^ = A_ik^ U_kk^-1^;  A_ij -= L_ik U_kj
+    if (sgemm(blas, ct, k2, w, k2, 1.0f, invL, K2, Akj, 2 * n, 0.0f, W1, K2) != CUBLAS_STATUS_SUCCESS) return 2;
+    if (sgemm(blas, ct, 2 * w, k2, k2, 1.0f, Ehat, 2 * w, invU, K2, 0.0f, Lhat, 2 * w) != CUBLAS_STATUS_SUCCESS) return 2;
+    if (sgemm(blas, ct, 2 * w, w, k2, -1.0f, Lhat, 2 * w, W1, K2, 1.0f, Aij, 2 * n) != CUBLAS_STATUS_SUCCESS) return 2;
+    *lib_calls += 3;
+    // U_kj back into A; L_ik = the even columns of L_ik^
+    if (cudaMemcpy2DAsync(Akj, (size_t)2 * n * 4, W1, (size_t)K2 * 4, (size_t)k2 * 4, w, cudaMemcpyDeviceToDevice, st) !=
+        cudaSuccess)
+      return 1;
+    if (cudaMemcpy2DAsync(A + (size_t)k0 * n + k1, (size_t)n * 8, Lhat, (size_t)2 * (2 * w) * 4, (size_t)2 * w * 4, nbk,
+                          cudaMemcpyDeviceToDevice, st) != cudaSuccess)
+      return 1;
+  }
+  return 0;
+}
+
+int mixed_lu_solve(cudaStream_t st, cublasHandle_t blas, int n, int nrhs, const float2* A, const int* perm, float2* X,
+                   float2* tmp, long long* launches, long long* lib_calls) {
+  size_t tot = (size_t)n * nrhs;
+  k_gather_rows<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(X, tmp, n, nrhs, perm);
+  *launches += 1;
+  if (cudaGetLastError() != cudaSuccess) return 1;
+  const cuComplex one = make_cuComplex(1.0f, 0.0f);
+  if (cublasCtrsm(blas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N, CUBLAS_DIAG_UNIT, n, nrhs, &one,
+                  (const cuComplex*)A, n, (cuComplex*)tmp, n) != CUBLAS_STATUS_SUCCESS)
+    return 2;
+  if (cublasCtrsm(blas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT, n, nrhs, &one,
+                  (const cuComplex*)A, n, (cuComplex*)tmp, n) != CUBLAS_STATUS_SUCCESS)
+    return 2;
+  *lib_calls += 2;
+  if (cudaMemcpyAsync(X, tmp, tot * sizeof(float2), cudaMemcpyDeviceToDevice, st) != cudaSuccess) return 1;
+  return 0;
+}

@@ -19,6 +19,7 @@ LIB_PATH = os.path.join(_HERE, "libhams_b200.so")
 HAMS_NK = 200
 PREC_FP64 = 0
 PREC_MIXED = 1
+LU_BLOCK_EMU, LU_BLOCK_TF32, LU_LIBRARY = 0, 1, 2
 
 c_int = ctypes.c_int32
 c_dbl = ctypes.c_double
@@ -35,7 +36,7 @@ class HamsGeom(ctypes.Structure):
 class HamsOpts(ctypes.Structure):
     _fields_ = [("depth", c_dbl), ("rho", c_dbl), ("g", c_dbl), ("xw", c_dbl * 2), ("amp", c_dbl), ("isol", c_int),
                 ("irsp", c_int), ("precision", c_int), ("device", c_int), ("refine_tol", c_dbl),
-                ("refine_max", c_int), ("reserved", c_int * 7)]
+                ("refine_max", c_int), ("lu_kind", c_int), ("reserved", c_int * 6)]
 
 
 class HamsWave(ctypes.Structure):
@@ -129,7 +130,7 @@ class Context:
     """
 
     def __init__(self, geom, depth, rho=1000.0, g=9.80665, isol=1, irsp=0, precision=PREC_FP64, device=0,
-                 xw=(0.0, 0.0), amp=1.0, refine_tol=0.0, refine_max=0):
+                 xw=(0.0, 0.0), amp=1.0, refine_tol=0.0, refine_max=0, lu_kind=0):
         lib = load_library()
         self._keep = {}
         f = lambda k, dt: self._keep.setdefault(k, np.asfortranarray(geom[k], dtype=dt))
@@ -148,7 +149,7 @@ class Context:
             g_.ixyz_p = _d(ixyz_p)
         o = HamsOpts(depth=float(depth), rho=float(rho), g=float(g), amp=float(amp), isol=int(isol), irsp=int(irsp),
                      precision=int(precision), device=int(device), refine_tol=float(refine_tol),
-                     refine_max=int(refine_max))
+                     refine_max=int(refine_max), lu_kind=int(lu_kind))
         o.xw[0], o.xw[1] = xw
         self.depth, self.g = float(depth), float(g)
         self._h = ctypes.c_void_p()
@@ -207,12 +208,12 @@ class Context:
 
     def timings(self):
         """Stage times of the last solve (ms), per-branch Green kernel times and pair counts."""
-        ms = np.zeros(15)
-        load_library().hams_last_timings(self._h, _d(ms), 15)
+        ms = np.zeros(16)
+        load_library().hams_last_timings(self._h, _d(ms), 16)
         return dict(green=ms[0], rhs=ms[1], solve=ms[2], forces=ms[3], total=ms[4], green_linton=ms[5],
                     green_pidcock=ms[6], green_eigene=ms[7], green_eigen=ms[8], factor=ms[9], refine_sweeps=int(ms[10]),
                     pairs_linton=int(ms[11]), pairs_pidcock=int(ms[12]), pairs_eigene=int(ms[13]),
-                    pairs_eigen=int(ms[14]))
+                    pairs_eigen=int(ms[14]), lu_used=int(ms[15]))
 
     def launch_count(self):
         """Kernels of this library launched so far on this context."""

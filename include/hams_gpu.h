@@ -38,6 +38,14 @@ enum {
   HAMS_ERR_NUMERIC = -5      /* non-finite result or refinement stalled*/
 };
 
+/* Complex64 factorisation of the mixed form.  BLOCK: 64-row blocks pivoted
+ * inside each diagonal block, the complex products as real GEMMs on the
+ * tensor cores with FP32 accumulation -- inputs rounded to TF32
+ * (BLOCK_TF32) or FP32 emulated on BF16 tensor cores (BLOCK_EMU); the
+ * library's partially pivoted LU (LIBRARY) is also the fallback when the
+ * refinement of a block factorisation does not converge. */
+enum { HAMS_LU_BLOCK_EMU = 0, HAMS_LU_BLOCK_TF32 = 1, HAMS_LU_LIBRARY = 2 };
+
 /* Numerical form of a solve. */
 enum {
   HAMS_PREC_FP64 = 0,  /* plain FP64 drop-in: FP64 assembly, FP64 LU           */
@@ -78,7 +86,8 @@ typedef struct hams_opts {
   int32_t device;   /* CUDA device ordinal                                       */
   double refine_tol;/* mixed: relative residual target of the refinement (<=0: 1e-12) */
   int32_t refine_max;/* mixed: refinement sweeps (<=0: 30)                       */
-  int32_t reserved[7];
+  int32_t lu_kind;  /* mixed: HAMS_LU_BLOCK_EMU (0), HAMS_LU_BLOCK_TF32, HAMS_LU_LIBRARY */
+  int32_t reserved[6];
 } hams_opts;
 
 /* One frequency after CalWaveProperts (ImplementSubs.f90:40): V = w^2/g
@@ -167,8 +176,9 @@ int hams_eval_green_static(hams_ctx *ctx, const hams_wave *wave, int32_t npts, c
  * [1] right-hand sides, [2] factorisation + solves, [3] reductions,
  * [4] whole call, [5..8] Green kernels of the LINTON, PIDCOCK, EIGENE and
  * EIGEN branches (finite depth), [9] LU factorisation, [10] refinement
- * sweeps (mixed form), [11..14] pairs in each branch.  n is the capacity of
- * ms (15 fills all). Returns the number written. */
+ * sweeps (mixed form), [11..14] pairs in each branch, [15] the mixed
+ * form's factorisation (HAMS_LU_*; -1 for FP64).  n is the capacity of ms
+ * (16 fills all). Returns the number written. */
 int hams_last_timings(hams_ctx *ctx, double *ms, int32_t n);
 
 /* Kernels of this library launched since the context was created (library

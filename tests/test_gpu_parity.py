@@ -130,14 +130,39 @@ def test_solve_matches_oracle(deck, nfreq):
         assert rel(ex, oex) < 1e-7, rel(ex, oex)
 
 
-def test_mixed_precision_config1():
-    d, ctx = deck_context("config1", precision=hams_b200.PREC_MIXED)
+@pytest.mark.parametrize("lu_kind", [hams_b200.LU_BLOCK_EMU, hams_b200.LU_BLOCK_TF32, hams_b200.LU_LIBRARY])
+def test_mixed_precision_config1(lu_kind):
+    d, ctx = deck_context("config1", precision=hams_b200.PREC_MIXED, lu_kind=lu_kind)
     oc = oracle_case_from_deck(d)
     betas = np.radians(d["wvhd"])
     for omega in d["wvnb"]:
         am, bd, ex = ctx.solve_frequency(hams_b200.wave_properties(omega, d["h"], 9.80665), betas)
+        assert ctx.timings()["lu_used"] == lu_kind  # no fallback to the library LU
         oam, obd, oex, _ = oc.solve(oc.wave(omega), betas)
         assert rel(am, oam) < 1e-6 and rel(bd, obd) < 1e-6 and rel(ex, oex) < 1e-6
+
+
+@pytest.mark.parametrize("lu_kind", [hams_b200.LU_BLOCK_EMU, hams_b200.LU_BLOCK_TF32])
+def test_mixed_block_lu_array(lu_kind):
+    """2x2 cylinder array (4 x 96 panels, six 64-row blocks) in 40 m: the block LU with
+    refinement against the FP64 oracle, and the refinement stays short."""
+    bodies, centres = [], []
+    for iy in range(2):
+        for ix in range(2):
+            bodies.append(meshgen.cylinder(3.0, 6.0, 16, 4, 2, 15.0 * ix, 15.0 * iy))
+            centres.append((15.0 * ix, 15.0 * iy, 0.0))
+    xyz, ncn, ncon, cnt = meshgen.combine(bodies)
+    oc = oracle_lib.Case(xyz, ncn, ncon, cnt, np.array(centres), 40.0, rho=1025.0, g=9.81)
+    geom = hams_b200.prepare_geometry(xyz, ncn, ncon, cnt, np.array(centres))
+    ctx = hams_b200.Context(geom, 40.0, rho=1025.0, g=9.81, precision=hams_b200.PREC_MIXED, lu_kind=lu_kind)
+    betas = np.radians([0.0, 60.0])
+    for omega in (0.4, 1.6):
+        am, bd, ex = ctx.solve_frequency(hams_b200.wave_properties(omega, 40.0, 9.81), betas)
+        t = ctx.timings()
+        assert t["lu_used"] == lu_kind and t["refine_sweeps"] <= (4 if lu_kind == hams_b200.LU_BLOCK_EMU else 12)
+        oam, obd, oex, _ = oc.solve(oc.wave(omega), betas)
+        assert rel(am, oam) < 1e-7 and rel(bd, obd) < 1e-7 and rel(ex, oex) < 1e-7
+    ctx.close()
 
 
 @pytest.mark.parametrize("omega", [0.1, 1.0, 3.0])
