@@ -34,6 +34,7 @@ import meshgen  # noqa: E402
 METRIC = "freq-solves/s @5.4k panels: surrogate+mixed vs plain FP64 GPU @≤1e-4 rel err"
 UNIT = "freq-solves/s"
 RHO, G = 1025.0, 9.81
+LANES = 4  # frequencies in flight in hams_solve_batch (the library's default)
 WORKLOAD = "3x3 cylinder array R=4 T=8 spacing 20 m, 5400 quad panels, depth 50 m, 40 freq 0.2-2.5 rad/s, " \
            "headings 0/30/60/90 deg (54 rad + 4 dif RHS)"
 
@@ -205,32 +206,28 @@ def rel(a, b):
 
 
 def run_form(hb, dev, geom, case, prec, omegas, betas, warmup, steps, barrier, want_results, sampler=None):
+    """K frequencies through hams_solve_batch (frequencies in flight on several streams), timed
+    between two events on the context's stream."""
     ctx = hb.Context(geom, case["depth"], rho=RHO, g=G, precision=prec, device=dev)
     waves = [hb.wave_properties(om, case["depth"], G) for om in omegas]
-    for s in range(warmup):
-        ctx.solve_frequency(waves[s % len(waves)], betas)
-    results, eig_ms, eig_pairs, sweeps = [], [], 0, []
+    if warmup:  # at least one frequency per lane, so that no lane is created inside the timed region
+        ctx.solve_batch([waves[s % len(waves)] for s in range(max(warmup, LANES))], betas)
     barrier()
     if sampler:
         sampler.start()
     l0, lib0 = ctx.launch_count(), ctx.library_call_count()
     ctx.mark(0)
-    for s in range(steps):
-        r = ctx.solve_frequency(waves[s % len(waves)], betas)
-        tm = ctx.timings()
-        eig_ms.append(tm["green_eigene"])
-        eig_pairs = tm["pairs_eigene"]
-        sweeps.append(tm["refine_sweeps"])
-        if want_results:
-            results.append(r)
+    res = ctx.solve_batch(waves[:steps], betas) if steps else None
     ctx.mark(1)
     ms = ctx.elapsed_ms(0, 1)
     launches, libcalls = ctx.launch_count() - l0, ctx.library_call_count() - lib0
     clocks = sampler.stop() if sampler else None
+    tm = ctx.timings()  # the context's own last frequency
     barrier()
     ctx.close()
-    return dict(ms=ms, launches=launches, lib_calls=libcalls, eig_ms=eig_ms, eig_pairs=eig_pairs, results=results,
-                clocks=clocks, sweeps=sweeps)
+    results = [tuple(r[k] for r in res) for k in range(steps)] if (want_results and res is not None) else []
+    return dict(ms=ms, launches=launches, lib_calls=libcalls, eig_ms=[tm["green_eigene"]], eig_pairs=tm["pairs_eigene"],
+                results=results, clocks=clocks, sweeps=[tm["refine_sweeps"]])
 
 
 def e2e_form(hb, dev, case, xyz, ncn, ncon, cnt, xr, prec, omegas, betas, steps, barrier):
@@ -242,8 +239,7 @@ def e2e_form(hb, dev, case, xyz, ncn, ncon, cnt, xr, prec, omegas, betas, steps,
     t = time.perf_counter()
     geom = hb.prepare_geometry(xyz, ncn, ncon, cnt, xr)
     ctx = hb.Context(geom, case["depth"], rho=RHO, g=G, precision=prec, device=dev)
-    for s in range(steps):
-        ctx.solve_frequency(hb.wave_properties(omegas[s % len(omegas)], case["depth"], G), betas)
+    ctx.solve_batch([hb.wave_properties(omegas[s % len(omegas)], case["depth"], G) for s in range(steps)], betas)
     ctx.close()
     torch.cuda.synchronize()
     el = time.perf_counter() - t
@@ -314,7 +310,7 @@ def gpu_arm(args):
             "config": {"workload": WORKLOAD, "form": args.form, "panels": int(ncn.size),
                        "rhs_per_step": 6 * int(cnt.size) + len(betas),
                        "l2": "no flush: the 5400x5400 complex system (0.47 GB) and pair tables exceed the 126 MB L2",
-                       "parallelism": f"frequency shards x{ws}"},
+                       "parallelism": f"frequency shards x{ws}, {LANES} frequencies in flight per GPU"},
             "clocks": main["clocks"], "gpu_launches": main["launches"], "library_calls": main["lib_calls"],
             "e2e": {"value": ws * args.steps / e2e_s, "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h,

@@ -32,6 +32,7 @@
 #include <cstdio>
 #include <cstring>
 #include <mutex>
+#include <thread>
 #include <string>
 #include <vector>
 
@@ -417,15 +418,17 @@ template <class T>
 struct DBuf {
   T* p = nullptr;
   size_t n = 0;
+  bool own = true;  // false: a view of another context's buffer
   DBuf() = default;
   DBuf(const DBuf&) = delete;
   DBuf& operator=(const DBuf&) = delete;
   ~DBuf() { release(); }
   int alloc(size_t count) {
     if (count <= n && p) return 0;
-    if (p) cudaFree(p);
+    if (p && own) cudaFree(p);
     p = nullptr;
     n = 0;
+    own = true;
     if (count == 0) return 0;
     if (cudaMalloc(&p, count * sizeof(T)) != cudaSuccess) {
       p = nullptr;
@@ -434,10 +437,17 @@ struct DBuf {
     n = count;
     return 0;
   }
+  void view(const DBuf& o) {
+    release();
+    p = o.p;
+    n = o.n;
+    own = false;
+  }
   void release() {
-    if (p) cudaFree(p);
+    if (p && own) cudaFree(p);
     p = nullptr;
     n = 0;
+    own = true;
   }
 };
 
@@ -483,6 +493,10 @@ struct hams_ctx {
   std::atomic<long long> lib_calls{0};  // cuBLAS / cuSOLVER / CUB calls
   cudaEvent_t marks[8] = {};
   int refine_sweeps = 0;
+  // batch lanes: contexts that share this one's geometry and pair data (views)
+  // and own their stream, handles and per-frequency buffers
+  std::vector<hams_ctx*> lanes;
+  bool is_lane = false;
 };
 
 static int launch_check(hams_ctx* c, int count = 1) {
@@ -500,13 +514,17 @@ extern "C" const char* hams_last_error(void) { return g_err.c_str(); }
 extern "C" void hams_ctx_destroy(hams_ctx* c) {
   if (!c) return;
   cudaSetDevice(c->dev);
+  for (hams_ctx* l : c->lanes) hams_ctx_destroy(l);
+  c->lanes.clear();
   if (c->st) cudaStreamSynchronize(c->st);
   c->xq.release(); c->fxyz.release(); c->ds.release(); c->pnsz.release(); c->nrm.release(); c->vtx.release();
   c->ncn.release(); c->body.release(); c->bstart.release(); c->rs.release(); c->rd.release(); c->pairs.release();
   c->chunks.release(); c->chunk_body.release(); c->A.release(); c->S.release(); c->B.release(); c->part.release();
   c->wd.release(); c->C.release(); c->D.release(); c->X.release(); c->R.release(); c->Af.release(); c->Xf.release();
   c->wvn.release(); c->beta.release(); c->outbuf.release(); c->colratio.release(); c->ipiv.release();
-  c->info.release(); c->ovf.release(); c->work.release(); c->work32.release();
+  c->info.release(); c->ovf.release(); c->work.release(); c->work32.release(); c->luw.release(); c->perm.release();
+  c->mt_pm.release(); c->mt_ac.release(); c->mt_fld.release(); c->mt_fldt.release(); c->mt_src.release();
+  c->mt_srct.release();
   for (auto& e : c->ev)
     if (e) cudaEventDestroy(e);
   for (auto& e : c->evb)
@@ -519,6 +537,8 @@ extern "C" void hams_ctx_destroy(hams_ctx* c) {
   if (c->st) cudaStreamDestroy(c->st);
   delete c;
 }
+
+static int ctx_frequency_buffers(hams_ctx* c);
 
 static int ctx_setup(hams_ctx* c, const hams_geom* geo) {
   const int n = c->n, tn = c->tn, nb = c->nb;
@@ -606,6 +626,15 @@ static int ctx_setup(hams_ctx* c, const hams_geom* geo) {
   CU(cudaMemcpyAsync(c->chunks.p, c->chunks_h.data(), c->chunks_h.size() * sizeof(int2), cudaMemcpyHostToDevice, c->st));
   CU(cudaMemcpyAsync(c->chunk_body.p, cb.data(), cb.size() * sizeof(int), cudaMemcpyHostToDevice, c->st));
 
+  TRY(ctx_frequency_buffers(c));
+  CU(cudaStreamSynchronize(c->st));
+  return 0;
+}
+
+// Buffers of one frequency in flight: mode tables, A and S, roots, flags.
+static int ctx_frequency_buffers(hams_ctx* c) {
+  const int n = c->n, tn = c->tn;
+  size_t np = (size_t)tn * n;
   if (c->opts.depth >= 0.0) {
     const size_t km = hams::kModeMax;
     TRY(c->mt_pm.alloc(km)); TRY(c->mt_ac.alloc(km));
@@ -623,7 +652,55 @@ static int ctx_setup(hams_ctx* c, const hams_geom* geo) {
   TRY(c->ovf.alloc(1));
   TRY(c->ipiv.alloc(n));
   TRY(c->info.alloc(1));
-  CU(cudaStreamSynchronize(c->st));
+  return 0;
+}
+
+// Stream, library handles and events of a context, on its device.
+static int ctx_handles(hams_ctx* c) {
+  if (cudaSetDevice(c->dev) != cudaSuccess) return fail(HAMS_ERR_CUDA, "cudaSetDevice(%d) failed", c->dev);
+  if (cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking) != cudaSuccess)
+    return fail(HAMS_ERR_CUDA, "stream creation failed");
+  if (cublasCreate(&c->blas) != CUBLAS_STATUS_SUCCESS) return fail(HAMS_ERR_CUDA, "cublasCreate failed");
+  if (cusolverDnCreate(&c->solver) != CUSOLVER_STATUS_SUCCESS) return fail(HAMS_ERR_CUDA, "cusolverDnCreate failed");
+  cublasSetStream(c->blas, c->st);
+  cusolverDnSetStream(c->solver, c->st);
+  for (auto& e : c->ev) CU(cudaEventCreate(&e));
+  for (auto& e : c->evb) CU(cudaEventCreate(&e));
+  for (auto& e : c->marks) CU(cudaEventCreate(&e));
+  CU(cudaEventCreate(&c->evf));
+  return 0;
+}
+
+// A batch lane of c: its own stream, handles and per-frequency buffers; the
+// geometry, Rankine terms and pair lists are views of c's.
+static int make_lane(hams_ctx* c, hams_ctx** out) {
+  hams_ctx* l = new hams_ctx();
+  l->is_lane = true;
+  l->opts = c->opts;
+  l->dev = c->dev;
+  l->n = c->n;
+  l->nl = c->nl;
+  l->tn = c->tn;
+  l->nb = c->nb;
+  l->body_nelem = c->body_nelem;
+  int rc = ctx_handles(l);
+  if (!rc) {
+    l->xq.view(c->xq); l->fxyz.view(c->fxyz); l->ds.view(c->ds); l->pnsz.view(c->pnsz); l->nrm.view(c->nrm);
+    l->vtx.view(c->vtx); l->ncn.view(c->ncn); l->body.view(c->body); l->bstart.view(c->bstart);
+    l->rs.view(c->rs); l->rd.view(c->rd); l->pairs.view(c->pairs); l->chunks.view(c->chunks);
+    l->chunk_body.view(c->chunk_body);
+    l->g = c->g;
+    for (int b = 0; b < 5; ++b) l->bin_off[b] = c->bin_off[b];
+    l->chunks_h = c->chunks_h;
+    rc = ctx_frequency_buffers(l);
+  }
+  if (rc < 0) {
+    std::string keep = g_err;
+    hams_ctx_destroy(l);
+    g_err = keep;
+    return rc;
+  }
+  *out = l;
   return 0;
 }
 
@@ -647,21 +724,8 @@ extern "C" int hams_ctx_create(const hams_geom* geo, const hams_opts* opts, hams
   c->tn = c->n + c->nl;
   c->nb = geo->nbody;
   c->body_nelem.assign(geo->body_nelem, geo->body_nelem + geo->nbody);
-  int rc = 0;
-  if (cudaSetDevice(c->dev) != cudaSuccess) rc = fail(HAMS_ERR_CUDA, "cudaSetDevice(%d) failed", c->dev);
-  if (!rc && cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking) != cudaSuccess)
-    rc = fail(HAMS_ERR_CUDA, "stream creation failed");
-  if (!rc && cublasCreate(&c->blas) != CUBLAS_STATUS_SUCCESS) rc = fail(HAMS_ERR_CUDA, "cublasCreate failed");
-  if (!rc && cusolverDnCreate(&c->solver) != CUSOLVER_STATUS_SUCCESS) rc = fail(HAMS_ERR_CUDA, "cusolverDnCreate failed");
-  if (!rc) {
-    cublasSetStream(c->blas, c->st);
-    cusolverDnSetStream(c->solver, c->st);
-    for (auto& e : c->ev) cudaEventCreate(&e);
-    for (auto& e : c->evb) cudaEventCreate(&e);
-    for (auto& e : c->marks) cudaEventCreate(&e);
-    cudaEventCreate(&c->evf);
-    rc = ctx_setup(c, geo);
-  }
+  int rc = ctx_handles(c);
+  if (!rc) rc = ctx_setup(c, geo);
   if (rc < 0) {
     std::string keep = g_err;
     hams_ctx_destroy(c);
@@ -941,30 +1005,67 @@ extern "C" int hams_solve_frequency(hams_ctx* c, const hams_wave* w, int32_t nbe
   return solve_one(c, w, nbeta, beta, amas, bdmp, exfc);
 }
 
+// Frequencies in flight at once in hams_solve_batch when opts.batch_lanes is 0.
+constexpr int kDefaultLanes = 4;
+
 extern "C" int hams_solve_batch(hams_ctx* c, int32_t nfreq, const hams_wave* waves, int32_t nbeta, const double* beta,
                                 double* amas, double* bdmp, double* exfc) {
   g_err.clear();
   if (!c || !waves || nfreq < 0 || (nbeta > 0 && !beta)) return fail(HAMS_ERR_ARG, "null argument");
   if (cudaSetDevice(c->dev) != cudaSuccess) return fail(HAMS_ERR_CUDA, "cudaSetDevice failed");
+  if (nfreq == 0) return 0;
   const int ndof = 6 * c->nb;
-  std::vector<double> a((size_t)ndof * ndof), b((size_t)ndof * ndof), x(2 * (size_t)ndof * std::max(nbeta, 1));
-  int worst = 0;
-  for (int k = 0; k < nfreq; ++k) {
-    int rc = solve_one(c, &waves[k], nbeta, beta, a.data(), b.data(), x.data());
-    if (rc < 0) return rc;
-    if (rc > 0 && !worst) worst = rc;
-    // scatter into (nfreq, ...) column-major arrays with the frequency index leading
-    for (size_t e = 0; e < (size_t)ndof * ndof; ++e) {
-      if (amas) amas[k + e * nfreq] = a[e];
-      if (bdmp) bdmp[k + e * nfreq] = b[e];
-    }
-    if (exfc)
-      for (size_t e = 0; e < (size_t)ndof * nbeta; ++e) {
-        exfc[2 * (k + e * nfreq)] = x[2 * e];
-        exfc[2 * (k + e * nfreq) + 1] = x[2 * e + 1];
-      }
+  int L = c->opts.batch_lanes > 0 ? c->opts.batch_lanes : kDefaultLanes;
+  L = std::max(1, std::min(L, nfreq));
+  while ((int)c->lanes.size() < L - 1) {
+    hams_ctx* l = nullptr;
+    TRY(make_lane(c, &l));
+    c->lanes.push_back(l);
   }
-  return worst;
+  std::vector<hams_ctx*> lane{c};
+  for (int t = 0; t + 1 < L; ++t) lane.push_back(c->lanes[t]);
+  std::vector<int> rc_of(nfreq, 0), lane_rc(L, 0);
+  std::vector<std::string> lane_err(L);
+  // lane t solves frequencies t, t + L, ... on its own stream and host thread
+  auto run = [&](int t) {
+    if (cudaSetDevice(c->dev) != cudaSuccess) {
+      lane_rc[t] = HAMS_ERR_CUDA;
+      lane_err[t] = "cudaSetDevice failed";
+      return;
+    }
+    std::vector<double> a((size_t)ndof * ndof), b((size_t)ndof * ndof), x(2 * (size_t)ndof * std::max(nbeta, 1));
+    for (int k = t; k < nfreq; k += L) {
+      int rc = solve_one(lane[t], &waves[k], nbeta, beta, a.data(), b.data(), x.data());
+      if (rc < 0) {
+        lane_rc[t] = rc;
+        lane_err[t] = g_err;
+        return;
+      }
+      rc_of[k] = rc;
+      // scatter into (nfreq, ...) column-major arrays with the frequency index leading
+      for (size_t e = 0; e < (size_t)ndof * ndof; ++e) {
+        if (amas) amas[k + e * nfreq] = a[e];
+        if (bdmp) bdmp[k + e * nfreq] = b[e];
+      }
+      if (exfc)
+        for (size_t e = 0; e < (size_t)ndof * nbeta; ++e) {
+          exfc[2 * (k + e * nfreq)] = x[2 * e];
+          exfc[2 * (k + e * nfreq) + 1] = x[2 * e + 1];
+        }
+    }
+  };
+  std::vector<std::thread> th;
+  for (int t = 1; t < L; ++t) th.emplace_back(run, t);
+  run(0);
+  for (auto& x : th) x.join();
+  for (int t = 0; t < L; ++t)
+    if (lane_rc[t] < 0) {
+      g_err = lane_err[t];
+      return lane_rc[t];
+    }
+  for (int k = 0; k < nfreq; ++k)
+    if (rc_of[k] > 0) return rc_of[k];  // singular pivot of the first such frequency
+  return 0;
 }
 
 extern "C" int hams_assemble(hams_ctx* c, const hams_wave* w, int32_t nbeta, const double* beta, double* amat,
@@ -1098,9 +1199,19 @@ extern "C" int hams_last_timings(hams_ctx* c, double* ms, int32_t n) {
   return k;
 }
 
-extern "C" int64_t hams_launch_count(hams_ctx* c) { return c ? (int64_t)c->launches.load() : 0; }
+extern "C" int64_t hams_launch_count(hams_ctx* c) {
+  if (!c) return 0;
+  long long t = c->launches.load();
+  for (hams_ctx* l : c->lanes) t += l->launches.load();
+  return (int64_t)t;
+}
 
-extern "C" int64_t hams_library_call_count(hams_ctx* c) { return c ? (int64_t)c->lib_calls.load() : 0; }
+extern "C" int64_t hams_library_call_count(hams_ctx* c) {
+  if (!c) return 0;
+  long long t = c->lib_calls.load();
+  for (hams_ctx* l : c->lanes) t += l->lib_calls.load();
+  return (int64_t)t;
+}
 
 extern "C" int hams_mark(hams_ctx* c, int32_t slot) {
   if (!c || slot < 0 || slot >= 8) return fail(HAMS_ERR_ARG, "bad mark slot");

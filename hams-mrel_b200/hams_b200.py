@@ -36,7 +36,8 @@ class HamsGeom(ctypes.Structure):
 class HamsOpts(ctypes.Structure):
     _fields_ = [("depth", c_dbl), ("rho", c_dbl), ("g", c_dbl), ("xw", c_dbl * 2), ("amp", c_dbl), ("isol", c_int),
                 ("irsp", c_int), ("precision", c_int), ("device", c_int), ("refine_tol", c_dbl),
-                ("refine_max", c_int), ("lu_kind", c_int), ("reserved", c_int * 6)]
+                ("refine_max", c_int), ("lu_kind", c_int), ("batch_lanes", c_int),
+                ("reserved", c_int * 5)]
 
 
 class HamsWave(ctypes.Structure):
@@ -130,7 +131,8 @@ class Context:
     """
 
     def __init__(self, geom, depth, rho=1000.0, g=9.80665, isol=1, irsp=0, precision=PREC_FP64, device=0,
-                 xw=(0.0, 0.0), amp=1.0, refine_tol=0.0, refine_max=0, lu_kind=0):
+                 xw=(0.0, 0.0), amp=1.0, refine_tol=0.0, refine_max=0, lu_kind=0,
+                 batch_lanes=0):
         lib = load_library()
         self._keep = {}
         f = lambda k, dt: self._keep.setdefault(k, np.asfortranarray(geom[k], dtype=dt))
@@ -149,7 +151,7 @@ class Context:
             g_.ixyz_p = _d(ixyz_p)
         o = HamsOpts(depth=float(depth), rho=float(rho), g=float(g), amp=float(amp), isol=int(isol), irsp=int(irsp),
                      precision=int(precision), device=int(device), refine_tol=float(refine_tol),
-                     refine_max=int(refine_max), lu_kind=int(lu_kind))
+                     refine_max=int(refine_max), lu_kind=int(lu_kind), batch_lanes=int(batch_lanes))
         o.xw[0], o.xw[1] = xw
         self.depth, self.g = float(depth), float(g)
         self._h = ctypes.c_void_p()

@@ -87,7 +87,8 @@ typedef struct hams_opts {
   double refine_tol;/* mixed: relative residual target of the refinement (<=0: 1e-12) */
   int32_t refine_max;/* mixed: refinement sweeps (<=0: 30)                       */
   int32_t lu_kind;  /* mixed: HAMS_LU_BLOCK_EMU (0), HAMS_LU_BLOCK_TF32, HAMS_LU_LIBRARY */
-  int32_t reserved[6];
+  int32_t batch_lanes;/* hams_solve_batch: frequencies in flight (<=0: 4)          */
+  int32_t reserved[5];
 } hams_opts;
 
 /* One frequency after CalWaveProperts (ImplementSubs.f90:40): V = w^2/g
@@ -133,9 +134,13 @@ void hams_ctx_destroy(hams_ctx *ctx);
 int hams_solve_frequency(hams_ctx *ctx, const hams_wave *wave, int32_t nbeta, const double *beta_rad, double *amas,
                          double *bdmp, double *exfc);
 
-/* nfreq frequencies back to back, results stacked along a leading frequency
- * index: amas/bdmp (nfreq,6nb,6nb), exfc (nfreq,nbeta,6nb), column-major as
- * AMAS_MULTI_COMB / EXFC_MULTI_COMB. */
+/* nfreq frequencies, results stacked along a leading frequency index:
+ * amas/bdmp (nfreq,6nb,6nb), exfc (nfreq,nbeta,6nb), column-major as
+ * AMAS_MULTI_COMB / EXFC_MULTI_COMB.  opts.batch_lanes frequencies are in
+ * flight at once, each on its own stream and host thread with its own
+ * per-frequency buffers (about 1.3 GB per lane at 5,400 panels), sharing the
+ * context's geometry; lanes are created on first use and kept.  Returns the
+ * first error, or the singular-pivot index of the first frequency with one. */
 int hams_solve_batch(hams_ctx *ctx, int32_t nfreq, const hams_wave *waves, int32_t nbeta, const double *beta_rad,
                      double *amas, double *bdmp, double *exfc);
 
