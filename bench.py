@@ -35,6 +35,18 @@ METRIC = "freq-solves/s @5.4k panels: surrogate+mixed vs plain FP64 GPU @≤1e-4
 UNIT = "freq-solves/s"
 RHO, G = 1025.0, 9.81
 LANES = 4  # frequencies in flight in hams_solve_batch (the library's default)
+SG_FAR = 3.0  # surrogate pairs: centre distance beyond 3 source-panel sizes
+
+
+def _peaks():
+    try:
+        with open(os.path.join(REPO, "MEASURED_PEAKS.json")) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return {"bf16_tflops": 1590.0, "hbm_gbs": 6650.0}  # earlier measurement on this pool (fallback)
+
+
+PEAKS = _peaks()
 WORKLOAD = "3x3 cylinder array R=4 T=8 spacing 20 m, 5400 quad panels, depth 50 m, 40 freq 0.2-2.5 rad/s, " \
            "headings 0/30/60/90 deg (54 rad + 4 dif RHS)"
 
@@ -44,8 +56,10 @@ WORKLOAD = "3x3 cylinder array R=4 T=8 spacing 20 m, 5400 quad panels, depth 50 
 # its DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum).
 # Both belong to the kernel version they were captured from
 # (profiles/k_green_series_eigene_c2_array.md).
-EIGENE_FP64_FLOPS_PER_PAIR = 71716
-EIGENE_DRAM_BYTES_PER_LAUNCH = 10.19e9
+EIGENE_FP64_FLOPS_PER_PAIR = None
+EIGENE_DRAM_BYTES_PER_LAUNCH = None
+# DRAM bytes of one launch of the surrogate kernel on this workload (ncu), or None
+SG_DRAM_BYTES_PER_LAUNCH = None
 
 
 def build_case():
@@ -205,10 +219,12 @@ def rel(a, b):
     return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
 
 
-def run_form(hb, dev, geom, case, prec, omegas, betas, warmup, steps, barrier, want_results, sampler=None):
+def run_form(hb, dev, geom, case, prec, omegas, betas, warmup, steps, barrier, want_results, sampler=None, sg=None):
     """K frequencies through hams_solve_batch (frequencies in flight on several streams), timed
     between two events on the context's stream."""
     ctx = hb.Context(geom, case["depth"], rho=RHO, g=G, precision=prec, device=dev)
+    if sg is not None:
+        ctx.set_surrogate(sg, SG_FAR)
     waves = [hb.wave_properties(om, case["depth"], G) for om in omegas]
     if warmup:  # at least one frequency per lane, so that no lane is created inside the timed region
         ctx.solve_batch([waves[s % len(waves)] for s in range(max(warmup, LANES))], betas)
@@ -226,11 +242,10 @@ def run_form(hb, dev, geom, case, prec, omegas, betas, warmup, steps, barrier, w
     barrier()
     ctx.close()
     results = [tuple(r[k] for r in res) for k in range(steps)] if (want_results and res is not None) else []
-    return dict(ms=ms, launches=launches, lib_calls=libcalls, eig_ms=[tm["green_eigene"]], eig_pairs=tm["pairs_eigene"],
-                results=results, clocks=clocks, sweeps=[tm["refine_sweeps"]])
+    return dict(ms=ms, launches=launches, lib_calls=libcalls, timings=tm, results=results, clocks=clocks)
 
 
-def e2e_form(hb, dev, case, xyz, ncn, ncon, cnt, xr, prec, omegas, betas, steps, barrier):
+def e2e_form(hb, dev, case, xyz, ncn, ncon, cnt, xr, prec, omegas, betas, steps, barrier, sg=None):
     """Deck through the C ABI from host buffers: geometry, context, K frequencies."""
     import torch
 
@@ -239,6 +254,8 @@ def e2e_form(hb, dev, case, xyz, ncn, ncon, cnt, xr, prec, omegas, betas, steps,
     t = time.perf_counter()
     geom = hb.prepare_geometry(xyz, ncn, ncon, cnt, xr)
     ctx = hb.Context(geom, case["depth"], rho=RHO, g=G, precision=prec, device=dev)
+    if sg is not None:
+        ctx.set_surrogate(sg, SG_FAR)
     ctx.solve_batch([hb.wave_properties(omegas[s % len(omegas)], case["depth"], G) for s in range(steps)], betas)
     ctx.close()
     torch.cuda.synchronize()
@@ -246,9 +263,16 @@ def e2e_form(hb, dev, case, xyz, ncn, ncon, cnt, xr, prec, omegas, betas, steps,
     n, nb, ndof = ncn.size, cnt.size, 6 * cnt.size
     geom_bytes = xyz.nbytes + ncn.astype(np.int32).nbytes + 4 * 4 * n + 8 * (3 + 1 + 1 + 6) * n + 4 * nb
     wave_bytes = 8 * 205 + 8 * len(betas)
-    h2d = geom_bytes / steps + wave_bytes
+    sg_bytes = 4 * hb.surrogate_param_count() if sg is not None else 0
+    h2d = (geom_bytes + sg_bytes) / steps + wave_bytes
     d2h = 8 * 2 * ndof * ndof + 16 * len(betas) * ndof
     return el, int(round(h2d)), int(d2h)
+
+
+# forms: precision, surrogate on, dtype
+FORMS = {"surrogate": ("mixed", True, "f64 near + f16/f32 MLP far, c64 LU + f64 refinement"),
+         "mixed": ("mixed", False, "f64, c64 LU + f64 refinement"),
+         "fp64": ("fp64", False, "f64")}
 
 
 def gpu_arm(args):
@@ -276,6 +300,7 @@ def gpu_arm(args):
         return float(t.item())
 
     import hams_b200 as hb
+    import train_surrogate
 
     case, xyz, ncn, ncon, cnt, xr = build_case()
     geom = hb.prepare_geometry(xyz, ncn, ncon, cnt, xr)
@@ -284,55 +309,84 @@ def gpu_arm(args):
     # weak scaling: rank r takes frequencies r*K, r*K+1, ... of the repeated sweep
     om_rank = np.array([allom[(rank * args.steps + s) % len(allom)] for s in range(args.steps)])
     om_warm = np.array([allom[(s * 7 + 3) % len(allom)] for s in range(args.warmup)])
-    prec_main = hb.PREC_MIXED if args.form == "mixed" else hb.PREC_FP64
-    want_cmp = args.form == "mixed"
+    sgp = train_surrogate.load()
+    prec = {"mixed": hb.PREC_MIXED, "fp64": hb.PREC_FP64}
+
+    def form_args(name):
+        pr, on, _ = FORMS[name]
+        return prec[pr], (sgp if on else None)
 
     sampler = ClockSampler(local)
-    main = run_form(hb, local, geom, case, prec_main, np.concatenate([om_warm, om_rank]), betas, args.warmup, 0,
-                    barrier, False)  # warm the library and caches on this deck
-    main = run_form(hb, local, geom, case, prec_main, om_rank, betas, args.warmup, args.steps, barrier, want_cmp, sampler)
-    fp64 = None
-    if want_cmp:
-        fp64 = run_form(hb, local, geom, case, hb.PREC_FP64, om_rank, betas, args.warmup, args.steps, barrier, True)
+    p_main, sg_main = form_args(args.form)
+    run_form(hb, local, geom, case, p_main, np.concatenate([om_warm, om_rank]), betas, args.warmup, 0, barrier,
+             False, sg=sg_main)  # warm the library and caches on this deck
+    runs = {args.form: run_form(hb, local, geom, case, p_main, om_rank, betas, args.warmup, args.steps, barrier, True,
+                                sampler, sg=sg_main)}
+    for other in FORMS:
+        if other != args.form and not args.only_form:
+            pr, sg = form_args(other)
+            runs[other] = run_form(hb, local, geom, case, pr, om_rank, betas, args.warmup, args.steps, barrier, True,
+                                   sg=sg)
+    main = runs[args.form]
     ms = max_over_ranks(main["ms"])
-    ms_fp64 = max_over_ranks(fp64["ms"]) if fp64 else None
-    err = None
-    if fp64:
-        e = [max(rel(a[0], b[0]), rel(a[1], b[1]), rel(a[2], b[2])) for a, b in zip(main["results"], fp64["results"])]
-        err = max_over_ranks(max(e))
-    e2e_s, h2d, d2h = e2e_form(hb, local, case, xyz, ncn, ncon, cnt, xr, prec_main, om_rank, betas, args.steps, barrier)
+    forms = {}
+    for name, r in runs.items():
+        v = ws * args.steps / (max_over_ranks(r["ms"]) * 1e-3)
+        err = None
+        if "fp64" in runs and name != "fp64":
+            e = [max(rel(a[0], b[0]), rel(a[1], b[1]), rel(a[2], b[2])) for a, b in
+                 zip(r["results"], runs["fp64"]["results"])]
+            err = max_over_ranks(max(e))
+            med = float(np.median(e))
+        forms[name] = {"value": v, "rel_err_vs_fp64": err}
+        if err is not None:
+            forms[name]["rel_err_median"] = med
+    e2e_s, h2d, d2h = e2e_form(hb, local, case, xyz, ncn, ncon, cnt, xr, p_main, om_rank, betas, args.steps,
+                               barrier, sg=sg_main)
     e2e_s = max_over_ranks(e2e_s)
 
     value = ws * args.steps / (ms * 1e-3)
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64+c64-lu" if args.form == "mixed" else "f64", "data": "synthetic",
+            "vs_baseline": None, "dtype": FORMS[args.form][2], "data": "synthetic",
             "config": {"workload": WORKLOAD, "form": args.form, "panels": int(ncn.size),
                        "rhs_per_step": 6 * int(cnt.size) + len(betas),
                        "l2": "no flush: the 5400x5400 complex system (0.47 GB) and pair tables exceed the 126 MB L2",
-                       "parallelism": f"frequency shards x{ws}, {LANES} frequencies in flight per GPU"},
+                       "parallelism": f"frequency shards x{ws}, {LANES} frequencies in flight per GPU",
+                       "surrogate": f"far pairs beyond {SG_FAR} panel sizes" if sg_main is not None else None},
             "clocks": main["clocks"], "gpu_launches": main["launches"], "library_calls": main["lib_calls"],
             "e2e": {"value": ws * args.steps / e2e_s, "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h,
-                    "includes": "host geometry prep, context set-up (upload, Rankine tables, pair sort) and K "
-                                "frequency solves through the C ABI from host buffers"}}
-    if fp64:
-        line["fp64_value"] = ws * args.steps / (ms_fp64 * 1e-3)
-        line["rel_err_vs_fp64"] = err
-        line["refine_sweeps_mean"] = float(np.mean(main["sweeps"]))
-    # roofline of the dominant kernel: the EIGENE-branch series Green kernel
-    eig_ms = float(np.mean(main["eig_ms"]))
-    peak = hb.measure_fp64_peak(local) if rank == 0 else None
-    roof = {"kernel": "k_green_series<EIGENE>", "bound": "fp64", "unit": "TFLOP/s", "launch_ms": eig_ms,
-            "pairs_per_launch": main["eig_pairs"], "peak": peak,
-            "peak_source": "measured in this run: FP64 FMA loop on all SMs (no FP64 figure in MEASURED_PEAKS.json)",
-            "achieved": None, "frac": None, "traffic": None}
-    if EIGENE_FP64_FLOPS_PER_PAIR and peak:
-        ach = EIGENE_FP64_FLOPS_PER_PAIR * main["eig_pairs"] / (eig_ms * 1e-3) / 1e12
-        roof.update(achieved=ach, frac=ach / peak, flops_per_pair=EIGENE_FP64_FLOPS_PER_PAIR)
-    if EIGENE_DRAM_BYTES_PER_LAUNCH:
-        roof["traffic"] = EIGENE_DRAM_BYTES_PER_LAUNCH
-    line["roofline"] = roof
+                    "includes": "host geometry prep, context set-up (upload, Rankine tables, pair sort, surrogate "
+                                "upload) and K frequency solves through the C ABI from host buffers"},
+            "forms": forms}
+    if "fp64" in forms and args.form != "fp64":
+        line["speedup_vs_fp64"] = value / forms["fp64"]["value"]
+        line["rel_err_vs_fp64"] = forms[args.form]["rel_err_vs_fp64"]
+    tm = main["timings"]
+    if sg_main is not None and tm["pairs_surrogate"] > 0:
+        # dominant kernel: the surrogate (tensor cores: 3 hidden layers and the padded output layer)
+        flops = 2.0 * (3 * 128 * 128 + 128 * 8)
+        ach = flops * tm["pairs_surrogate"] / (tm["green_surrogate"] * 1e-3) / 1e12
+        peak = PEAKS.get("bf16_tflops")
+        line["roofline"] = {"kernel": "k_green_sg", "bound": "tensor", "unit": "TFLOP/s", "achieved": ach,
+                            "peak": peak, "frac": ach / peak if peak else None, "traffic": SG_DRAM_BYTES_PER_LAUNCH,
+                            "peak_source": "of measured: dense bf16 cuBLAS burst (MEASURED_PEAKS.json); the kernel "
+                                           "runs FP16 mma.sync",
+                            "launch_ms": tm["green_surrogate"], "pairs_per_launch": tm["pairs_surrogate"],
+                            "flops_per_pair": flops}
+    else:
+        eig_ms = tm["green_eigene"]
+        peak = hb.measure_fp64_peak(local) if rank == 0 else None
+        roof = {"kernel": "k_green_series<EIGENE>", "bound": "fp64", "unit": "TFLOP/s", "launch_ms": eig_ms,
+                "pairs_per_launch": tm["pairs_eigene"], "peak": peak,
+                "peak_source": "measured in this run: FP64 FMA loop on all SMs (no FP64 figure in "
+                               "MEASURED_PEAKS.json)", "achieved": None, "frac": None,
+                "traffic": EIGENE_DRAM_BYTES_PER_LAUNCH}
+        if EIGENE_FP64_FLOPS_PER_PAIR and peak and eig_ms > 0:
+            ach = EIGENE_FP64_FLOPS_PER_PAIR * tm["pairs_eigene"] / (eig_ms * 1e-3) / 1e12
+            roof.update(achieved=ach, frac=ach / peak, flops_per_pair=EIGENE_FP64_FLOPS_PER_PAIR)
+        line["roofline"] = roof
     if rank == 0 and ws == 1 and not args.no_cpu:
         sec, cores, sample, parts = cpu_sample_time(case, xyz, ncn, ncon, cnt, xr, float(allom[len(allom) // 2]),
                                                     target_s=args.cpu_seconds or 8.0)
@@ -351,7 +405,8 @@ def main():
     ap.add_argument("--steps", type=int, default=40)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
-    ap.add_argument("--form", choices=["mixed", "fp64"], default="mixed")
+    ap.add_argument("--form", choices=list(FORMS), default="surrogate")
+    ap.add_argument("--only-form", action="store_true", help="time only --form (no fp64 / other forms beside it)")
     ap.add_argument("--cpu-seconds", type=float, default=None,
                     help="CPU work per baseline sample (default 8 s; 3 s per step of --impl reference)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")

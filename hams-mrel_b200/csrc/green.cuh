@@ -629,6 +629,8 @@ __host__ __device__ __forceinline__ int fin_terms(double rr, double h) {
 template <int BR, class SC>
 __device__ inline grn4 fingreen3d(double xq, double xp, double yq, double yp, double zq, double zp, double v,
                                   const double* __restrict__ wvn, double h, int flag, SC* sc, int* overflow);
+__device__ inline grn4 finish_green(cplx fg[3], double xpq, double ypq, double zq, double zp, double rr, double r,
+                                    double r1, int flag);
 template <int BR, class MD, class SC>
 __device__ inline grn4 fingreen3d(double xq, double xp, double yq, double yp, double zq, double zp, double v,
                                   const double* __restrict__ wvn, double h, int flag, SC* sc, int* overflow,
@@ -636,13 +638,22 @@ __device__ inline grn4 fingreen3d(double xq, double xp, double yq, double yp, do
   double xpq = xq - xp, ypq = yq - yp, zpq = zq + zp;
   double rr = sqrt(xpq * xpq + ypq * ypq);
   double r = sqrt(rr * rr + (zp - zq) * (zp - zq)), r1 = sqrt(rr * rr + zpq * zpq);
-  grn4 o;
   cplx fg[3];
   double wk = wvn[0];
   if constexpr (BR == kLinton) linton(rr, zq, zp, v, wk, wvn, h, fg, overflow);
   else if constexpr (BR == kPidcock) pidcock(rr, zq, zp, v, wk, wvn, h, fg, *sc, md, overflow);
   else if constexpr (BR == kEigenE) eigene(rr, zq, zp, wk, wvn, h, fg, *sc, md, overflow);
   else eigen(rr, zq, zp, wk, wvn, h, fg, md);
+  return finish_green(fg, xpq, ypq, zq, zp, rr, r, r1, flag);
+}
+
+// The tail of FINGREEN3D (FinGreen3D.f90:124-150): the wave part fg (G and
+// its R and zq derivatives) projected on x and y, plus 1/r1 (and 1/r for far
+// pairs) and their gradients.
+__device__ inline grn4 finish_green(cplx fg[3], double xpq, double ypq, double zq, double zp, double rr, double r,
+                                    double r1, int flag) {
+  grn4 o;
+  double zpq = zq + zp;
   if (rr == 0.0) fg[1] = cmk(0.0, 0.0);
   o.g[0] = fg[0];
   o.g[3] = fg[2];

@@ -84,6 +84,8 @@ static int fail(int code, const char* fmt, ...) {
 
 #include "kernels.cuh"
 #include "lu_mixed.h"
+#include "green_sg.h"
+#include "surrogate.h"
 
 // ---------------------------------------------------------------------------
 // setup kernels
@@ -118,7 +120,11 @@ __global__ void k_rankine(DevGeom g, double* __restrict__ rs, double* __restrict
 }
 
 // Sort key of a pair: branch (2 bits) and epsilon-table length (8 bits).
-__global__ void k_pair_keys(DevGeom g, double h, uint32_t* __restrict__ keys, uint32_t* __restrict__ idx) {
+// Sort key of a pair: branch << 8 | series length.  With the surrogate on,
+// EIGENE / EIGEN pairs farther apart than far x the source panel's size and
+// inside the network's domain go to bins 4 (EIGENE) and 5 (EIGEN).
+__global__ void k_pair_keys(DevGeom g, double h, int sg_on, double far, uint32_t* __restrict__ keys,
+                            uint32_t* __restrict__ idx) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   int j = blockIdx.y;
   if (i >= g.tn) return;
@@ -127,6 +133,11 @@ __global__ void k_pair_keys(DevGeom g, double h, uint32_t* __restrict__ keys, ui
   double rr = sqrt(dx * dx + dy * dy);
   int b = hams::fin_branch(rr, h);
   int nt = hams::fin_terms(rr, h);
+  if (sg_on && (b == hams::kEigenE || b == hams::kEigen)) {
+    double zq = g.xq[j + 2 * g.n], zp = g.fxyz[i + 2 * g.tn], dz = zq - zp;
+    bool far_pair = sqrt(dx * dx + dy * dy + dz * dz) > far * g.pnsz[j];
+    if (far_pair && sg::in_domain(rr / h, (zq + h) / h, (zp + h) / h, sg::kKmin)) b = b == hams::kEigenE ? 4 : 5;
+  }
   keys[p] = (uint32_t)(b << 8) | (uint32_t)(nt & 0xff);
   idx[p] = (uint32_t)p;
 }
@@ -414,6 +425,7 @@ __global__ void k_colnorm_ratio(const double2* __restrict__ r, const double2* __
 // ---------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------
+constexpr int kBins = 6;
 template <class T>
 struct DBuf {
   T* p = nullptr;
@@ -466,7 +478,9 @@ struct hams_ctx {
   // frequency-independent pair data
   DBuf<double> rs, rd;
   DBuf<uint32_t> pairs;
-  long long bin_off[5] = {0, 0, 0, 0, 0};  // [branch] start offsets into pairs, bin_off[4] = total
+  // start offsets into pairs of bins 0-3 (branches LINTON, PIDCOCK, EIGENE,
+  // EIGEN), 4-5 (surrogate pairs of EIGENE, EIGEN); bin_off[6] = total
+  long long bin_off[kBins + 1] = {};
   // chunks of source panels for the RHS reduction
   std::vector<int2> chunks_h;
   DBuf<int2> chunks;
@@ -485,9 +499,9 @@ struct hams_ctx {
   DBuf<char> work32;
   // timing: ev[0..5] stage marks, evb[0..4] branch marks, evf after the factorisation
   cudaEvent_t ev[6] = {};
-  cudaEvent_t evb[5] = {};
+  cudaEvent_t evb[6] = {};
   cudaEvent_t evf = nullptr;
-  static constexpr int kTimings = 16;
+  static constexpr int kTimings = 18;
   double last_ms[kTimings] = {};
   std::atomic<long long> launches{0};   // kernels of this library
   std::atomic<long long> lib_calls{0};  // cuBLAS / cuSOLVER / CUB calls
@@ -497,6 +511,14 @@ struct hams_ctx {
   // and own their stream, handles and per-frequency buffers
   std::vector<hams_ctx*> lanes;
   bool is_lane = false;
+  // MLP surrogate of far-field pairs (hams_ctx_set_surrogate)
+  int sg_on = 0;
+  double sg_far = 3.0;
+  DBuf<uint16_t> sg_wh;
+  DBuf<float> sg_w0, sg_bias;
+  SgDev sgd{};
+  int sms = 148;
+  int sg_used = 0;  // the last solve evaluated its far pairs with the surrogate
 };
 
 static int launch_check(hams_ctx* c, int count = 1) {
@@ -510,6 +532,9 @@ extern "C" int hams_wave_properties(int32_t inft, double value, double depth, do
                                     hams_wave* o);
 
 extern "C" const char* hams_last_error(void) { return g_err.c_str(); }
+
+// error reporting for the other translation units of the library
+int hams_set_error(int code, const char* msg) { return fail(code, "%s", msg); }
 
 extern "C" void hams_ctx_destroy(hams_ctx* c) {
   if (!c) return;
@@ -539,6 +564,32 @@ extern "C" void hams_ctx_destroy(hams_ctx* c) {
 }
 
 static int ctx_frequency_buffers(hams_ctx* c);
+
+// Sorted pair list and bin offsets (finite depth); rebuilt when the surrogate
+// is switched on or off.
+static int build_pairs(hams_ctx* c) {
+  const int n = c->n, tn = c->tn;
+  size_t np = (size_t)tn * n;
+  if (np > 0xffffffffull) return fail(HAMS_ERR_UNSUPPORTED, "%zu pairs exceed the 32-bit pair index", np);
+  DBuf<uint32_t> keys, keys2, idx;
+  TRY(keys.alloc(np)); TRY(keys2.alloc(np)); TRY(idx.alloc(np)); TRY(c->pairs.alloc(np));
+  dim3 grid2((tn + 127) / 128, n);
+  k_pair_keys<<<grid2, 128, 0, c->st>>>(c->g, c->opts.depth, c->sg_on, c->sg_far, keys.p, idx.p);
+  TRY(launch_check(c));
+  size_t tmp = 0;
+  cub::DeviceRadixSort::SortPairs(nullptr, tmp, keys.p, keys2.p, idx.p, c->pairs.p, np, 0, 11, c->st);
+  DBuf<char> tbuf;
+  TRY(tbuf.alloc(tmp));
+  CU(cub::DeviceRadixSort::SortPairs(tbuf.p, tmp, keys.p, keys2.p, idx.p, c->pairs.p, np, 0, 11, c->st));
+  c->lib_calls += 1;
+  // bin boundaries: first index of each bin in the sorted keys
+  std::vector<uint32_t> hk(np);
+  CU(cudaMemcpyAsync(hk.data(), keys2.p, np * 4, cudaMemcpyDeviceToHost, c->st));
+  CU(cudaStreamSynchronize(c->st));
+  for (int b = 0; b <= kBins; ++b)
+    c->bin_off[b] = std::lower_bound(hk.begin(), hk.end(), (uint32_t)(b << 8), [](uint32_t a, uint32_t v) { return a < v; }) - hk.begin();
+  return 0;
+}
 
 static int ctx_setup(hams_ctx* c, const hams_geom* geo) {
   const int n = c->n, tn = c->tn, nb = c->nb;
@@ -592,26 +643,7 @@ static int ctx_setup(hams_ctx* c, const hams_geom* geo) {
   TRY(launch_check(c));
 
   // branch-sorted pair list (finite depth)
-  if (c->opts.depth >= 0.0) {
-    if (np > 0xffffffffull) return fail(HAMS_ERR_UNSUPPORTED, "%zu pairs exceed the 32-bit pair index", np);
-    DBuf<uint32_t> keys, keys2, idx;
-    TRY(keys.alloc(np)); TRY(keys2.alloc(np)); TRY(idx.alloc(np)); TRY(c->pairs.alloc(np));
-    k_pair_keys<<<grid2, 128, 0, c->st>>>(c->g, c->opts.depth, keys.p, idx.p);
-    TRY(launch_check(c));
-    size_t tmp = 0;
-    cub::DeviceRadixSort::SortPairs(nullptr, tmp, keys.p, keys2.p, idx.p, c->pairs.p, np, 0, 10, c->st);
-    DBuf<char> tbuf;
-    TRY(tbuf.alloc(tmp));
-    CU(cub::DeviceRadixSort::SortPairs(tbuf.p, tmp, keys.p, keys2.p, idx.p, c->pairs.p, np, 0, 10, c->st));
-    c->lib_calls += 1;
-    // bin boundaries: first index of each branch in the sorted keys
-    std::vector<uint32_t> hk(np);
-    CU(cudaMemcpyAsync(hk.data(), keys2.p, np * 4, cudaMemcpyDeviceToHost, c->st));
-    CU(cudaStreamSynchronize(c->st));
-    for (int b = 0; b <= 4; ++b)
-      c->bin_off[b] = std::lower_bound(hk.begin(), hk.end(), (uint32_t)(b << 8), [](uint32_t a, uint32_t v) { return a < v; }) - hk.begin();
-    keys.release(); keys2.release(); idx.release(); tbuf.release();
-  }
+  if (c->opts.depth >= 0.0) TRY(build_pairs(c));
 
   // chunks of source panels for the RHS reduction
   c->chunks_h.clear();
@@ -642,7 +674,7 @@ static int ctx_frequency_buffers(hams_ctx* c) {
     TRY(c->mt_fld.alloc(km * tn)); TRY(c->mt_fldt.alloc(km * tn));
     // modes needed by the longest series present: PIDCOCK 99, EIGENE 50, EIGEN 10
     int nmode = 11;
-    if (c->bin_off[3] > c->bin_off[2]) nmode = hams::kEigenEMax + 1;
+    if (c->bin_off[3] > c->bin_off[2] || c->bin_off[5] > c->bin_off[4]) nmode = hams::kEigenEMax + 1;
     if (c->bin_off[2] > c->bin_off[1]) nmode = hams::kPidcockMax + 1;
     c->mt = hams::ModeTab{n, tn, nmode, c->mt_pm.p, c->mt_ac.p, c->mt_src.p, c->mt_srct.p, c->mt_fld.p, c->mt_fldt.p};
   }
@@ -664,6 +696,7 @@ static int ctx_handles(hams_ctx* c) {
   if (cusolverDnCreate(&c->solver) != CUSOLVER_STATUS_SUCCESS) return fail(HAMS_ERR_CUDA, "cusolverDnCreate failed");
   cublasSetStream(c->blas, c->st);
   cusolverDnSetStream(c->solver, c->st);
+  cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, c->dev);
   for (auto& e : c->ev) CU(cudaEventCreate(&e));
   for (auto& e : c->evb) CU(cudaEventCreate(&e));
   for (auto& e : c->marks) CU(cudaEventCreate(&e));
@@ -690,7 +723,11 @@ static int make_lane(hams_ctx* c, hams_ctx** out) {
     l->rs.view(c->rs); l->rd.view(c->rd); l->pairs.view(c->pairs); l->chunks.view(c->chunks);
     l->chunk_body.view(c->chunk_body);
     l->g = c->g;
-    for (int b = 0; b < 5; ++b) l->bin_off[b] = c->bin_off[b];
+    for (int b = 0; b <= kBins; ++b) l->bin_off[b] = c->bin_off[b];
+    l->sg_on = c->sg_on;
+    l->sg_far = c->sg_far;
+    l->sgd = c->sgd;
+    l->sms = c->sms;
     l->chunks_h = c->chunks_h;
     rc = ctx_frequency_buffers(l);
   }
@@ -780,6 +817,30 @@ static int assemble_dev(hams_ctx* c, const hams_wave* w, int nbeta) {
       TRY(launch_check(c));
     }
     CU(cudaEventRecord(c->evb[4], c->st));
+    // far pairs: the surrogate, or the series when this frequency is outside its domain
+    const long long cs = c->bin_off[6] - c->bin_off[4];
+    const double hh = c->opts.depth, K = wd.wk * hh * tanh(wd.wk * hh);
+    if (cs > 0) {
+      if (!wd.limit && K >= sg::kKmin && K <= sg::kKmax) {
+        if (launch_green_sg(c->st, c->sms, c->g, wd, c->sgd, K, c->pairs.p + c->bin_off[4], cs, c->rs.p, c->rd.p,
+                            c->A.p, c->S.p))
+          return fail(HAMS_ERR_CUDA, "surrogate kernel launch failed");
+        c->launches += 1;
+        c->sg_used = 1;
+      } else {
+        long long ce = c->bin_off[5] - c->bin_off[4], cg = c->bin_off[6] - c->bin_off[5];
+        if (ce > 0)
+          launch_green_series(hams::kEigenE, (unsigned)((ce + 127) / 128), c->st, c->g, wd, c->wvn.p, c->mt,
+                              c->pairs.p + c->bin_off[4], ce, c->rs.p, c->rd.p, c->A.p, c->S.p, c->ovf.p);
+        if (cg > 0)
+          k_green_fin<3><<<(unsigned)((cg + 127) / 128), 128, 0, c->st>>>(c->g, wd, c->wvn.p, c->mt,
+                                                                          c->pairs.p + c->bin_off[5], cg, c->rs.p,
+                                                                          c->rd.p, c->A.p, c->S.p, c->ovf.p);
+        TRY(launch_check(c, (ce > 0) + (cg > 0)));
+        c->sg_used = 0;
+      }
+    }
+    CU(cudaEventRecord(c->evb[5], c->st));
   }
   CU(cudaEventRecord(c->ev[1], c->st));
   // right-hand sides
@@ -992,6 +1053,9 @@ static int solve_one(hams_ctx* c, const hams_wave* w, int nbeta, const double* b
   if (cudaEventElapsedTime(&ms, c->ev[2], c->evf) == cudaSuccess) c->last_ms[9] = ms;
   c->last_ms[10] = c->opts.precision == HAMS_PREC_MIXED ? (double)c->refine_sweeps : 0.0;
   c->last_ms[15] = c->opts.precision == HAMS_PREC_MIXED ? (double)c->lu_used : -1.0;
+  c->last_ms[16] = 0.0;
+  if (c->opts.depth >= 0.0 && cudaEventElapsedTime(&ms, c->evb[4], c->evb[5]) == cudaSuccess) c->last_ms[16] = ms;
+  c->last_ms[17] = c->sg_used ? (double)(c->bin_off[6] - c->bin_off[4]) : 0.0;
   if (ovf) return fail(HAMS_ERR_NUMERIC, "adaptive quadrature stack overflow in the LINTON branch");
   if (info > 0) return info;  // singular pivot, LAPACK style
   return 0;
@@ -1189,6 +1253,53 @@ extern "C" int hams_eval_green_static(hams_ctx* c, const hams_wave* w, int32_t n
   CU(cudaMemcpyAsync(&ovf, dovf, sizeof(int), cudaMemcpyDeviceToHost, c->st));
   CU(cudaStreamSynchronize(c->st));
   if (ovf) return fail(HAMS_ERR_NUMERIC, "adaptive quadrature stack overflow in the LINTON branch");
+  return 0;
+}
+
+extern "C" int hams_ctx_set_surrogate(hams_ctx* c, const float* params, int32_t nparams, double far_factor) {
+  g_err.clear();
+  if (!c || c->is_lane) return fail(HAMS_ERR_ARG, "null context");
+  if (params && nparams != sg::kParams)
+    return fail(HAMS_ERR_ARG, "surrogate parameter vector has %d floats, %d expected", nparams, sg::kParams);
+  if (params && !(far_factor > 0.0)) return fail(HAMS_ERR_ARG, "far_factor must be positive");
+  if (c->opts.depth < 0.0 && params) return fail(HAMS_ERR_UNSUPPORTED, "the surrogate covers finite depth only");
+  if (cudaSetDevice(c->dev) != cudaSuccess) return fail(HAMS_ERR_CUDA, "cudaSetDevice failed");
+  for (hams_ctx* l : c->lanes) CU(cudaStreamSynchronize(l->st));
+  CU(cudaStreamSynchronize(c->st));
+  if (params) {
+    std::vector<__half> wh;
+    std::vector<float> w0, bias;
+    pack_surrogate(params, wh, w0, bias);
+    TRY(c->sg_wh.alloc(wh.size()));
+    TRY(c->sg_w0.alloc(w0.size()));
+    TRY(c->sg_bias.alloc(bias.size()));
+    CU(cudaMemcpy(c->sg_wh.p, wh.data(), wh.size() * 2, cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(c->sg_w0.p, w0.data(), w0.size() * 4, cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(c->sg_bias.p, bias.data(), bias.size() * 4, cudaMemcpyHostToDevice));
+    c->sgd.wh = reinterpret_cast<const __half*>(c->sg_wh.p);
+    c->sgd.w0 = c->sg_w0.p;
+    c->sgd.bias = c->sg_bias.p;
+    for (int k = 0; k < sg::kOut; ++k) {
+      c->sgd.mean[k] = params[sg::kNormOff + k];
+      c->sgd.scale[k] = params[sg::kNormOff + sg::kOut + k];
+    }
+    c->sg_on = 1;
+    c->sg_far = far_factor;
+  } else {
+    c->sg_on = 0;
+  }
+  TRY(build_pairs(c));
+  int nmode = c->mt.nmode;
+  if (c->bin_off[3] > c->bin_off[2] || c->bin_off[5] > c->bin_off[4]) nmode = std::max(nmode, hams::kEigenEMax + 1);
+  c->mt.nmode = nmode;
+  for (hams_ctx* l : c->lanes) {
+    for (int b = 0; b <= kBins; ++b) l->bin_off[b] = c->bin_off[b];
+    l->pairs.view(c->pairs);
+    l->sg_on = c->sg_on;
+    l->sg_far = c->sg_far;
+    l->sgd = c->sgd;
+    l->mt.nmode = nmode;
+  }
   return 0;
 }
 

@@ -12,11 +12,13 @@
 
 #include "../../include/hams_gpu.h"
 
+#include "host_wave.h"
+
 namespace {
-
 constexpr double kPi = 3.141592653589793;
+}  // namespace
 
-void dispersion(double* wvn, int nrt, double w, double h) {
+void hams_dispersion(double* wvn, int nrt, double w, double h) {
   const double g = 9.807;
   double x = w * w * h / g, y, t;
   if (x > 0.0 && x <= 2.0) {
@@ -56,8 +58,6 @@ void dispersion(double* wvn, int nrt, double w, double h) {
   }
 }
 
-}  // namespace
-
 extern "C" int hams_wave_properties(int32_t inft, double value, double depth, double g, int32_t sybo_kk,
                                     hams_wave* o) {
   if (!o) return HAMS_ERR_ARG;
@@ -78,7 +78,7 @@ extern "C" int hams_wave_properties(int32_t inft, double value, double depth, do
       o->v = value;
       o->w1 = std::sqrt(g * o->v);
       if (deep) o->wk = o->v;
-      else { dispersion(o->wvn, HAMS_NK, o->w1, depth); o->wk = o->wvn[0]; }
+      else { hams_dispersion(o->wvn, HAMS_NK, o->w1, depth); o->wk = o->wvn[0]; }
       o->wl = 2.0 * kPi / o->wk;
       o->tp = 2.0 * kPi / o->w1;
       break;
@@ -86,7 +86,7 @@ extern "C" int hams_wave_properties(int32_t inft, double value, double depth, do
       o->wk = value;
       o->v = deep ? o->wk : o->wk * std::tanh(o->wk * depth);
       o->w1 = std::sqrt(g * o->v);
-      if (!deep) dispersion(o->wvn, HAMS_NK, o->w1, depth);
+      if (!deep) hams_dispersion(o->wvn, HAMS_NK, o->w1, depth);
       o->wl = 2.0 * kPi / o->wk;
       o->tp = 2.0 * kPi / o->w1;
       break;
@@ -94,7 +94,7 @@ extern "C" int hams_wave_properties(int32_t inft, double value, double depth, do
       o->w1 = value;
       o->v = o->w1 * o->w1 / g;
       if (deep) o->wk = o->v;
-      else { dispersion(o->wvn, HAMS_NK, o->w1, depth); o->wk = o->wvn[0]; }
+      else { hams_dispersion(o->wvn, HAMS_NK, o->w1, depth); o->wk = o->wvn[0]; }
       o->wl = 2.0 * kPi / o->wk;
       o->tp = 2.0 * kPi / o->w1;
       break;
@@ -103,7 +103,7 @@ extern "C" int hams_wave_properties(int32_t inft, double value, double depth, do
       o->w1 = 2.0 * kPi / o->tp;
       o->v = o->w1 * o->w1 / g;
       if (deep) o->wk = o->v;
-      else { dispersion(o->wvn, HAMS_NK, o->w1, depth); o->wk = o->wvn[0]; }
+      else { hams_dispersion(o->wvn, HAMS_NK, o->w1, depth); o->wk = o->wvn[0]; }
       o->wl = 2.0 * kPi / o->wk;
       break;
     case 5:
@@ -111,7 +111,7 @@ extern "C" int hams_wave_properties(int32_t inft, double value, double depth, do
       o->wk = 2.0 * kPi / o->wl;
       o->v = deep ? o->wk : o->wk * std::tanh(o->wk * depth);
       o->w1 = std::sqrt(g * o->v);
-      if (!deep) dispersion(o->wvn, HAMS_NK, o->w1, depth);
+      if (!deep) hams_dispersion(o->wvn, HAMS_NK, o->w1, depth);
       break;
     default:
       return HAMS_ERR_ARG;

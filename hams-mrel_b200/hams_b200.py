@@ -44,6 +44,11 @@ class HamsWave(ctypes.Structure):
     _fields_ = [("v", c_dbl), ("wk", c_dbl), ("w1", c_dbl), ("tp", c_dbl), ("wl", c_dbl), ("wvn", c_dbl * HAMS_NK)]
 
 
+class SgTrain(ctypes.Structure):
+    _fields_ = [("n_train", c_int), ("n_test", c_int), ("batch", c_int), ("steps", c_int), ("nslice", c_int),
+                ("reserved0", c_int), ("seed", ctypes.c_uint64), ("lr", c_dbl), ("reserved", c_dbl * 4)]
+
+
 class HamsError(RuntimeError):
     def __init__(self, code, msg):
         super().__init__(f"hams error {code}: {msg}")
@@ -80,6 +85,13 @@ def load_library(path=LIB_PATH):
     lib.hams_measure_fp64_peak.argtypes = [c_int, P_dbl]
     lib.hams_prepare_geometry.argtypes = [c_int, P_dbl, c_int, P_int, P_int, c_int, P_int, P_dbl, P_dbl, P_dbl, P_dbl,
                                           P_dbl]
+    P_flt = ctypes.POINTER(ctypes.c_float)
+    lib.hams_surrogate_param_count.restype = c_int
+    lib.hams_ctx_set_surrogate.argtypes = [ctypes.c_void_p, P_flt, c_int, c_dbl]
+    lib.hams_surrogate_samples.argtypes = [c_int, c_int, ctypes.c_uint64, c_int, P_dbl]
+    lib.hams_surrogate_train.argtypes = [c_int, ctypes.POINTER(SgTrain), P_flt, P_dbl]
+    lib.hams_surrogate_eval.argtypes = [c_int, P_flt, c_int, P_dbl, P_dbl]
+    lib.hams_surrogate_grad.argtypes = [c_int, P_flt, c_int, P_flt, P_flt, P_dbl, P_flt]
     _LIB = lib
     return lib
 
@@ -210,12 +222,22 @@ class Context:
 
     def timings(self):
         """Stage times of the last solve (ms), per-branch Green kernel times and pair counts."""
-        ms = np.zeros(16)
-        load_library().hams_last_timings(self._h, _d(ms), 16)
+        ms = np.zeros(18)
+        load_library().hams_last_timings(self._h, _d(ms), 18)
         return dict(green=ms[0], rhs=ms[1], solve=ms[2], forces=ms[3], total=ms[4], green_linton=ms[5],
                     green_pidcock=ms[6], green_eigene=ms[7], green_eigen=ms[8], factor=ms[9], refine_sweeps=int(ms[10]),
                     pairs_linton=int(ms[11]), pairs_pidcock=int(ms[12]), pairs_eigene=int(ms[13]),
-                    pairs_eigen=int(ms[14]), lu_used=int(ms[15]))
+                    pairs_eigen=int(ms[14]), lu_used=int(ms[15]), green_surrogate=ms[16],
+                    pairs_surrogate=int(ms[17]))
+
+    def set_surrogate(self, params, far_factor=3.0):
+        """Far pairs from the trained network (params float32), or the series again (params None)."""
+        lib = load_library()
+        if params is None:
+            _check(lib.hams_ctx_set_surrogate(self._h, None, 0, 0.0))
+            return
+        self._sg = np.ascontiguousarray(params, dtype=np.float32)
+        _check(lib.hams_ctx_set_surrogate(self._h, _f(self._sg), self._sg.size, float(far_factor)))
 
     def launch_count(self):
         """Kernels of this library launched so far on this context."""
@@ -239,3 +261,54 @@ def measure_fp64_peak(device=0):
     t = ctypes.c_double()
     _check(load_library().hams_measure_fp64_peak(device, ctypes.byref(t)))
     return t.value
+
+
+# ---------------------------------------------------------------------------
+# MLP surrogate of the finite-depth evanescent Green function
+# ---------------------------------------------------------------------------
+def _f(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+
+
+def surrogate_param_count():
+    return int(load_library().hams_surrogate_param_count())
+
+
+def surrogate_samples(n, seed=1, nslice=256, device=0):
+    """n samples of the series: columns X, Zq, Zp, K, t0, t1, t2."""
+    raw = np.zeros((n, 7), order="F")
+    _check(load_library().hams_surrogate_samples(device, n, seed, nslice, _d(raw)))
+    return raw
+
+
+def surrogate_train(n_train=4_000_000, n_test=200_000, batch=4096, steps=20000, nslice=256, seed=1, lr=2e-3,
+                    device=0):
+    """Generate samples and train on the GPU; returns (params float32, stats dict)."""
+    cfg = SgTrain(n_train=n_train, n_test=n_test, batch=batch, steps=steps, nslice=nslice, seed=seed, lr=lr)
+    params = np.zeros(surrogate_param_count(), dtype=np.float32)
+    st = np.zeros(9)
+    _check(load_library().hams_surrogate_train(device, ctypes.byref(cfg), _f(params), _d(st)))
+    stats = dict(rms_rel=st[0:3].tolist(), max_rel=st[3:6].tolist(), loss=float(st[6]), train_ms=float(st[7]),
+                 sample_ms=float(st[8]))
+    return params, stats
+
+
+def surrogate_eval(params, x, device=0):
+    """FP32 network outputs t (n,3) for inputs x (n,4) = X, Zq, Zp, K."""
+    params = np.ascontiguousarray(params, dtype=np.float32)
+    x = np.asfortranarray(x, dtype=np.float64)
+    t = np.zeros((x.shape[0], 3), order="F")
+    _check(load_library().hams_surrogate_eval(device, _f(params), x.shape[0], _d(x), _d(t)))
+    return t
+
+
+def surrogate_grad(params, feats, targ, device=0):
+    """Loss and gradient of the normalised MSE for feats (4,n), targ (3,n)."""
+    params = np.ascontiguousarray(params, dtype=np.float32)
+    feats = np.asfortranarray(feats, dtype=np.float32)
+    targ = np.asfortranarray(targ, dtype=np.float32)
+    grad = np.zeros_like(params)
+    loss = ctypes.c_double()
+    _check(load_library().hams_surrogate_grad(device, _f(params), feats.shape[1], _f(feats), _f(targ),
+                                              ctypes.byref(loss), _f(grad)))
+    return loss.value, grad

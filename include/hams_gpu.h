@@ -177,13 +177,57 @@ int hams_eval_green(hams_ctx *ctx, const hams_wave *wave, int32_t npts, const do
 int hams_eval_green_static(hams_ctx *ctx, const hams_wave *wave, int32_t npts, const double *pts,
                            const int32_t *flag, double *grn);
 
+/*
+ * MLP surrogate of the finite-depth evanescent Green function (no
+ * counterpart in the reference; the reference always sums the series of
+ * FinGreen3D.f90:281-506).  Inputs per panel pair: X = R/h, the source and
+ * field depths above the bottom (zq+h)/h, (zp+h)/h, and K = k0 h tanh(k0 h);
+ * outputs the evanescent part of the wave term (without the propagating mode
+ * and with 1/r, 1/r1 removed) and its R and zq derivatives, in depth units,
+ * scaled by X, X^2, X^2.  Domain X in [0.05, 3], depths in [0.5, 1],
+ * K in [0.04, 40]; 4 SiLU hidden layers of width 128.
+ */
+typedef struct hams_sg_train {
+  int32_t n_train, n_test; /* samples generated from the series (training, held out) */
+  int32_t batch, steps;    /* minibatch size, Adam steps                              */
+  int32_t nslice;          /* K values sampled (log-spaced over the domain)           */
+  int32_t reserved0;
+  uint64_t seed;
+  double lr;               /* peak learning rate (warm-up, then cosine decay)         */
+  double reserved[4];
+} hams_sg_train;
+
+/* Number of floats in a parameter vector. */
+int32_t hams_surrogate_param_count(void);
+/* n training samples from the series: raw (n,7) = X, Zq, Zp, K, t0, t1, t2. */
+int hams_surrogate_samples(int32_t device, int32_t n, uint64_t seed, int32_t nslice, double *raw);
+/* Generates samples and trains on the GPU; params receives the network,
+ * stats (9): held-out RMS error / RMS of t0..t2, max error / max |t| of
+ * t0..t2, final training loss, training and sampling time (ms). */
+int hams_surrogate_train(int32_t device, const hams_sg_train *cfg, float *params, double *stats);
+/* Reference FP32 evaluation: x (n,4) = X, Zq, Zp, K -> t (n,3). */
+int hams_surrogate_eval(int32_t device, const float *params, int32_t n, const double *x, double *t);
+/* Mean squared error of normalised outputs and its gradient for inputs
+ * feats (4,n) (features in [-1,1]) and normalised targets targ (3,n). */
+int hams_surrogate_grad(int32_t device, const float *params, int32_t n, const float *feats, const float *targ,
+                        double *loss, float *grad);
+
+/* Switches the surrogate on for the far pairs of ctx (params: a trained
+ * vector, nparams = hams_surrogate_param_count()) or off (params NULL).  A
+ * pair is far when its centre distance exceeds far_factor times the source
+ * panel's longest edge, it lies in the network's domain, and it falls in the
+ * EIGENE or EIGEN branch; frequencies with K outside the domain keep the
+ * series for all pairs.  Finite depth only. */
+int hams_ctx_set_surrogate(hams_ctx *ctx, const float *params, int32_t nparams, double far_factor);
+
 /* Timing of the last solve in milliseconds: [0] Green/assembly kernels,
  * [1] right-hand sides, [2] factorisation + solves, [3] reductions,
  * [4] whole call, [5..8] Green kernels of the LINTON, PIDCOCK, EIGENE and
  * EIGEN branches (finite depth), [9] LU factorisation, [10] refinement
  * sweeps (mixed form), [11..14] pairs in each branch, [15] the mixed
- * form's factorisation (HAMS_LU_*; -1 for FP64).  n is the capacity of ms
- * (16 fills all). Returns the number written. */
+ * form's factorisation (HAMS_LU_*; -1 for FP64), [16] the surrogate kernel
+ * (or the series standing in for it), [17] pairs the surrogate evaluated.
+ * n is the capacity of ms (18 fills all). Returns the number written. */
 int hams_last_timings(hams_ctx *ctx, double *ms, int32_t n);
 
 /* Kernels of this library launched since the context was created (library
