@@ -52,13 +52,25 @@ void launch_green_series(int br, unsigned blocks, cudaStream_t st, DevGeom g, Wa
 
 // Per-frequency mode tables (ModeTab) for modes 2..nmode-1: one thread per
 // (mode, panel) entry, the expressions of InlineModes (green.cuh), compiled
-// here without fused multiply-adds like the series that read them.
+// here without fused multiply-adds like the series that read them.  Slot 1
+// holds the propagating mode's factors for the surrogate kernel: pm[1] =
+// pi / NM0, src = (sinh, cosh) of k0 (zq + h), fld = cosh of k0 (zp + h).
 __global__ void k_mode_tables(DevGeom g, WaveDev w, const double* __restrict__ wvn, int nmode, double* pm, double* ac,
                               double2* src, double2* srct, double* fld, double* fldt) {
   int k = blockIdx.x * blockDim.x + threadIdx.x;
-  int i = blockIdx.y + 2;  // mode number
+  int i = blockIdx.y + 1;  // mode number (1: propagating-mode factors)
   if (i >= nmode) return;
   const double h = w.h;
+  if (i == 1) {
+    const double wk = w.wk;
+    if (k < g.n) {
+      double zfh = g.xq[k + 2 * g.n] + h;
+      src[g.n + k] = make_double2(sinh(wk * zfh), cosh(wk * zfh));
+    }
+    if (k < g.tn) fld[g.tn + k] = cosh(wk * (g.fxyz[k + 2 * g.tn] + h));
+    if (k == 0) pm[1] = 3.141592653589793 / (h / 2.0 * (1.0 + sinh(2.0 * wk * h) / (2.0 * wk * h)));
+    return;
+  }
   if (k < g.n) {
     hams::InlineModes md{wvn, h, w.v, g.xq[k + 2 * g.n] + h, 0.0};
     double s, c;
@@ -81,7 +93,7 @@ __global__ void k_mode_tables(DevGeom g, WaveDev w, const double* __restrict__ w
 
 void launch_mode_tables(cudaStream_t st, DevGeom g, WaveDev w, const double* wvn, int nmode, double* pm, double* ac,
                         double2* src, double2* srct, double* fld, double* fldt) {
-  dim3 grid((g.tn + 127) / 128, nmode - 2);
+  dim3 grid((g.tn + 127) / 128, nmode - 1);
   k_mode_tables<<<grid, 128, 0, st>>>(g, w, wvn, nmode, pm, ac, src, srct, fld, fldt);
 }
 

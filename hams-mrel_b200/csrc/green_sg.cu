@@ -50,7 +50,7 @@ __device__ __forceinline__ void ldsm_x4(const __half* row, uint32_t& r0, uint32_
 
 }  // namespace
 
-__global__ void __launch_bounds__(128, 2) k_green_sg(DevGeom g, WaveDev w, SgDev sp, double K,
+__global__ void __launch_bounds__(128, 2) k_green_sg(DevGeom g, WaveDev w, SgDev sp, hams::ModeTab mt, double K,
                                                      const uint32_t* __restrict__ pairs, long long count,
                                                      const double* __restrict__ rs, const double* __restrict__ rd,
                                                      double2* __restrict__ A, double2* __restrict__ S) {
@@ -170,9 +170,18 @@ __global__ void __launch_bounds__(128, 2) k_green_sg(DevGeom g, WaveDev w, SgDev
     if (lane < 16 && live) {
       const double t0 = sp.mean[0] + sp.scale[0] * y0, t1 = sp.mean[1] + sp.scale[1] * y1,
                    t2 = sp.mean[2] + sp.scale[2] * y2;
+      // propagating mode (FinGreen3D.f90:311-322) from the per-frequency factors
       hams::cplx fg[3];
       double rk[3];
-      hams::prop_mode(rr, zq + h, zp + h, w.wk, h, fg);
+      {
+        const double2 sc = mt.src[g.n + j];
+        const double czp = mt.fld[g.tn + i], p0 = mt.pm[1] * sc.y * czp, dp0 = mt.pm[1] * sc.x * czp;
+        double j0, j1, y0, y1;
+        hams::jy01b(w.wk * rr, j0, j1, y0, y1);
+        fg[0] = hams::cmk(-p0 * y0, p0 * j0);
+        fg[1] = hams::cmk(w.wk * p0 * y1, -w.wk * p0 * j1);
+        fg[2] = hams::cmk(-w.wk * dp0 * y0, w.wk * dp0 * j0);
+      }
       sg::rankine_parts(rr, zq, zp, rk);
       fg[0].re += t0 / (X * h) + rk[0];
       fg[1].re += t1 / (X * X * h * h) + rk[1];
@@ -186,13 +195,14 @@ __global__ void __launch_bounds__(128, 2) k_green_sg(DevGeom g, WaveDev w, SgDev
   }
 }
 
-int launch_green_sg(cudaStream_t st, int sms, DevGeom g, WaveDev w, const SgDev& sp, double K, const uint32_t* pairs,
+int launch_green_sg(cudaStream_t st, int sms, DevGeom g, WaveDev w, const SgDev& sp, const hams::ModeTab& mt, double K,
+                    const uint32_t* pairs,
                     long long count, const double* rs, const double* rd, double2* A, double2* S) {
   if (count <= 0) return 0;
   if (cudaFuncSetAttribute(k_green_sg, cudaFuncAttributeMaxDynamicSharedMemorySize, kSgSmem) != cudaSuccess) return 1;
   long long groups = (count + 15) / 16;
   long long blocks = std::min<long long>(2LL * sms, (groups + 3) / 4);
-  k_green_sg<<<(unsigned)blocks, 128, kSgSmem, st>>>(g, w, sp, K, pairs, count, rs, rd, A, S);
+  k_green_sg<<<(unsigned)blocks, 128, kSgSmem, st>>>(g, w, sp, mt, K, pairs, count, rs, rd, A, S);
   return cudaGetLastError() == cudaSuccess ? 0 : 1;
 }
 

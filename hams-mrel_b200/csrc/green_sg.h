@@ -25,10 +25,12 @@ struct SgDev {
 };
 
 // Green functions of `count` far pairs (list of pair indices) from the
-// network at dispersion parameter K = k0 h tanh(k0 h); returns 0 or 1 on a
-// launch error.
-int launch_green_sg(cudaStream_t st, int sms, DevGeom g, WaveDev w, const SgDev& sp, double K, const uint32_t* pairs,
-                    long long count, const double* rs, const double* rd, double2* A, double2* S);
+// network at dispersion parameter K = k0 h tanh(k0 h), the propagating mode
+// from slot 1 of the frequency's mode tables; returns 0 or 1 on a launch
+// error.
+int launch_green_sg(cudaStream_t st, int sms, DevGeom g, WaveDev w, const SgDev& sp, const hams::ModeTab& mt, double K,
+                    const uint32_t* pairs, long long count, const double* rs, const double* rd, double2* A,
+                    double2* S);
 
 // Trained parameters (surrogate.h layout) into the kernel's layout.
 void pack_surrogate(const float* P, std::vector<__half>& wh, std::vector<float>& w0, std::vector<float>& bias);

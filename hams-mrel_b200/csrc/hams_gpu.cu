@@ -822,8 +822,8 @@ static int assemble_dev(hams_ctx* c, const hams_wave* w, int nbeta) {
     const double hh = c->opts.depth, K = wd.wk * hh * tanh(wd.wk * hh);
     if (cs > 0) {
       if (!wd.limit && K >= sg::kKmin && K <= sg::kKmax) {
-        if (launch_green_sg(c->st, c->sms, c->g, wd, c->sgd, K, c->pairs.p + c->bin_off[4], cs, c->rs.p, c->rd.p,
-                            c->A.p, c->S.p))
+        if (launch_green_sg(c->st, c->sms, c->g, wd, c->sgd, c->mt, K, c->pairs.p + c->bin_off[4], cs, c->rs.p,
+                            c->rd.p, c->A.p, c->S.p))
           return fail(HAMS_ERR_CUDA, "surrogate kernel launch failed");
         c->launches += 1;
         c->sg_used = 1;

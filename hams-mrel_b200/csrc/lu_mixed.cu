@@ -48,23 +48,91 @@ __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
   return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
 
+__device__ __forceinline__ float2 cmac(float2 s, float2 a, float2 b) {
+  return make_float2(s.x + a.x * b.x - a.y * b.y, s.y + a.x * b.y + a.y * b.x);
+}
+
+// Inverse of the unit lower (lower) or the upper triangle of T (kNB x kNB,
+// ld kLd) into X: the 8 x 8 diagonal blocks by substitution, then three
+// doubling levels X21 = -X22 (L21 X11) (lower) or X12 = -X11 (U12 X22)
+// (upper), each product spread over the block's 256 threads; W holds the
+// inner products of one level (at most 32 columns).
+__device__ void tri_inverse(const float2* T, float2* X, float2* W, bool lower) {
+  const int tid = threadIdx.x;
+  for (int e = tid; e < kNB * kNB; e += 256) X[(e / kNB) * kLd + e % kNB] = make_float2(0.0f, 0.0f);
+  __syncthreads();
+  if (tid < kNB) {
+    const int c = tid, b0 = c & ~7;
+    if (lower) {
+      X[c * kLd + c] = make_float2(1.0f, 0.0f);
+      for (int i = c + 1; i < b0 + 8; ++i) {
+        float2 acc = make_float2(0.0f, 0.0f);
+        for (int k = c; k < i; ++k) acc = cmac(acc, T[k * kLd + i], X[c * kLd + k]);
+        X[c * kLd + i] = make_float2(-acc.x, -acc.y);
+      }
+    } else {
+      for (int i = c; i >= b0; --i) {
+        float2 acc = make_float2(i == c ? 1.0f : 0.0f, 0.0f);
+        for (int k = i + 1; k <= c; ++k) {
+          float2 t = cmac(make_float2(0.0f, 0.0f), T[k * kLd + i], X[c * kLd + k]);
+          acc.x -= t.x;
+          acc.y -= t.y;
+        }
+        const float2 d = T[i * kLd + i];
+        const float dd = d.x * d.x + d.y * d.y;
+        X[c * kLd + i] = dd > 0.0f ? make_float2((acc.x * d.x + acc.y * d.y) / dd, (acc.y * d.x - acc.x * d.y) / dd)
+                                   : make_float2(0.0f, 0.0f);
+      }
+    }
+  }
+  __syncthreads();
+  for (int sz = 8; sz < kNB; sz *= 2) {
+    const int tot = (kNB / (2 * sz)) * sz * sz;
+    for (int e = tid; e < tot; e += 256) {
+      const int q = e / (sz * sz), rem = e % (sz * sz), c = rem / sz, i = rem % sz, b0 = 2 * sz * q;
+      float2 acc = make_float2(0.0f, 0.0f);
+      if (lower)  // W = L21 X11
+        for (int k = c; k < sz; ++k) acc = cmac(acc, T[(b0 + k) * kLd + b0 + sz + i], X[(b0 + c) * kLd + b0 + k]);
+      else  // W = U12 X22
+        for (int k = 0; k <= c; ++k) acc = cmac(acc, T[(b0 + sz + k) * kLd + b0 + i], X[(b0 + sz + c) * kLd + b0 + sz + k]);
+      W[(q * sz + c) * kLd + i] = acc;
+    }
+    __syncthreads();
+    for (int e = tid; e < tot; e += 256) {
+      const int q = e / (sz * sz), rem = e % (sz * sz), c = rem / sz, i = rem % sz, b0 = 2 * sz * q;
+      float2 acc = make_float2(0.0f, 0.0f);
+      if (lower) {  // X21 = -X22 W
+        for (int k = 0; k <= i; ++k) acc = cmac(acc, X[(b0 + sz + k) * kLd + b0 + sz + i], W[(q * sz + c) * kLd + k]);
+        X[(b0 + c) * kLd + b0 + sz + i] = make_float2(-acc.x, -acc.y);
+      } else {  // X12 = -X11 W
+        for (int k = i; k < sz; ++k) acc = cmac(acc, X[(b0 + k) * kLd + b0 + i], W[(q * sz + c) * kLd + k]);
+        X[(b0 + sz + c) * kLd + b0 + i] = make_float2(-acc.x, -acc.y);
+      }
+    }
+    __syncthreads();
+  }
+}
+
 // One CTA of 256 threads: LU with partial pivoting of the nbk x nbk
 // diagonal block at (k0, k0), written back in place (unit L below, U on and
 // above the diagonal); the block's row permutation as global source rows in
 // perm; the expansions of L^-1 and U^-1 (2nbk x 2nbk, ld 2 kNB) in invL,
-// invU.  info gets 1 + the first global column whose pivot is zero.
+// invU.  info gets 1 + the first global column whose pivot is zero.  A
+// partial last block is padded with the identity to kNB.
 __global__ void __launch_bounds__(256) k_diag_lu(float2* A, int lda, int k0, int nbk, int* perm, float* invL,
                                                  float* invU, int* info) {
   extern __shared__ float2 sm[];
-  float2* T = sm;                 // [col * kLd + row]
-  float2* X = sm + kNB * kLd;     // L^-1
-  float2* Y = sm + 2 * kNB * kLd; // U^-1
+  float2* T = sm;                  // [col * kLd + row]
+  float2* X = sm + kNB * kLd;      // L^-1
+  float2* Y = sm + 2 * kNB * kLd;  // U^-1
+  float2* W = sm + 3 * kNB * kLd;  // inversion scratch (32 columns)
   __shared__ int piv[kNB];
   __shared__ int prm[kNB];
   const int tid = threadIdx.x, tx = tid % 16, ty = tid / 16;
-  for (int e = tid; e < nbk * nbk; e += 256) {
-    int r = e % nbk, c = e / nbk;
-    T[c * kLd + r] = A[(size_t)(k0 + c) * lda + k0 + r];
+  for (int e = tid; e < kNB * kNB; e += 256) {
+    int r = e % kNB, c = e / kNB;
+    T[c * kLd + r] = (r < nbk && c < nbk) ? A[(size_t)(k0 + c) * lda + k0 + r]
+                                          : make_float2(r == c ? 1.0f : 0.0f, 0.0f);
   }
   __syncthreads();
   for (int j = 0; j < nbk; ++j) {
@@ -93,18 +161,29 @@ __global__ void __launch_bounds__(256) k_diag_lu(float2* A, int lda, int k0, int
       }
     }
     __syncthreads();
-    const int p = piv[j];
-    if (p != j && tid < nbk) {
-      float2 t = T[tid * kLd + j];
-      T[tid * kLd + j] = T[tid * kLd + p];
-      T[tid * kLd + p] = t;
-    }
-    __syncthreads();
-    float2 d = T[j * kLd + j];
-    float dd = d.x * d.x + d.y * d.y;
-    if (dd > 0.0f && tid > j && tid < nbk) {
-      float2 rcp = make_float2(d.x / dd, -d.y / dd);
-      T[j * kLd + tid] = cmul(T[j * kLd + tid], rcp);
+    // row swap j <-> p and the multipliers of column j in one pass, from the
+    // values before the swap: thread t swaps column t (t != j) and scales
+    // row t of column j (t > j, t != p); thread j handles rows j and p of
+    // column j
+    {
+      const int p = piv[j];
+      const float2 d = T[j * kLd + p];  // the pivot
+      const float dd = d.x * d.x + d.y * d.y;
+      const float2 rcp = dd > 0.0f ? make_float2(d.x / dd, -d.y / dd) : make_float2(0.0f, 0.0f);
+      if (tid < nbk) {
+        if (tid != j) {
+          if (p != j) {
+            float2 t = T[tid * kLd + j];
+            T[tid * kLd + j] = T[tid * kLd + p];
+            T[tid * kLd + p] = t;
+          }
+          if (tid > j && tid != p && dd > 0.0f) T[j * kLd + tid] = cmul(T[j * kLd + tid], rcp);
+        } else {
+          const float2 old = T[j * kLd + j];
+          T[j * kLd + j] = d;
+          if (p != j) T[j * kLd + p] = dd > 0.0f ? cmul(old, rcp) : old;
+        }
+      }
     }
     __syncthreads();
     // rank-1 update: tx walks rows (consecutive in shared memory), ty columns
@@ -125,56 +204,8 @@ __global__ void __launch_bounds__(256) k_diag_lu(float2* A, int lda, int k0, int
       prm[piv[j]] = t;
     }
   }
-  // inverses by columns, four lanes per column sharing each inner product
-  {
-    const int c = tid / 4, q = tid % 4;
-    const bool live = c < nbk;
-    // L^-1 (unit lower): X(i,c) = -sum_{k=c}^{i-1} L(i,k) X(k,c)
-    if (live)
-      for (int i = q; i < nbk; i += 4) X[c * kLd + i] = make_float2(i == c ? 1.0f : 0.0f, 0.0f);
-    __syncwarp();
-    for (int i = 1; i < nbk; ++i) {
-      float2 s = make_float2(0.0f, 0.0f);
-      if (live && i > c)
-        for (int k = c + q; k < i; k += 4) {
-          float2 l = T[k * kLd + i], x = X[c * kLd + k];
-          s.x += l.x * x.x - l.y * x.y;
-          s.y += l.x * x.y + l.y * x.x;
-        }
-      s.x += __shfl_xor_sync(0xffffffffu, s.x, 1);
-      s.y += __shfl_xor_sync(0xffffffffu, s.y, 1);
-      s.x += __shfl_xor_sync(0xffffffffu, s.x, 2);
-      s.y += __shfl_xor_sync(0xffffffffu, s.y, 2);
-      if (live && i > c && q == 0) X[c * kLd + i] = make_float2(-s.x, -s.y);
-      __syncwarp();
-    }
-    // U^-1 (upper): Y(i,c) = (delta_ic - sum_{k=i+1}^{c} U(i,k) Y(k,c)) / U(i,i)
-    if (live)
-      for (int i = q; i < nbk; i += 4) Y[c * kLd + i] = make_float2(0.0f, 0.0f);
-    __syncwarp();
-    for (int i = nbk - 1; i >= 0; --i) {
-      float2 s = make_float2(0.0f, 0.0f);
-      if (live && i <= c)
-        for (int k = i + 1 + q; k <= c; k += 4) {
-          float2 u = T[k * kLd + i], y = Y[c * kLd + k];
-          s.x += u.x * y.x - u.y * y.y;
-          s.y += u.x * y.y + u.y * y.x;
-        }
-      s.x += __shfl_xor_sync(0xffffffffu, s.x, 1);
-      s.y += __shfl_xor_sync(0xffffffffu, s.y, 1);
-      s.x += __shfl_xor_sync(0xffffffffu, s.x, 2);
-      s.y += __shfl_xor_sync(0xffffffffu, s.y, 2);
-      if (live && i <= c && q == 0) {
-        float2 d = T[i * kLd + i];
-        float dd = d.x * d.x + d.y * d.y;
-        float nx = (i == c ? 1.0f : 0.0f) - s.x, ny = -s.y;
-        Y[c * kLd + i] = dd > 0.0f ? make_float2((nx * d.x + ny * d.y) / dd, (ny * d.x - nx * d.y) / dd)
-                                   : make_float2(0.0f, 0.0f);
-      }
-      __syncwarp();
-    }
-  }
-  __syncthreads();
+  tri_inverse(T, X, W, true);
+  tri_inverse(T, Y, W, false);
   for (int e = tid; e < nbk * nbk; e += 256) {
     int r = e % nbk, c = e / nbk;
     A[(size_t)(k0 + c) * lda + k0 + r] = T[c * kLd + r];
@@ -232,7 +263,7 @@ size_t mixed_lu_workspace_elems(int n) {
 
 int mixed_lu_factor(cudaStream_t st, cublasHandle_t blas, cublasComputeType_t ct, int n, float2* A, int* perm,
                     float2* work, int* dinfo, long long* launches, long long* lib_calls) {
-  const int smem = 3 * kNB * kLd * (int)sizeof(float2);
+  const int smem = (3 * kNB + 32) * kLd * (int)sizeof(float2);
   if (cudaFuncSetAttribute(k_diag_lu, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess) return 1;
   const int nblk = (n + kNB - 1) / kNB, K2 = 2 * kNB;
   float* W1 = (float*)work;                     // U panel, real 2nbk x w (ld 2kNB)
