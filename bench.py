@@ -292,22 +292,20 @@ def gpu_arm(args):
             dist.barrier()
         torch.cuda.synchronize()
 
-    def max_over_ranks(x):
-        if ws == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
-
     import hams_b200 as hb
+    import shard
     import train_surrogate
+
+    def max_over_ranks(x):
+        return shard.max_over_ranks(x, dist if ws > 1 else None, device="cuda")
 
     case, xyz, ncn, ncon, cnt, xr = build_case()
     geom = hb.prepare_geometry(xyz, ncn, ncon, cnt, xr)
     betas = np.radians(case["betas_deg"])
     allom = case["omegas"]
-    # weak scaling: rank r takes frequencies r*K, r*K+1, ... of the repeated sweep
-    om_rank = np.array([allom[(rank * args.steps + s) % len(allom)] for s in range(args.steps)])
+    # weak scaling: rank r takes the contiguous block r*K ... r*K + K-1 of the repeated sweep
+    lo, hi = shard.block(ws * args.steps, rank, ws)
+    om_rank = np.array([allom[i % len(allom)] for i in range(lo, hi)])
     om_warm = np.array([allom[(s * 7 + 3) % len(allom)] for s in range(args.warmup)])
     sgp = train_surrogate.load()
     prec = {"mixed": hb.PREC_MIXED, "fp64": hb.PREC_FP64}

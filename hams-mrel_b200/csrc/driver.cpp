@@ -1,0 +1,467 @@
+// driver.cpp -- hams_b200_run: a HAMS-MREL deck through the B200 library.
+//
+//   hams_b200_run <inputdir> <outputdir> [--mixed] [--surrogate FILE] [--far F]
+//                 [--lanes N] [--device D]
+//
+// Reads the reference's input deck -- ControlFile.in (ReadControlFile,
+// src/InputFiles.f90:46-224), HullMesh[_k].pnl and, with IRSP = 1,
+// WaterPlaneMesh[_k].pnl (src/ReadPanelMesh.f90:46-99,
+// src/ReadPanelMeshMulti.f90:46-111, local coordinate systems applied on
+// read), gen_mod_{body}_{dof}.txt generalized normals -- solves every
+// frequency and heading through the C ABI of include/hams_gpu.h, and writes
+// the HAMS-format added mass, damping and excitation files
+// <outputdir>/Hams_format/OAMASS{1..6}.txt, ODAMPING{1..6}.txt,
+// OEXFOR{1..6}.txt in the order and formats of RFORCE_MULTI / EFORCE_MULTI
+// (src/PotentWavForceMulti.f90).  Constants are the reference's
+// (rho 1000, g 9.80665, unit amplitude, wave reference point at the origin).
+#include <sys/stat.h>
+
+#include <cctype>
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <sstream>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/hams_gpu.h"
+
+namespace {
+
+constexpr double kPi = 3.141592653589793;
+
+struct Lines {
+  std::vector<std::string> v;
+  size_t cur = 0;
+  explicit Lines(const std::string& path) {
+    std::ifstream f(path);
+    if (!f) throw std::runtime_error("cannot open " + path);
+    std::string l;
+    while (std::getline(f, l)) {
+      while (!l.empty() && (l.back() == '\r' || l.back() == '\n')) l.pop_back();
+      v.push_back(l);
+    }
+  }
+  const std::string& next() {
+    static const std::string empty;
+    return cur < v.size() ? v[cur++] : empty;
+  }
+  const std::string* peek() const { return cur < v.size() ? &v[cur] : nullptr; }
+};
+
+// Columns [skip, skip + w) of a record with blanks removed (Fortran BN editing).
+std::string field(const std::string& l, int skip, int w) {
+  std::string o;
+  for (int i = skip; i < skip + w && i < (int)l.size(); ++i)
+    if (l[i] != ' ' && l[i] != '\t') o += l[i];
+  return o;
+}
+
+// Fortran F/E/D input of a field with d implied decimals when it has no point.
+double fortran_real(std::string s, int d) {
+  if (s.empty()) return 0.0;
+  bool point = false;
+  for (char& c : s) {
+    if (c == 'd' || c == 'D' || c == 'q' || c == 'Q') c = 'E';
+    if (c == '.') point = true;
+  }
+  for (size_t i = 1; i < s.size(); ++i)  // exponent written as a bare sign: 1.0+3
+    if ((s[i] == '+' || s[i] == '-') && std::isdigit((unsigned char)s[i - 1]) && s[i - 1] != 'E') {
+      s.insert(i, "E");
+      break;
+    }
+  double v = std::strtod(s.c_str(), nullptr);
+  if (!point)
+    for (int e = 0; e < d; ++e) v /= 10.0;
+  return v;
+}
+
+double read_f(Lines& r, int skip, int w, int d) { return fortran_real(field(r.next(), skip, w), d); }
+int read_i(Lines& r, int skip, int w) { return (int)std::strtol(field(r.next(), skip, w).c_str(), nullptr, 10); }
+
+// List-directed read of n values, across records.
+std::vector<double> read_list(Lines& r, int n) {
+  std::vector<double> v;
+  while ((int)v.size() < n) {
+    if (r.cur >= r.v.size()) throw std::runtime_error("unexpected end of file in a list");
+    std::string l = r.next();
+    for (char& c : l)
+      if (c == ',' || c == '\t') c = ' ';
+      else if (c == 'd' || c == 'D') c = 'E';
+    std::istringstream is(l);
+    std::string tok;
+    while ((int)v.size() < n && is >> tok) v.push_back(std::strtod(tok.c_str(), nullptr));
+  }
+  return v;
+}
+
+struct Mesh {
+  int nelem = 0, ntnd = 0, isx = 0, isy = 0;
+  std::vector<double> xyz;  // ntnd x 3, row-major
+  std::vector<int> ncn, ncon;  // ncon nelem x 4, row-major
+};
+
+Mesh read_pnl(const std::string& path, bool lid) {
+  Lines r(path);
+  Mesh m;
+  r.next();
+  r.next();
+  r.next();
+  auto h = read_list(r, 4);
+  m.nelem = (int)h[0];
+  m.ntnd = (int)h[1];
+  m.isx = (int)h[2];
+  m.isy = (int)h[3];
+  r.next();
+  r.next();
+  m.xyz.resize(3 * (size_t)m.ntnd);
+  m.ncn.resize(m.nelem);
+  m.ncon.assign(4 * (size_t)m.nelem, 0);
+  for (int i = 0; i < m.ntnd; ++i) {
+    auto v = read_list(r, 4);
+    for (int k = 0; k < 3; ++k) m.xyz[3 * i + k] = v[1 + k];
+    if (lid && std::fabs(v[3]) > (double)1.E-10f) throw std::runtime_error(path + ": water-plane node off z = 0");
+  }
+  r.next();
+  r.next();
+  r.next();
+  for (int i = 0; i < m.nelem; ++i) {
+    std::istringstream is(r.next());
+    int id = 0, nc = 0;
+    is >> id >> nc;
+    if (nc != 3 && nc != 4) throw std::runtime_error(path + ": panel with " + std::to_string(nc) + " vertices");
+    m.ncn[i] = nc;
+    for (int k = 0; k < nc; ++k) is >> m.ncon[4 * i + k];
+  }
+  return m;
+}
+
+bool exists(const std::string& p) {
+  struct stat st;
+  return stat(p.c_str(), &st) == 0;
+}
+
+struct Deck {
+  double h = 0.0;
+  int sybo = 0, inft = 3, ouft = 3, nbody = 1, isol = 1, irsp = 0, isolv = 1;
+  std::vector<double> wvnb, wvhd, xr /* (nb,3) */, lcs /* (nb,4) */;
+  // combined hull (column-major, 1-based connectivity) and lid centres
+  int nelem = 0, ntnd = 0, isx = 0, isy = 0;
+  std::vector<double> xyz, xyz_p, ds, pnsz, dxyz, ixyz_p;
+  std::vector<int> ncn, ncon, body_nelem;
+  int inelem = 0;
+};
+
+Deck load(const std::string& dir) {
+  Deck d;
+  Lines r(dir + "/ControlFile.in");
+  r.next();
+  r.next();
+  d.h = read_f(r, 14, 30, 15);
+  r.next();
+  r.next();
+  d.sybo = read_i(r, 27, 16);
+  d.inft = read_i(r, 25, 16);
+  d.ouft = read_i(r, 25, 17);
+  int npet = read_i(r, 26, 16);
+  const int ifs = d.sybo == 1 ? 2 : 0;
+  if (npet > 0) {
+    auto v = read_list(r, npet);
+    d.wvnb.assign(ifs, 0.0);
+    d.wvnb.insert(d.wvnb.end(), v.begin(), v.end());
+  } else {
+    npet = -npet;
+    double w1 = read_f(r, 27, 30, 15), dw = read_f(r, 19, 30, 15);
+    d.wvnb.assign(ifs, 0.0);
+    for (int i = 0; i < npet; ++i) d.wvnb.push_back(w1 + i * dw);
+  }
+  r.next();
+  r.next();
+  const std::string bodycheck = r.next();
+  d.nbody = bodycheck.find("multi") != std::string::npos ? read_i(r, 24, 16) : 1;
+  const int nb = d.nbody;
+  if (nb < 1) throw std::runtime_error("number of bodies < 1");
+  d.lcs.assign(4 * (size_t)nb, 0.0);
+  if (nb > 1) {
+    for (int b = 0; b < nb; ++b) {
+      const std::string l = r.next();
+      for (int k = 0; k < 4; ++k) d.lcs[b + nb * k] = fortran_real(field(l, 26 + 12 * k, 12), 3);
+    }
+    r.next();
+    r.next();
+    r.next();
+  }
+  int nbeta = read_i(r, 23, 16);
+  if (nbeta > 0) {
+    d.wvhd = read_list(r, nbeta);
+  } else {
+    nbeta = -nbeta;
+    double b1 = read_f(r, 20, 30, 15), db = read_f(r, 17, 30, 15);
+    for (int i = 0; i < nbeta; ++i) d.wvhd.push_back(b1 + i * db);
+  }
+  r.next();
+  r.next();
+  d.xr.assign(3 * (size_t)nb, 0.0);
+  for (int b = 0; b < nb; ++b) {
+    const std::string l = r.next();
+    for (int k = 0; k < 3; ++k) d.xr[b + nb * k] = fortran_real(field(l, 28 + 12 * k, 12), 3);
+  }
+  read_f(r, 26, 30, 15);  // reference body length (not used by this path)
+  d.isol = read_i(r, 26, 16);
+  d.irsp = read_i(r, 23, 16);
+  read_i(r, 23, 16);  // NTHREAD
+  if (const std::string* l = r.peek())
+    if (l->find("Solver_type") != std::string::npos) {
+      d.isolv = (int)std::strtol(field(*l, 26, 16).c_str(), nullptr, 10);
+      r.next();
+    }
+
+  // meshes, bodies stacked in order, local coordinates rotated and shifted
+  std::vector<Mesh> hull(nb), lid(nb);
+  for (int b = 0; b < nb; ++b) {
+    const std::string sfx = nb == 1 ? "" : "_" + std::to_string(b + 1);
+    hull[b] = read_pnl(dir + "/HullMesh" + sfx + ".pnl", false);
+    d.isx = hull[b].isx;
+    d.isy = hull[b].isy;
+    d.nelem += hull[b].nelem;
+    d.ntnd += hull[b].ntnd;
+    d.body_nelem.push_back(hull[b].nelem);
+    if (d.irsp == 1) {
+      const std::string lp = dir + "/WaterPlaneMesh" + sfx + ".pnl";
+      if (exists(lp)) lid[b] = read_pnl(lp, true);
+      else if (nb == 1) throw std::runtime_error(lp + " is missing (IRSP = 1)");
+      d.inelem += lid[b].nelem;
+    }
+  }
+  const int n = d.nelem, nt = d.ntnd;
+  d.xyz.assign(3 * (size_t)nt, 0.0);
+  d.ncn.assign(n, 0);
+  d.ncon.assign(4 * (size_t)n, 0);
+  auto place = [&](const Mesh& m, int b, std::vector<double>& xyz, int ntot, int off_n) {
+    const double c = std::cos(d.lcs[b + 3 * nb]), s = std::sin(d.lcs[b + 3 * nb]);
+    for (int i = 0; i < m.ntnd; ++i) {
+      const double x = m.xyz[3 * i], y = m.xyz[3 * i + 1];
+      if (nb > 1) {
+        xyz[off_n + i] = 0.0 + d.lcs[b] + c * x - s * y;
+        xyz[off_n + i + ntot] = 0.0 + d.lcs[b + nb] + s * x + c * y;
+      } else {
+        xyz[off_n + i] = x;
+        xyz[off_n + i + ntot] = y;
+      }
+      xyz[off_n + i + 2 * (size_t)ntot] = m.xyz[3 * i + 2];
+    }
+  };
+  int off_e = 0, off_n = 0;
+  for (int b = 0; b < nb; ++b) {
+    place(hull[b], b, d.xyz, nt, off_n);
+    for (int i = 0; i < hull[b].nelem; ++i) {
+      d.ncn[off_e + i] = hull[b].ncn[i];
+      for (int k = 0; k < 4; ++k) {
+        int id = hull[b].ncon[4 * i + k];
+        d.ncon[off_e + i + (size_t)n * k] = id ? id + off_n : 0;
+      }
+    }
+    off_e += hull[b].nelem;
+    off_n += hull[b].ntnd;
+  }
+  d.xyz_p.assign(3 * (size_t)n, 0.0);
+  d.ds.assign(n, 0.0);
+  d.pnsz.assign(n, 0.0);
+  d.dxyz.assign(6 * (size_t)n, 0.0);
+  int rc = hams_prepare_geometry(nt, d.xyz.data(), n, d.ncn.data(), d.ncon.data(), nb, d.body_nelem.data(),
+                                 d.xr.data(), d.xyz_p.data(), d.ds.data(), d.pnsz.data(), d.dxyz.data());
+  if (rc) throw std::runtime_error(std::string("geometry: ") + hams_last_error());
+  // generalized modes override the normals of a body (ReadPanelMeshMulti.f90:170-200)
+  int i0 = 0;
+  for (int b = 0; b < nb; ++b) {
+    for (int dof = 1; dof <= 6; ++dof) {
+      const std::string gp = dir + "/gen_mod_" + std::to_string(nb == 1 ? 1 : b + 1) + "_" + std::to_string(dof) + ".txt";
+      std::ifstream f(gp);
+      if (!f) continue;
+      std::string l;
+      for (int i = 0; i < d.body_nelem[b] && std::getline(f, l); ++i) {
+        for (char& c : l)
+          if (c == 'd' || c == 'D') c = 'E';
+        std::istringstream is(l);
+        int pid = 0;
+        double val = 0.0;
+        if (!(is >> pid >> val)) break;
+        d.dxyz[i0 + pid - 1 + (size_t)n * (dof - 1)] = val;
+      }
+    }
+    i0 += d.body_nelem[b];
+  }
+  // lid centres (the lids' own normals are not used by the solve)
+  if (d.inelem > 0) {
+    int lnt = 0;
+    for (int b = 0; b < nb; ++b) lnt += lid[b].ntnd;
+    std::vector<double> lxyz(3 * (size_t)lnt, 0.0);
+    std::vector<int> lncn(d.inelem), lncon(4 * (size_t)d.inelem, 0), one{d.inelem};
+    int le = 0, ln = 0;
+    for (int b = 0; b < nb; ++b) {
+      place(lid[b], b, lxyz, lnt, ln);
+      for (int i = 0; i < lid[b].nelem; ++i) {
+        lncn[le + i] = lid[b].ncn[i];
+        for (int k = 0; k < 4; ++k) {
+          int id = lid[b].ncon[4 * i + k];
+          lncon[le + i + (size_t)d.inelem * k] = id ? id + ln : 0;
+        }
+      }
+      le += lid[b].nelem;
+      ln += lid[b].ntnd;
+    }
+    std::vector<double> zero3(3, 0.0), lds(d.inelem), lsz(d.inelem), ldx(6 * (size_t)d.inelem);
+    d.ixyz_p.assign(3 * (size_t)d.inelem, 0.0);
+    rc = hams_prepare_geometry(lnt, lxyz.data(), d.inelem, lncn.data(), lncon.data(), 1, one.data(), zero3.data(),
+                               d.ixyz_p.data(), lds.data(), lsz.data(), ldx.data());
+    if (rc) throw std::runtime_error(std::string("lid geometry: ") + hams_last_error());
+  }
+  return d;
+}
+
+// Fortran Ew.d output editing: 0.dddd...E+xx, right-aligned in w columns.
+std::string fmt_e(int w, int dg, double v) {
+  char out[64], full[64];
+  if (v == 0.0) {
+    std::string z = "0." + std::string(dg, '0') + "E+00";
+    std::snprintf(out, sizeof(out), "%*s", w, z.c_str());
+    return out;
+  }
+  char m[64];
+  std::snprintf(m, sizeof(m), "%.*e", dg - 1, std::fabs(v));
+  int e = std::atoi(std::strchr(m, 'e') + 1) + 1;
+  std::string mant = "0.";
+  mant += m[0];
+  for (const char* p = m + 2; *p && *p != 'e'; ++p) mant += *p;
+  if (e >= -99 && e <= 99)
+    std::snprintf(full, sizeof(full), "%s%sE%c%02d", v < 0 ? "-" : "", mant.c_str(), e < 0 ? '-' : '+', std::abs(e));
+  else
+    std::snprintf(full, sizeof(full), "%s%s%c%03d", v < 0 ? "-" : "", mant.c_str(), e < 0 ? '-' : '+', std::abs(e));
+  std::snprintf(out, sizeof(out), "%*s", w, full);
+  return out;
+}
+
+std::vector<float> read_params(const std::string& path) {
+  std::ifstream f(path, std::ios::binary);
+  if (!f) throw std::runtime_error("cannot open " + path);
+  std::vector<float> p(hams_surrogate_param_count());
+  f.read(reinterpret_cast<char*>(p.data()), p.size() * sizeof(float));
+  if (f.gcount() != (std::streamsize)(p.size() * sizeof(float))) throw std::runtime_error(path + ": short parameter file");
+  return p;
+}
+
+int usage() {
+  std::fprintf(stderr,
+               "usage: hams_b200_run <inputdir> <outputdir> [--mixed] [--surrogate FILE] [--far F] [--lanes N] "
+               "[--device D]\n");
+  return 2;
+}
+
+}  // namespace
+
+int main(int argc, char** argv) {
+  if (argc < 3) return usage();
+  const std::string in = argv[1], out = argv[2];
+  int precision = HAMS_PREC_FP64, lanes = 0, device = 0;
+  std::string sgfile;
+  double far = 3.0;
+  for (int a = 3; a < argc; ++a) {
+    std::string s = argv[a];
+    if (s == "--mixed") precision = HAMS_PREC_MIXED;
+    else if (s == "--surrogate" && a + 1 < argc) sgfile = argv[++a];
+    else if (s == "--far" && a + 1 < argc) far = std::atof(argv[++a]);
+    else if (s == "--lanes" && a + 1 < argc) lanes = std::atoi(argv[++a]);
+    else if (s == "--device" && a + 1 < argc) device = std::atoi(argv[++a]);
+    else return usage();
+  }
+  try {
+    Deck d = load(in);
+    if (d.isx || d.isy) throw std::runtime_error("geometric symmetry (ISX/ISY != 0) is not built in the GPU path");
+    if (d.isolv == 2) std::fprintf(stderr, "hams_b200_run: Solver_type 2 (GMRES) requested; using the LU solver\n");
+    const int nb = d.nbody, ndof = 6 * nb, nf = (int)d.wvnb.size(), nbeta = (int)d.wvhd.size();
+    const double g = 9.80665;
+    hams_geom geo{};
+    geo.nelem = d.nelem;
+    geo.ntnd = d.ntnd;
+    geo.nbody = nb;
+    geo.xyz = d.xyz.data();
+    geo.ncn = d.ncn.data();
+    geo.ncon = d.ncon.data();
+    geo.xyz_p = d.xyz_p.data();
+    geo.ds = d.ds.data();
+    geo.pnsz = d.pnsz.data();
+    geo.dxyz = d.dxyz.data();
+    geo.body_nelem = d.body_nelem.data();
+    geo.inelem = d.inelem;
+    geo.ixyz_p = d.inelem ? d.ixyz_p.data() : nullptr;
+    hams_opts o{};
+    o.depth = d.h;
+    o.rho = 1000.0;
+    o.g = g;
+    o.amp = 1.0;
+    o.isol = d.isol;
+    o.irsp = d.irsp;
+    o.precision = precision;
+    o.device = device;
+    o.batch_lanes = lanes;
+    hams_ctx* ctx = nullptr;
+    if (hams_ctx_create(&geo, &o, &ctx)) throw std::runtime_error(std::string("context: ") + hams_last_error());
+    if (!sgfile.empty()) {
+      auto p = read_params(sgfile);
+      if (hams_ctx_set_surrogate(ctx, p.data(), (int32_t)p.size(), far))
+        throw std::runtime_error(std::string("surrogate: ") + hams_last_error());
+    }
+    std::vector<hams_wave> waves(nf);
+    for (int k = 0; k < nf; ++k)
+      if (hams_wave_properties(d.inft, d.wvnb[k], d.h, g, d.sybo == 1 && k < 2 ? k + 1 : 0, &waves[k]))
+        throw std::runtime_error(std::string("wave properties: ") + hams_last_error());
+    std::vector<double> beta(nbeta);
+    for (int i = 0; i < nbeta; ++i) beta[i] = d.wvhd[i] * kPi / 180.0;
+    std::vector<double> amas((size_t)nf * ndof * ndof), bdmp(amas.size()), exfc(2 * (size_t)nf * std::max(nbeta, 1) * ndof);
+    int rc = hams_solve_batch(ctx, nf, waves.data(), nbeta, beta.data(), amas.data(), bdmp.data(), exfc.data());
+    hams_ctx_destroy(ctx);
+    if (rc < 0) throw std::runtime_error(std::string("solve: ") + hams_last_error());
+    if (rc > 0) std::fprintf(stderr, "hams_b200_run: singular pivot %d\n", rc);
+    const std::string hd = out + "/Hams_format";
+    mkdir(out.c_str(), 0755);
+    mkdir(hd.c_str(), 0755);
+    for (int md = 0; md < 6; ++md) {
+      const std::string s = std::to_string(md + 1) + ".txt";
+      std::ofstream fa(hd + "/OAMASS" + s), fd(hd + "/ODAMPING" + s), fx(hd + "/OEXFOR" + s);
+      if (!fa || !fd || !fx) throw std::runtime_error("cannot write to " + hd);
+      char head[64];
+      for (int k = 0; k < nf; ++k) {
+        std::snprintf(head, sizeof(head), "%7.3f %7.3f ", waves[k].wk, waves[k].w1);
+        // RFORCE_MULTI: body pairs (M, N), row 6M + md, six columns of body N
+        for (int b1 = 0; b1 < nb; ++b1)
+          for (int b2 = 0; b2 < nb; ++b2) {
+            fa << head;
+            fd << head;
+            for (int c = 0; c < 6; ++c) {
+              const size_t e = k + (size_t)nf * ((6 * b1 + md) + (size_t)ndof * (6 * b2 + c));
+              fa << fmt_e(14, 5, amas[e]);
+              fd << fmt_e(14, 5, bdmp[e]);
+            }
+            fa << '\n';
+            fd << '\n';
+          }
+        // EFORCE_MULTI: headings outer, bodies inner
+        for (int ib = 0; ib < nbeta; ++ib)
+          for (int b1 = 0; b1 < nb; ++b1) {
+            const size_t e = k + (size_t)nf * (ib + (size_t)nbeta * (6 * b1 + md));
+            fx << head << fmt_e(14, 6, exfc[2 * e]) << fmt_e(14, 6, exfc[2 * e + 1]) << '\n';
+          }
+      }
+    }
+    std::printf("hams_b200_run: %d frequencies, %d headings, %d panels, %d bodies -> %s\n", nf, nbeta, d.nelem, nb,
+                hd.c_str());
+  } catch (const std::exception& e) {
+    std::fprintf(stderr, "hams_b200_run: %s\n", e.what());
+    return 1;
+  }
+  return 0;
+}
