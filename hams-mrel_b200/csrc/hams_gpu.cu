@@ -519,6 +519,7 @@ struct hams_ctx {
   SgDev sgd{};
   int sms = 148;
   int sg_used = 0;  // the last solve evaluated its far pairs with the surrogate
+  std::string note;  // what the last solve changed on its own (fallbacks), or empty
 };
 
 static int launch_check(hams_ctx* c, int count = 1) {
@@ -888,7 +889,9 @@ static int mixed_solve(hams_ctx* c, double2* M, const double2* rhs, int ldr, int
     int rc = mixed_lu_factor(c->st, c->blas, ct, n, c->Af.p, c->perm.p, c->luw.p, c->info.p, &la, &lb);
     c->launches += la;
     c->lib_calls += lb;
-    if (rc) return fail(HAMS_ERR_NUMERIC, "block LU: %s failed", rc == 1 ? "CUDA" : "cuBLAS");
+    if (rc == 1) return fail(HAMS_ERR_NUMERIC, "block LU: CUDA failed");
+    if (rc) return fail(HAMS_ERR_NUMERIC, "block LU: cuBLAS status %d in GEMM %d of block %d", rc % 100, rc % 1000 / 100,
+                        rc / 1000);
     int zp = 0;
     CU(cudaMemcpyAsync(&zp, c->info.p, sizeof(int), cudaMemcpyDeviceToHost, c->st));
     CU(cudaStreamSynchronize(c->st));
@@ -994,11 +997,20 @@ static int solve_dev(hams_ctx* c, int nrhs, int* info_host) {
   // mixed: complex64 LU of a rounded copy + FP64 iterative refinement; the
   // block LU falls back to the library's partially pivoted LU when its
   // refinement does not converge
-  const int kind = c->opts.lu_kind;
+  int kind = c->opts.lu_kind;
+  c->note.clear();
+  if (kind == HAMS_LU_BLOCK_EMU) {
+    int ver = 0;
+    if (cublasGetVersion(c->blas, &ver) != CUBLAS_STATUS_SUCCESS || ver < 120900) {
+      kind = HAMS_LU_BLOCK_TF32;  // FP32 emulation on BF16 tensor cores arrived with cuBLAS 12.9
+      c->note = "cuBLAS " + std::to_string(ver) + " has no BF16x9 emulation: block LU on TF32";
+    }
+  }
   if (kind == HAMS_LU_BLOCK_EMU || kind == HAMS_LU_BLOCK_TF32) {
     int rc = mixed_solve(c, M, rhs, ldr, nrhs, kind, info_host);
     if (rc == 0) return 0;
     if (rc != HAMS_ERR_NUMERIC) return rc;
+    c->note += (c->note.empty() ? "" : "; ") + std::string("block LU replaced by the library LU: ") + g_err;
     g_err.clear();
   }
   return mixed_solve(c, M, rhs, ldr, nrhs, HAMS_LU_LIBRARY, info_host);
@@ -1309,6 +1321,8 @@ extern "C" int hams_last_timings(hams_ctx* c, double* ms, int32_t n) {
   for (int i = 0; i < k; ++i) ms[i] = c->last_ms[i];
   return k;
 }
+
+extern "C" const char* hams_last_note(hams_ctx* c) { return c ? c->note.c_str() : ""; }
 
 extern "C" int64_t hams_launch_count(hams_ctx* c) {
   if (!c) return 0;

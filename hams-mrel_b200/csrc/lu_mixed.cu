@@ -287,9 +287,13 @@ int mixed_lu_factor(cudaStream_t st, cublasHandle_t blas, cublasComputeType_t ct
     float* Akj = Ar + (size_t)k1 * 2 * n + 2 * k0;  // real 2nbk x w, ld 2n
     float* Aij = Ar + (size_t)k1 * 2 * n + 2 * k1;  // real 2w x w, ld 2n
     // U_kj = L_kk^-1 A_kj;  L_ik^ = A_ik^ U_kk^-1^;  A_ij -= L_ik U_kj
-    if (sgemm(blas, ct, k2, w, k2, 1.0f, invL, K2, Akj, 2 * n, 0.0f, W1, K2) != CUBLAS_STATUS_SUCCESS) return 2;
-    if (sgemm(blas, ct, 2 * w, k2, k2, 1.0f, Ehat, 2 * w, invU, K2, 0.0f, Lhat, 2 * w) != CUBLAS_STATUS_SUCCESS) return 2;
-    if (sgemm(blas, ct, 2 * w, w, k2, -1.0f, Lhat, 2 * w, W1, K2, 1.0f, Aij, 2 * n) != CUBLAS_STATUS_SUCCESS) return 2;
+    cublasStatus_t bs;
+    if ((bs = sgemm(blas, ct, k2, w, k2, 1.0f, invL, K2, Akj, 2 * n, 0.0f, W1, K2)) != CUBLAS_STATUS_SUCCESS)
+      return 100 + 1000 * b + (int)bs;
+    if ((bs = sgemm(blas, ct, 2 * w, k2, k2, 1.0f, Ehat, 2 * w, invU, K2, 0.0f, Lhat, 2 * w)) != CUBLAS_STATUS_SUCCESS)
+      return 200 + 1000 * b + (int)bs;
+    if ((bs = sgemm(blas, ct, 2 * w, w, k2, -1.0f, Lhat, 2 * w, W1, K2, 1.0f, Aij, 2 * n)) != CUBLAS_STATUS_SUCCESS)
+      return 300 + 1000 * b + (int)bs;
     *lib_calls += 3;
     // U_kj back into A; L_ik = the even columns of L_ik^
     if (cudaMemcpy2DAsync(Akj, (size_t)2 * n * 4, W1, (size_t)K2 * 4, (size_t)k2 * 4, w, cudaMemcpyDeviceToDevice, st) !=

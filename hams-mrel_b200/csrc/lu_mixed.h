@@ -10,7 +10,8 @@ size_t mixed_lu_workspace_elems(int n);
 // P block diagonal (pivoting inside each 64-row diagonal block); perm (n)
 // receives the permutation as source rows, dinfo 1 + the first column with
 // a zero pivot (or a large value if none).  GEMMs run on cuBLAS with compute
-// type ct.  Returns 0, 1 on a CUDA error, 2 on a cuBLAS error.
+// type ct.  Returns 0, 1 on a CUDA error, or 100 g + 1000 b + status for a
+// cuBLAS error of GEMM g (1-3) at block b.
 int mixed_lu_factor(cudaStream_t st, cublasHandle_t blas, cublasComputeType_t ct, int n, float2* A, int* perm,
                     float2* work, int* dinfo, long long* launches, long long* lib_calls);
 

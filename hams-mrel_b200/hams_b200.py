@@ -19,7 +19,7 @@ LIB_PATH = os.path.join(_HERE, "libhams_b200.so")
 HAMS_NK = 200
 PREC_FP64 = 0
 PREC_MIXED = 1
-LU_BLOCK_EMU, LU_BLOCK_TF32, LU_LIBRARY = 0, 1, 2
+LU_BLOCK_TF32, LU_BLOCK_EMU, LU_LIBRARY = 0, 1, 2
 
 c_int = ctypes.c_int32
 c_dbl = ctypes.c_double
@@ -78,6 +78,8 @@ def load_library(path=LIB_PATH):
     lib.hams_launch_count.argtypes = [ctypes.c_void_p]
     lib.hams_launch_count.restype = ctypes.c_int64
     lib.hams_last_error.restype = ctypes.c_char_p
+    lib.hams_last_note.argtypes = [ctypes.c_void_p]
+    lib.hams_last_note.restype = ctypes.c_char_p
     lib.hams_library_call_count.argtypes = [ctypes.c_void_p]
     lib.hams_library_call_count.restype = ctypes.c_int64
     lib.hams_mark.argtypes = [ctypes.c_void_p, c_int]
@@ -238,6 +240,10 @@ class Context:
             return
         self._sg = np.ascontiguousarray(params, dtype=np.float32)
         _check(lib.hams_ctx_set_surrogate(self._h, _f(self._sg), self._sg.size, float(far_factor)))
+
+    def note(self):
+        """What the last solve decided on its own (e.g. a fallback to the library LU), or ''."""
+        return load_library().hams_last_note(self._h).decode()
 
     def launch_count(self):
         """Kernels of this library launched so far on this context."""

@@ -41,10 +41,12 @@ enum {
 /* Complex64 factorisation of the mixed form.  BLOCK: 64-row blocks pivoted
  * inside each diagonal block, the complex products as real GEMMs on the
  * tensor cores with FP32 accumulation -- inputs rounded to TF32
- * (BLOCK_TF32) or FP32 emulated on BF16 tensor cores (BLOCK_EMU); the
- * library's partially pivoted LU (LIBRARY) is also the fallback when the
- * refinement of a block factorisation does not converge. */
-enum { HAMS_LU_BLOCK_EMU = 0, HAMS_LU_BLOCK_TF32 = 1, HAMS_LU_LIBRARY = 2 };
+ * (BLOCK_TF32, the default) or FP32 emulated on BF16 tensor cores
+ * (BLOCK_EMU, needs the cuBLAS 12.9 emulation; with an older cuBLAS loaded
+ * in the process it runs as BLOCK_TF32); the library's partially pivoted LU
+ * (LIBRARY) is also the fallback when the refinement of a block
+ * factorisation does not converge. */
+enum { HAMS_LU_BLOCK_TF32 = 0, HAMS_LU_BLOCK_EMU = 1, HAMS_LU_LIBRARY = 2 };
 
 /* Numerical form of a solve. */
 enum {
@@ -86,7 +88,7 @@ typedef struct hams_opts {
   int32_t device;   /* CUDA device ordinal                                       */
   double refine_tol;/* mixed: relative residual target of the refinement (<=0: 1e-12) */
   int32_t refine_max;/* mixed: refinement sweeps (<=0: 30)                       */
-  int32_t lu_kind;  /* mixed: HAMS_LU_BLOCK_EMU (0), HAMS_LU_BLOCK_TF32, HAMS_LU_LIBRARY */
+  int32_t lu_kind;  /* mixed: HAMS_LU_BLOCK_TF32 (0), HAMS_LU_BLOCK_EMU, HAMS_LU_LIBRARY */
   int32_t batch_lanes;/* hams_solve_batch: frequencies in flight (<=0: 4)          */
   int32_t reserved[5];
 } hams_opts;
@@ -229,6 +231,10 @@ int hams_ctx_set_surrogate(hams_ctx *ctx, const float *params, int32_t nparams, 
  * (or the series standing in for it), [17] pairs the surrogate evaluated.
  * n is the capacity of ms (18 fills all). Returns the number written. */
 int hams_last_timings(hams_ctx *ctx, double *ms, int32_t n);
+
+/* What the last solve of ctx decided on its own, e.g. the reason it fell back
+ * from the block LU to the library LU; empty when nothing. */
+const char *hams_last_note(hams_ctx *ctx);
 
 /* Kernels of this library launched since the context was created (library
  * calls into cuBLAS / cuSOLVER / CUB are counted by hams_library_call_count). */

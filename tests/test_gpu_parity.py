@@ -137,7 +137,10 @@ def test_mixed_precision_config1(lu_kind):
     betas = np.radians(d["wvhd"])
     for omega in d["wvnb"]:
         am, bd, ex = ctx.solve_frequency(hams_b200.wave_properties(omega, d["h"], 9.80665), betas)
-        assert ctx.timings()["lu_used"] == lu_kind  # no fallback to the library LU
+        used = ctx.timings()["lu_used"]
+        # no fallback to the library LU (the emulated GEMM runs as TF32 under a cuBLAS older than 12.9)
+        assert used == lu_kind or (lu_kind == hams_b200.LU_BLOCK_EMU and used == hams_b200.LU_BLOCK_TF32
+                                   and "emulation" in ctx.note()), ctx.note()
         oam, obd, oex, _ = oc.solve(oc.wave(omega), betas)
         assert rel(am, oam) < 1e-6 and rel(bd, obd) < 1e-6 and rel(ex, oex) < 1e-6
 
@@ -159,7 +162,10 @@ def test_mixed_block_lu_array(lu_kind):
     for omega in (0.4, 1.6):
         am, bd, ex = ctx.solve_frequency(hams_b200.wave_properties(omega, 40.0, 9.81), betas)
         t = ctx.timings()
-        assert t["lu_used"] == lu_kind and t["refine_sweeps"] <= (4 if lu_kind == hams_b200.LU_BLOCK_EMU else 12)
+        used = t["lu_used"]
+        assert used == lu_kind or (lu_kind == hams_b200.LU_BLOCK_EMU and used == hams_b200.LU_BLOCK_TF32
+                                   and "emulation" in ctx.note()), ctx.note()
+        assert t["refine_sweeps"] <= (4 if used == hams_b200.LU_BLOCK_EMU else 12)
         oam, obd, oex, _ = oc.solve(oc.wave(omega), betas)
         assert rel(am, oam) < 1e-7 and rel(bd, obd) < 1e-7 and rel(ex, oex) < 1e-7
     ctx.close()
