@@ -381,7 +381,6 @@ int main(int argc, char** argv) {
   try {
     Deck d = load(in);
     if (d.isx || d.isy) throw std::runtime_error("geometric symmetry (ISX/ISY != 0) is not built in the GPU path");
-    if (d.isolv == 2) std::fprintf(stderr, "hams_b200_run: Solver_type 2 (GMRES) requested; using the LU solver\n");
     const int nb = d.nbody, ndof = 6 * nb, nf = (int)d.wvnb.size(), nbeta = (int)d.wvhd.size();
     const double g = 9.80665;
     hams_geom geo{};
@@ -408,6 +407,7 @@ int main(int argc, char** argv) {
     o.precision = precision;
     o.device = device;
     o.batch_lanes = lanes;
+    o.solver = d.isolv == 2 ? HAMS_SOLVER_GMRES : HAMS_SOLVER_LU;
     hams_ctx* ctx = nullptr;
     if (hams_ctx_create(&geo, &o, &ctx)) throw std::runtime_error(std::string("context: ") + hams_last_error());
     if (!sgfile.empty()) {
@@ -423,6 +423,7 @@ int main(int argc, char** argv) {
     for (int i = 0; i < nbeta; ++i) beta[i] = d.wvhd[i] * kPi / 180.0;
     std::vector<double> amas((size_t)nf * ndof * ndof), bdmp(amas.size()), exfc(2 * (size_t)nf * std::max(nbeta, 1) * ndof);
     int rc = hams_solve_batch(ctx, nf, waves.data(), nbeta, beta.data(), amas.data(), bdmp.data(), exfc.data());
+    if (rc >= 0 && *hams_last_note(ctx)) std::fprintf(stderr, "hams_b200_run: %s\n", hams_last_note(ctx));
     hams_ctx_destroy(ctx);
     if (rc < 0) throw std::runtime_error(std::string("solve: ") + hams_last_error());
     if (rc > 0) std::fprintf(stderr, "hams_b200_run: singular pivot %d\n", rc);

@@ -30,6 +30,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <complex>
 #include <cstring>
 #include <mutex>
 #include <thread>
@@ -399,6 +400,53 @@ __global__ void k_c2z(const float2* __restrict__ a, double2* __restrict__ b, siz
   for (; t < n; t += (size_t)gridDim.x * blockDim.x) b[t] = make_double2((double)a[t].x, (double)a[t].y);
 }
 // per-column max |r| / max |b| ratios -> out[col]
+// d[i] = M[i, i], or 1 where |M[i, i]| < 1e-30 (IterativeSolvers.f90:166-171)
+__global__ void k_jacobi_setup(const double2* __restrict__ M, int n, double2* __restrict__ d) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double2 v = M[i + (size_t)i * n];
+  d[i] = hypot(v.x, v.y) < 1e-30 ? make_double2(1.0, 0.0) : v;
+}
+
+// Z[i + n c] /= d[i]
+__global__ void k_jacobi_apply(const double2* __restrict__ d, int n, int ncol, double2* __restrict__ Z) {
+  size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= (size_t)n * ncol) return;
+  const double2 a = d[e % n], z = Z[e];
+  const double den = a.x * a.x + a.y * a.y;
+  Z[e] = make_double2((z.x * a.x + z.y * a.y) / den, (z.y * a.x - z.x * a.y) / den);
+}
+
+// out[c] = 2-norm of column c of W (n x ncol, ld n)
+__global__ void k_colnorm2(const double2* __restrict__ W, int n, double* __restrict__ out) {
+  const int col = blockIdx.x;
+  double s = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    double2 v = W[i + (size_t)col * n];
+    s += v.x * v.x + v.y * v.y;
+  }
+  __shared__ double sh[256];
+  sh[threadIdx.x] = s;
+  __syncthreads();
+  for (int k = blockDim.x / 2; k > 0; k >>= 1) {
+    if (threadIdx.x < k) sh[threadIdx.x] += sh[threadIdx.x + k];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[col] = sqrt(sh[0]);
+}
+
+// dst[i + dstride c] = W[i + n c] / nrm[c], zero where nrm[c] <= 1e-30
+// (IterativeSolvers.f90:412-416)
+__global__ void k_normalize_into(const double2* __restrict__ W, int n, int ncol, const double* __restrict__ nrm,
+                                 double2* __restrict__ dst, size_t dstride) {
+  size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= (size_t)n * ncol) return;
+  const int c = (int)(e / n), i = (int)(e % n);
+  const double s = nrm[c] > 1e-30 ? 1.0 / nrm[c] : 0.0;
+  const double2 v = W[e];
+  dst[i + dstride * c] = make_double2(v.x * s, v.y * s);
+}
+
 __global__ void k_colnorm_ratio(const double2* __restrict__ r, const double2* __restrict__ b, int n, int ld,
                                 double* __restrict__ out) {
   int col = blockIdx.x;
@@ -488,6 +536,9 @@ struct hams_ctx {
   // per-frequency buffers
   DBuf<double2> A, S, B, part, wd, C, D, X, R;
   DBuf<float2> Af, Xf, luw;
+  DBuf<double2> gv, gw, gz, gy, gpre;  // GMRES: Krylov basis, work, preconditioned, coefficients, body blocks
+  DBuf<double> gnrm;
+  DBuf<int> gpiv;
   DBuf<int> perm;
   int lu_used = -1;  // mixed form: factorisation used by the last solve (HAMS_LU_*)
   DBuf<double> wvn, beta, outbuf, colratio;
@@ -754,6 +805,7 @@ extern "C" int hams_ctx_create(const hams_geom* geo, const hams_opts* opts, hams
   if (opts->irsp == 1 && (geo->inelem <= 0 || !geo->ixyz_p)) return fail(HAMS_ERR_ARG, "irsp=1 needs water-plane panels");
   if (opts->precision != HAMS_PREC_FP64 && opts->precision != HAMS_PREC_MIXED)
     return fail(HAMS_ERR_ARG, "unknown precision %d", opts->precision);
+  if (opts->solver < 0 || opts->solver > HAMS_SOLVER_GMRES) return fail(HAMS_ERR_ARG, "unknown solver %d", opts->solver);
   hams_ctx* c = new hams_ctx();
   c->opts = *opts;
   c->dev = opts->device;
@@ -960,6 +1012,213 @@ static int mixed_solve(hams_ctx* c, double2* M, const double2* rhs, int ldr, int
   return 0;
 }
 
+// GMRES (IterativeSolvers.f90:324-484, ZGMRES_SOLVE): X (n x nrhs) from the
+// FP64 matrix M and the right-hand sides rhs, every column from zero,
+// restarted every m steps, right-preconditioned by the LU factors of each
+// body's diagonal block (:176-253) or, with one body, by the diagonal
+// (:154-174).  All columns advance together: one ZGEMM per step, classical
+// Gram-Schmidt applied twice as strided-batched GEMVs (the reference's
+// modified Gram-Schmidt one vector at a time, :399-406), the small
+// Hessenberg least-squares problems (Givens rotations) on the host.  A column
+// that misses the tolerance after gmres_maxit steps keeps its last iterate
+// and the solve's note says so (:475-480).
+static int gmres_solve(hams_ctx* c, double2* M, const double2* rhs, int nrhs) {
+  const int n = c->n, nb = c->nb;
+  const int m = c->opts.gmres_restart > 0 ? c->opts.gmres_restart : 25;
+  const int maxit = c->opts.gmres_maxit > 0 ? c->opts.gmres_maxit : 100;
+  const double tol = c->opts.gmres_tol > 0.0 ? c->opts.gmres_tol : 1e-4;
+  const cuDoubleComplex one = make_cuDoubleComplex(1.0, 0.0), zero = make_cuDoubleComplex(0.0, 0.0),
+                        mone = make_cuDoubleComplex(-1.0, 0.0);
+  const size_t vs = (size_t)n * (m + 1);  // basis stride of one column
+  TRY(c->gv.alloc(vs * nrhs));
+  TRY(c->gw.alloc((size_t)n * nrhs));
+  TRY(c->gz.alloc((size_t)n * nrhs));
+  TRY(c->gy.alloc((size_t)(m + 1) * nrhs));
+  TRY(c->gnrm.alloc(nrhs));
+  // preconditioner: LU of each body's diagonal block, packed one after
+  // another, or the diagonal of M with one body
+  std::vector<size_t> boff(nb + 1, 0);
+  std::vector<int> bst(nb + 1, 0);
+  for (int b = 0; b < nb; ++b) {
+    bst[b + 1] = bst[b] + c->body_nelem[b];
+    boff[b + 1] = boff[b] + (size_t)c->body_nelem[b] * c->body_nelem[b];
+  }
+  TRY(c->gpiv.alloc(n));
+  if (nb == 1) {
+    TRY(c->gpre.alloc(n));
+    k_jacobi_setup<<<(n + 255) / 256, 256, 0, c->st>>>(M, n, c->gpre.p);
+    TRY(launch_check(c));
+  } else {
+    TRY(c->gpre.alloc(boff[nb]));
+    int lwmax = 0;
+    for (int b = 0; b < nb; ++b) {
+      const int nn = c->body_nelem[b];
+      CU(cudaMemcpy2DAsync(c->gpre.p + boff[b], (size_t)nn * 16, M + bst[b] + (size_t)bst[b] * n, (size_t)n * 16,
+                           (size_t)nn * 16, nn, cudaMemcpyDeviceToDevice, c->st));
+      int lw = 0;
+      CUS(cusolverDnZgetrf_bufferSize(c->solver, nn, nn, (cuDoubleComplex*)(c->gpre.p + boff[b]), nn, &lw));
+      lwmax = std::max(lwmax, lw);
+    }
+    TRY(c->work.alloc((size_t)lwmax * sizeof(cuDoubleComplex)));
+    for (int b = 0; b < nb; ++b) {
+      const int nn = c->body_nelem[b];
+      CUS(cusolverDnZgetrf(c->solver, nn, nn, (cuDoubleComplex*)(c->gpre.p + boff[b]), nn,
+                           (cuDoubleComplex*)c->work.p, c->gpiv.p + bst[b], c->info.p));
+    }
+    c->lib_calls += 2 * nb;
+  }
+  CU(cudaEventRecord(c->evf, c->st));
+  auto precond = [&](double2* Z) -> int {  // Z (n x nrhs) <- P^-1 Z
+    if (nb == 1) {
+      k_jacobi_apply<<<(unsigned)(((size_t)n * nrhs + 255) / 256), 256, 0, c->st>>>(c->gpre.p, n, nrhs, Z);
+      return launch_check(c);
+    }
+    for (int b = 0; b < nb; ++b) {
+      const int nn = c->body_nelem[b];
+      CUS(cusolverDnZgetrs(c->solver, CUBLAS_OP_N, nn, nrhs, (cuDoubleComplex*)(c->gpre.p + boff[b]), nn,
+                           c->gpiv.p + bst[b], (cuDoubleComplex*)(Z + bst[b]), n, c->info.p));
+    }
+    c->lib_calls += nb;
+    return 0;
+  };
+  // right-hand-side norms
+  k_colnorm2<<<nrhs, 256, 0, c->st>>>(rhs, n, c->gnrm.p);
+  TRY(launch_check(c));
+  std::vector<double> bnorm(nrhs), nr(nrhs);
+  CU(cudaMemcpyAsync(bnorm.data(), c->gnrm.p, nrhs * 8, cudaMemcpyDeviceToHost, c->st));
+  CU(cudaMemsetAsync(c->X.p, 0, (size_t)n * nrhs * 16, c->st));
+  CU(cudaMemcpyAsync(c->gw.p, rhs, (size_t)n * nrhs * 16, cudaMemcpyDeviceToDevice, c->st));  // R = B - A 0
+  CU(cudaStreamSynchronize(c->st));
+  typedef std::complex<double> zc;
+  std::vector<zc> H((size_t)(m + 1) * m * nrhs), g((size_t)(m + 1) * nrhs), sn((size_t)m * nrhs);
+  std::vector<double> cr((size_t)m * nrhs), beta(nrhs);
+  std::vector<zc> hcol((size_t)(m + 1) * nrhs), y((size_t)(m + 1) * nrhs);
+  int iters = 0;
+  bool done = false;
+  while (!done) {
+    // V_0 = R / |R|
+    k_colnorm2<<<nrhs, 256, 0, c->st>>>(c->gw.p, n, c->gnrm.p);
+    k_normalize_into<<<(unsigned)(((size_t)n * nrhs + 255) / 256), 256, 0, c->st>>>(c->gw.p, n, nrhs, c->gnrm.p,
+                                                                                    c->gv.p, vs);
+    TRY(launch_check(c, 2));
+    CU(cudaMemcpyAsync(beta.data(), c->gnrm.p, nrhs * 8, cudaMemcpyDeviceToHost, c->st));
+    CU(cudaStreamSynchronize(c->st));
+    bool all = true;
+    for (int r = 0; r < nrhs; ++r) {
+      g[(size_t)r * (m + 1)] = beta[r];
+      for (int i = 1; i <= m; ++i) g[(size_t)r * (m + 1) + i] = 0.0;
+      if (beta[r] > tol * bnorm[r]) all = false;
+    }
+    if (all) break;
+    int k = 0;  // Arnoldi steps done in this cycle
+    for (int j = 0; j < m && iters < maxit; ++j, ++k, ++iters) {
+      // W = A M^-1 V_j
+      CU(cudaMemcpy2DAsync(c->gz.p, (size_t)n * 16, c->gv.p + (size_t)j * n, vs * 16, (size_t)n * 16, nrhs,
+                           cudaMemcpyDeviceToDevice, c->st));
+      TRY(precond(c->gz.p));
+      CUB_(cublasZgemm(c->blas, CUBLAS_OP_N, CUBLAS_OP_N, n, nrhs, n, &one, (cuDoubleComplex*)M, n,
+                       (cuDoubleComplex*)c->gz.p, n, &zero, (cuDoubleComplex*)c->gw.p, n));
+      c->lib_calls += 1;
+      for (size_t e = 0; e < hcol.size(); ++e) hcol[e] = 0.0;
+      for (int pass = 0; pass < 2; ++pass) {  // classical Gram-Schmidt, twice
+        CUB_(cublasZgemvStridedBatched(c->blas, CUBLAS_OP_C, n, j + 1, &one, (cuDoubleComplex*)c->gv.p, n, (long long)vs,
+                                       (cuDoubleComplex*)c->gw.p, 1, n, &zero, (cuDoubleComplex*)c->gy.p, 1, m + 1,
+                                       nrhs));
+        CUB_(cublasZgemvStridedBatched(c->blas, CUBLAS_OP_N, n, j + 1, &mone, (cuDoubleComplex*)c->gv.p, n, (long long)vs,
+                                       (cuDoubleComplex*)c->gy.p, 1, m + 1, &one, (cuDoubleComplex*)c->gw.p, 1, n,
+                                       nrhs));
+        c->lib_calls += 2;
+        CU(cudaMemcpyAsync(y.data(), c->gy.p, (size_t)(m + 1) * nrhs * 16, cudaMemcpyDeviceToHost, c->st));
+        CU(cudaStreamSynchronize(c->st));
+        for (int r = 0; r < nrhs; ++r)
+          for (int i = 0; i <= j; ++i) hcol[(size_t)r * (m + 1) + i] += y[(size_t)r * (m + 1) + i];
+      }
+      k_colnorm2<<<nrhs, 256, 0, c->st>>>(c->gw.p, n, c->gnrm.p);
+      k_normalize_into<<<(unsigned)(((size_t)n * nrhs + 255) / 256), 256, 0, c->st>>>(
+          c->gw.p, n, nrhs, c->gnrm.p, c->gv.p + (size_t)(j + 1) * n, vs);
+      TRY(launch_check(c, 2));
+      CU(cudaMemcpyAsync(nr.data(), c->gnrm.p, nrhs * 8, cudaMemcpyDeviceToHost, c->st));
+      CU(cudaStreamSynchronize(c->st));
+      all = true;
+      for (int r = 0; r < nrhs; ++r) {
+        zc* h = &hcol[(size_t)r * (m + 1)];
+        h[j + 1] = nr[r];
+        for (int i = 0; i < j; ++i) {  // earlier rotations
+          const size_t q = (size_t)r * m + i;
+          zc a = h[i], b = h[i + 1];
+          h[i] = cr[q] * a + sn[q] * b;
+          h[i + 1] = -std::conj(sn[q]) * a + cr[q] * b;
+        }
+        // complex Givens rotation: cr real, [cr sn; -conj(sn) cr] (h_j, h_j+1) = (rho, 0)
+        const double aa = std::abs(h[j]), bb = std::abs(h[j + 1]), rho = std::hypot(aa, bb);
+        const size_t q = (size_t)r * m + j;
+        if (bb < 1e-30) {
+          cr[q] = 1.0;
+          sn[q] = 0.0;
+        } else if (aa < 1e-30) {
+          cr[q] = 0.0;
+          sn[q] = std::conj(h[j + 1]) / bb;
+        } else {
+          cr[q] = aa / rho;
+          sn[q] = (h[j] / aa) * std::conj(h[j + 1]) / rho;
+        }
+        const zc gj = g[(size_t)r * (m + 1) + j];
+        g[(size_t)r * (m + 1) + j] = cr[q] * gj;
+        g[(size_t)r * (m + 1) + j + 1] = -std::conj(sn[q]) * gj;
+        h[j] = cr[q] * h[j] + sn[q] * h[j + 1];
+        h[j + 1] = 0.0;
+        for (int i = 0; i <= j; ++i) H[((size_t)r * m + j) * (m + 1) + i] = h[i];
+        if (std::abs(g[(size_t)r * (m + 1) + j + 1]) > tol * bnorm[r]) all = false;
+      }
+      if (all) {
+        ++k;
+        ++iters;
+        break;
+      }
+    }
+    if (k == 0) return fail(HAMS_ERR_NUMERIC, "GMRES: no progress");
+    // y = R^-1 g per column, X += M^-1 (V y)
+    for (int r = 0; r < nrhs; ++r) {
+      zc* yr = &y[(size_t)r * (m + 1)];
+      for (int i = k - 1; i >= 0; --i) {
+        zc s = g[(size_t)r * (m + 1) + i];
+        for (int l = i + 1; l < k; ++l) s -= H[((size_t)r * m + l) * (m + 1) + i] * yr[l];
+        const zc d = H[((size_t)r * m + i) * (m + 1) + i];
+        yr[i] = std::abs(d) < 1e-30 ? 0.0 : s / d;
+      }
+      for (int i = k; i <= m; ++i) yr[i] = 0.0;
+    }
+    CU(cudaMemcpyAsync(c->gy.p, y.data(), (size_t)(m + 1) * nrhs * 16, cudaMemcpyHostToDevice, c->st));
+    CUB_(cublasZgemvStridedBatched(c->blas, CUBLAS_OP_N, n, k, &one, (cuDoubleComplex*)c->gv.p, n, (long long)vs,
+                                   (cuDoubleComplex*)c->gy.p, 1, m + 1, &zero, (cuDoubleComplex*)c->gz.p, 1, n, nrhs));
+    c->lib_calls += 1;
+    TRY(precond(c->gz.p));
+    CUB_(cublasZaxpy(c->blas, n * nrhs, &one, (cuDoubleComplex*)c->gz.p, 1, (cuDoubleComplex*)c->X.p, 1));
+    // true residual R = B - A X for the next cycle and the stop test
+    CU(cudaMemcpyAsync(c->gw.p, rhs, (size_t)n * nrhs * 16, cudaMemcpyDeviceToDevice, c->st));
+    CUB_(cublasZgemm(c->blas, CUBLAS_OP_N, CUBLAS_OP_N, n, nrhs, n, &mone, (cuDoubleComplex*)M, n,
+                     (cuDoubleComplex*)c->X.p, n, &one, (cuDoubleComplex*)c->gw.p, n));
+    c->lib_calls += 3;
+    if (iters >= maxit) {
+      k_colnorm2<<<nrhs, 256, 0, c->st>>>(c->gw.p, n, c->gnrm.p);
+      TRY(launch_check(c));
+      CU(cudaMemcpyAsync(nr.data(), c->gnrm.p, nrhs * 8, cudaMemcpyDeviceToHost, c->st));
+      CU(cudaStreamSynchronize(c->st));
+      double worst = 0.0;
+      for (int r = 0; r < nrhs; ++r) worst = std::max(worst, bnorm[r] > 0 ? nr[r] / bnorm[r] : nr[r]);
+      if (worst > tol) {
+        char buf[128];
+        std::snprintf(buf, sizeof buf, "GMRES: relative residual %.3e after %d steps (tolerance %.1e)", worst, iters,
+                      tol);
+        c->note += (c->note.empty() ? "" : "; ") + std::string(buf);
+      }
+      done = true;
+    }
+  }
+  c->refine_sweeps = iters;
+  return 0;
+}
+
 // Solve on the device: X (n x nrhs) from A, B (or normal equations with lids).
 static int solve_dev(hams_ctx* c, int nrhs, int* info_host) {
   const int n = c->n, tn = c->tn;
@@ -982,6 +1241,10 @@ static int solve_dev(hams_ctx* c, int nrhs, int* info_host) {
   TRY(c->X.alloc((size_t)n * nrhs));
   CU(cudaMemcpy2DAsync(c->X.p, (size_t)n * 16, rhs, (size_t)ldr * 16, (size_t)n * 16, nrhs, cudaMemcpyDeviceToDevice, c->st));
   *info_host = 0;
+  c->note.clear();
+  // with lids GMRES iterates on the normal equations, as the reference does
+  // (AssbMatx_irr.f90:494-498)
+  if (c->opts.solver == HAMS_SOLVER_GMRES) return gmres_solve(c, M, rhs, nrhs);
   if (c->opts.precision == HAMS_PREC_FP64) {
     int lw = 0;
     CUS(cusolverDnZgetrf_bufferSize(c->solver, n, n, (cuDoubleComplex*)M, n, &lw));
@@ -998,7 +1261,6 @@ static int solve_dev(hams_ctx* c, int nrhs, int* info_host) {
   // block LU falls back to the library's partially pivoted LU when its
   // refinement does not converge
   int kind = c->opts.lu_kind;
-  c->note.clear();
   if (kind == HAMS_LU_BLOCK_EMU) {
     int ver = 0;
     if (cublasGetVersion(c->blas, &ver) != CUBLAS_STATUS_SUCCESS || ver < 120900) {
@@ -1063,7 +1325,8 @@ static int solve_one(hams_ctx* c, const hams_wave* w, int nbeta, const double* b
     if (c->opts.depth >= 0.0 && cudaEventElapsedTime(&ms, c->evb[b], c->evb[b + 1]) == cudaSuccess) c->last_ms[5 + b] = ms;
   }
   if (cudaEventElapsedTime(&ms, c->ev[2], c->evf) == cudaSuccess) c->last_ms[9] = ms;
-  c->last_ms[10] = c->opts.precision == HAMS_PREC_MIXED ? (double)c->refine_sweeps : 0.0;
+  c->last_ms[10] = (c->opts.precision == HAMS_PREC_MIXED || c->opts.solver == HAMS_SOLVER_GMRES)
+                       ? (double)c->refine_sweeps : 0.0;
   c->last_ms[15] = c->opts.precision == HAMS_PREC_MIXED ? (double)c->lu_used : -1.0;
   c->last_ms[16] = 0.0;
   if (c->opts.depth >= 0.0 && cudaEventElapsedTime(&ms, c->evb[4], c->evb[5]) == cudaSuccess) c->last_ms[16] = ms;
@@ -1101,7 +1364,7 @@ extern "C" int hams_solve_batch(hams_ctx* c, int32_t nfreq, const hams_wave* wav
   std::vector<hams_ctx*> lane{c};
   for (int t = 0; t + 1 < L; ++t) lane.push_back(c->lanes[t]);
   std::vector<int> rc_of(nfreq, 0), lane_rc(L, 0);
-  std::vector<std::string> lane_err(L);
+  std::vector<std::string> lane_err(L), note_of(nfreq);
   // lane t solves frequencies t, t + L, ... on its own stream and host thread
   auto run = [&](int t) {
     if (cudaSetDevice(c->dev) != cudaSuccess) {
@@ -1118,6 +1381,7 @@ extern "C" int hams_solve_batch(hams_ctx* c, int32_t nfreq, const hams_wave* wav
         return;
       }
       rc_of[k] = rc;
+      note_of[k] = lane[t]->note;
       // scatter into (nfreq, ...) column-major arrays with the frequency index leading
       for (size_t e = 0; e < (size_t)ndof * ndof; ++e) {
         if (amas) amas[k + e * nfreq] = a[e];
@@ -1134,6 +1398,9 @@ extern "C" int hams_solve_batch(hams_ctx* c, int32_t nfreq, const hams_wave* wav
   for (int t = 1; t < L; ++t) th.emplace_back(run, t);
   run(0);
   for (auto& x : th) x.join();
+  c->note.clear();  // the batch's note: each frequency's own, in order
+  for (int k = 0; k < nfreq; ++k)
+    if (!note_of[k].empty()) c->note += (c->note.empty() ? "" : "; ") + ("frequency " + std::to_string(k) + ": ") + note_of[k];
   for (int t = 0; t < L; ++t)
     if (lane_rc[t] < 0) {
       g_err = lane_err[t];

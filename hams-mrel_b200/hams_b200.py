@@ -20,6 +20,7 @@ HAMS_NK = 200
 PREC_FP64 = 0
 PREC_MIXED = 1
 LU_BLOCK_TF32, LU_BLOCK_EMU, LU_LIBRARY = 0, 1, 2
+SOLVER_LU, SOLVER_GMRES = 1, 2
 
 c_int = ctypes.c_int32
 c_dbl = ctypes.c_double
@@ -37,7 +38,8 @@ class HamsOpts(ctypes.Structure):
     _fields_ = [("depth", c_dbl), ("rho", c_dbl), ("g", c_dbl), ("xw", c_dbl * 2), ("amp", c_dbl), ("isol", c_int),
                 ("irsp", c_int), ("precision", c_int), ("device", c_int), ("refine_tol", c_dbl),
                 ("refine_max", c_int), ("lu_kind", c_int), ("batch_lanes", c_int),
-                ("reserved", c_int * 5)]
+                ("solver", c_int), ("gmres_restart", c_int), ("gmres_maxit", c_int), ("gmres_tol", c_dbl),
+                ("reserved", c_int * 4)]
 
 
 class HamsWave(ctypes.Structure):
@@ -146,7 +148,7 @@ class Context:
 
     def __init__(self, geom, depth, rho=1000.0, g=9.80665, isol=1, irsp=0, precision=PREC_FP64, device=0,
                  xw=(0.0, 0.0), amp=1.0, refine_tol=0.0, refine_max=0, lu_kind=0,
-                 batch_lanes=0):
+                 batch_lanes=0, solver=SOLVER_LU, gmres_restart=0, gmres_maxit=0, gmres_tol=0.0):
         lib = load_library()
         self._keep = {}
         f = lambda k, dt: self._keep.setdefault(k, np.asfortranarray(geom[k], dtype=dt))
@@ -165,7 +167,8 @@ class Context:
             g_.ixyz_p = _d(ixyz_p)
         o = HamsOpts(depth=float(depth), rho=float(rho), g=float(g), amp=float(amp), isol=int(isol), irsp=int(irsp),
                      precision=int(precision), device=int(device), refine_tol=float(refine_tol),
-                     refine_max=int(refine_max), lu_kind=int(lu_kind), batch_lanes=int(batch_lanes))
+                     refine_max=int(refine_max), lu_kind=int(lu_kind), batch_lanes=int(batch_lanes), solver=int(solver),
+                     gmres_restart=int(gmres_restart), gmres_maxit=int(gmres_maxit), gmres_tol=float(gmres_tol))
         o.xw[0], o.xw[1] = xw
         self.depth, self.g = float(depth), float(g)
         self._h = ctypes.c_void_p()
@@ -228,6 +231,7 @@ class Context:
         load_library().hams_last_timings(self._h, _d(ms), 18)
         return dict(green=ms[0], rhs=ms[1], solve=ms[2], forces=ms[3], total=ms[4], green_linton=ms[5],
                     green_pidcock=ms[6], green_eigene=ms[7], green_eigen=ms[8], factor=ms[9], refine_sweeps=int(ms[10]),
+                    iterations=int(ms[10]),
                     pairs_linton=int(ms[11]), pairs_pidcock=int(ms[12]), pairs_eigene=int(ms[13]),
                     pairs_eigen=int(ms[14]), lu_used=int(ms[15]), green_surrogate=ms[16],
                     pairs_surrogate=int(ms[17]))

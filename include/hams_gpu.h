@@ -48,6 +48,17 @@ enum {
  * factorisation does not converge. */
 enum { HAMS_LU_BLOCK_TF32 = 0, HAMS_LU_BLOCK_EMU = 1, HAMS_LU_LIBRARY = 2 };
 
+/* Linear solver (ControlFile Solver_type, InputFiles.f90:177-191).  GMRES
+ * (IterativeSolvers.f90:324-484): restarted, right-preconditioned -- by the
+ * LU factors of each body's diagonal block with two or more bodies
+ * (:176-253), by the diagonal with one body (:154-174) -- every right-hand
+ * side from zero, all right-hand sides advanced together (one matrix product
+ * per iteration); FP64 in every precision form.  A solve that misses the
+ * tolerance keeps its last iterate and says so in hams_last_note, as the
+ * reference warns and goes on (:475-480).  With lids (IRSP = 1) it
+ * iterates on the normal equations (AssbMatx_irr.f90:494-498). */
+enum { HAMS_SOLVER_LU = 1, HAMS_SOLVER_GMRES = 2 };
+
 /* Numerical form of a solve. */
 enum {
   HAMS_PREC_FP64 = 0,  /* plain FP64 drop-in: FP64 assembly, FP64 LU           */
@@ -90,7 +101,11 @@ typedef struct hams_opts {
   int32_t refine_max;/* mixed: refinement sweeps (<=0: 30)                       */
   int32_t lu_kind;  /* mixed: HAMS_LU_BLOCK_TF32 (0), HAMS_LU_BLOCK_EMU, HAMS_LU_LIBRARY */
   int32_t batch_lanes;/* hams_solve_batch: frequencies in flight (<=0: 4)          */
-  int32_t reserved[5];
+  int32_t solver;   /* HAMS_SOLVER_LU (0 or 1) or HAMS_SOLVER_GMRES (2), ISOLV     */
+  int32_t gmres_restart;/* GMRES restart length (<=0: 25, IterativeSolvers.f90:56) */
+  int32_t gmres_maxit;  /* GMRES iterations over all restarts (<=0: 100, :58)    */
+  double gmres_tol; /* GMRES relative residual target (<=0: 1e-4, :57)          */
+  int32_t reserved[4];
 } hams_opts;
 
 /* One frequency after CalWaveProperts (ImplementSubs.f90:40): V = w^2/g
@@ -226,14 +241,16 @@ int hams_ctx_set_surrogate(hams_ctx *ctx, const float *params, int32_t nparams, 
  * [1] right-hand sides, [2] factorisation + solves, [3] reductions,
  * [4] whole call, [5..8] Green kernels of the LINTON, PIDCOCK, EIGENE and
  * EIGEN branches (finite depth), [9] LU factorisation, [10] refinement
- * sweeps (mixed form), [11..14] pairs in each branch, [15] the mixed
+ * sweeps (mixed form) or GMRES iterations, [11..14] pairs in each branch, [15] the mixed
  * form's factorisation (HAMS_LU_*; -1 for FP64), [16] the surrogate kernel
  * (or the series standing in for it), [17] pairs the surrogate evaluated.
  * n is the capacity of ms (18 fills all). Returns the number written. */
 int hams_last_timings(hams_ctx *ctx, double *ms, int32_t n);
 
 /* What the last solve of ctx decided on its own, e.g. the reason it fell back
- * from the block LU to the library LU; empty when nothing. */
+ * from the block LU to the library LU, or a GMRES solve that missed its
+ * tolerance; after hams_solve_batch each frequency's note, prefixed by its
+ * index.  Empty when nothing. */
 const char *hams_last_note(hams_ctx *ctx);
 
 /* Kernels of this library launched since the context was created (library

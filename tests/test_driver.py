@@ -6,9 +6,13 @@ OAMASS/ODAMPING/OEXFOR files match the reference's expected files to the
 tolerances the CPU oracle meets (relative Frobenius per file, wave number and
 frequency columns printed identically), and match the oracle's own files to
 1e-7 (config1, example2) / 1e-5 (the lid case example5, whose normal equations
-square the condition number).
+square the condition number).  The config1 deck with Solver_type 2 (GMRES, the
+reference's config1_gmres deck) meets the reference's own GMRES-vs-LU bounds
+(test/test_integration_gmres.f90:48-101: relative Frobenius 1e-3 added mass,
+5e-2 damping).
 """
 import os
+import shutil
 import subprocess
 
 import numpy as np
@@ -67,3 +71,21 @@ def test_driver_reproduces_reference_files(tmp_path, deck, tol_a, tol_b, tol_x, 
             assert head == rhead == ohead
             assert np.linalg.norm(got - ref) / np.linalg.norm(ref) < tol, f"{deck} {kind}{m} vs reference"
             assert np.linalg.norm(got - orc) / np.linalg.norm(orc) < tol_oracle, f"{deck} {kind}{m} vs oracle"
+
+
+@pytest.mark.gpu
+def test_driver_gmres_deck(tmp_path):
+    inp = tmp_path / "input"
+    shutil.copytree(os.path.join(GOLDEN, "config1", "input"), inp)
+    lines = open(inp / "ControlFile.in").read().splitlines()
+    k = next(i for i, l in enumerate(lines) if "Number of threads" in l)
+    lines.insert(k + 1, "    Solver_type              2")
+    open(inp / "ControlFile.in", "w").write("\n".join(lines) + "\n")
+    r = subprocess.run([RUN, str(inp), str(tmp_path / "gpu")], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    for kind, tol in (("OAMASS", 1e-3), ("ODAMPING", 5e-2), ("OEXFOR", 1e-3)):
+        for m in range(1, 7):
+            head, got = _load(tmp_path / "gpu" / "Hams_format" / f"{kind}{m}.txt")
+            rhead, ref = _load(os.path.join(GOLDEN, "config1", "expected", f"{kind}{m}.txt"))
+            assert head == rhead
+            assert np.linalg.norm(got - ref) / np.linalg.norm(ref) < tol, f"GMRES {kind}{m} vs reference LU"
