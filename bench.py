@@ -36,6 +36,12 @@ UNIT = "freq-solves/s"
 RHO, G = 1025.0, 9.81
 LANES = 4  # frequencies in flight in hams_solve_batch (the library's default)
 SG_FAR = 3.0  # surrogate pairs: centre distance beyond 3 source-panel sizes
+# Frequencies the surrogate serves, by K = k0 h tanh(k0 h): on this array the
+# damping below 0.26 rad/s (K < 0.3) and the excitation above 2.05 rad/s
+# (K > 21.5, up to the first irregular frequency of the cylinders, 2.43 rad/s)
+# are small differences of large terms that amplify the network's error past
+# 1e-4; those frequencies keep the series.
+SG_K_RANGE = (0.3, 21.5)
 
 
 def _peaks():
@@ -59,7 +65,7 @@ WORKLOAD = "3x3 cylinder array R=4 T=8 spacing 20 m, 5400 quad panels, depth 50 
 EIGENE_FP64_FLOPS_PER_PAIR = None
 EIGENE_DRAM_BYTES_PER_LAUNCH = None
 # DRAM bytes of one launch of the surrogate kernel on this workload (ncu), or None
-SG_DRAM_BYTES_PER_LAUNCH = 2.909e9  # profiles/k_green_sg_c2_array.md
+SG_DRAM_BYTES_PER_LAUNCH = None
 
 
 def build_case():
@@ -225,7 +231,7 @@ def run_form(hb, dev, geom, case, prec, omegas, betas, warmup, steps, barrier, w
     between two events on the context's stream."""
     ctx = hb.Context(geom, case["depth"], rho=RHO, g=G, precision=prec, device=dev, refine_tol=tol)
     if sg is not None:
-        ctx.set_surrogate(sg, SG_FAR)
+        ctx.set_surrogate(sg, SG_FAR, SG_K_RANGE)
     waves = [hb.wave_properties(om, case["depth"], G) for om in omegas]
     if warmup:  # at least one frequency per lane, so that no lane is created inside the timed region
         ctx.solve_batch([waves[s % len(waves)] for s in range(max(warmup, LANES))], betas)
@@ -246,6 +252,23 @@ def run_form(hb, dev, geom, case, prec, omegas, betas, warmup, steps, barrier, w
     return dict(ms=ms, launches=launches, lib_calls=libcalls, timings=tm, results=results, clocks=clocks)
 
 
+def surrogate_kernel_time(hb, dev, geom, case, betas, sg, tol, reps=5):
+    """Average duration of the surrogate kernel alone (one lane), CUDA events on its stream."""
+    ctx = hb.Context(geom, case["depth"], rho=RHO, g=G, precision=hb.PREC_MIXED, device=dev, refine_tol=tol,
+                     batch_lanes=1)
+    ctx.set_surrogate(sg, SG_FAR, SG_K_RANGE)
+    w = hb.wave_properties(1.2, case["depth"], G)
+    ctx.solve_frequency(w, betas)
+    ms, pairs = [], 0
+    for _ in range(reps):
+        ctx.solve_frequency(w, betas)
+        t = ctx.timings()
+        ms.append(t["green_surrogate"])
+        pairs = t["pairs_surrogate"]
+    ctx.close()
+    return float(np.mean(ms)), int(pairs), None
+
+
 def e2e_form(hb, dev, case, xyz, ncn, ncon, cnt, xr, prec, omegas, betas, steps, barrier, sg=None, tol=0.0):
     """Deck through the C ABI from host buffers: geometry, context, K frequencies."""
     import torch
@@ -256,7 +279,7 @@ def e2e_form(hb, dev, case, xyz, ncn, ncon, cnt, xr, prec, omegas, betas, steps,
     geom = hb.prepare_geometry(xyz, ncn, ncon, cnt, xr)
     ctx = hb.Context(geom, case["depth"], rho=RHO, g=G, precision=prec, device=dev, refine_tol=tol)
     if sg is not None:
-        ctx.set_surrogate(sg, SG_FAR)
+        ctx.set_surrogate(sg, SG_FAR, SG_K_RANGE)
     ctx.solve_batch([hb.wave_properties(omegas[s % len(omegas)], case["depth"], G) for s in range(steps)], betas)
     ctx.close()
     torch.cuda.synchronize()
@@ -271,8 +294,9 @@ def e2e_form(hb, dev, case, xyz, ncn, ncon, cnt, xr, prec, omegas, betas, steps,
 
 
 # forms: precision, surrogate on, dtype, refinement target.  The surrogate form's
-# accuracy is set by the network (~1e-4), so its refinement stops at 1e-8.
-FORMS = {"surrogate": ("mixed", True, "f64 near + f16/f32 MLP far, c64 LU + f64 refinement", 1e-8),
+# accuracy is set by the network (~1e-5 in the outputs), so its refinement
+# stops at a relative residual of 1e-7.
+FORMS = {"surrogate": ("mixed", True, "f64 near + f16/f32 MLP far, c64 LU + f64 refinement", 1e-7),
          "mixed": ("mixed", False, "f64, c64 LU + f64 refinement", 1e-12),
          "fp64": ("fp64", False, "f64", 0.0)}
 
@@ -305,9 +329,11 @@ def gpu_arm(args):
     geom = hb.prepare_geometry(xyz, ncn, ncon, cnt, xr)
     betas = np.radians(case["betas_deg"])
     allom = case["omegas"]
-    # weak scaling: rank r takes the contiguous block r*K ... r*K + K-1 of the repeated sweep
-    lo, hi = shard.block(ws * args.steps, rank, ws)
-    om_rank = np.array([allom[i % len(allom)] for i in range(lo, hi)])
+    # weak scaling: the ws*K solves spread evenly over the sweep (cycling through it when ws*K
+    # exceeds its 40 frequencies), rank r taking every ws-th, so that every K samples the whole range
+    ntot = ws * args.steps
+    pick = (lambda q: (q * len(allom)) // ntot) if ntot <= len(allom) else (lambda q: q % len(allom))
+    om_rank = np.array([allom[pick(rank + ws * s)] for s in range(args.steps)])
     om_warm = np.array([allom[(s * 7 + 3) % len(allom)] for s in range(args.warmup)])
     sgp = train_surrogate.load()
     prec = {"mixed": hb.PREC_MIXED, "fp64": hb.PREC_FP64}
@@ -353,7 +379,9 @@ def gpu_arm(args):
                        "rhs_per_step": 6 * int(cnt.size) + len(betas),
                        "l2": "no flush: the 5400x5400 complex system (0.47 GB) and pair tables exceed the 126 MB L2",
                        "parallelism": f"frequency shards x{ws}, {LANES} frequencies in flight per GPU",
-                       "surrogate": f"far pairs beyond {SG_FAR} panel sizes" if sg_main is not None else None},
+                       "frequencies": "K solves per rank spread evenly over the 40-frequency sweep",
+                       "surrogate": (f"far pairs beyond {SG_FAR} panel sizes, frequencies with K = k0 h tanh(k0 h) in "
+                                     f"[{SG_K_RANGE[0]}, {SG_K_RANGE[1]}]") if sg_main is not None else None},
             "clocks": main["clocks"], "gpu_launches": main["launches"], "library_calls": main["lib_calls"],
             "e2e": {"value": ws * args.steps / e2e_s, "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h,
@@ -364,17 +392,21 @@ def gpu_arm(args):
         line["speedup_vs_fp64"] = value / forms["fp64"]["value"]
         line["rel_err_vs_fp64"] = forms[args.form]["rel_err_vs_fp64"]
     tm = main["timings"]
-    if sg_main is not None and tm["pairs_surrogate"] > 0:
-        # dominant kernel: the surrogate (tensor cores: 3 hidden layers and the padded output layer)
-        flops = 2.0 * (3 * 128 * 128 + 128 * 8)
-        ach = flops * tm["pairs_surrogate"] / (tm["green_surrogate"] * 1e-3) / 1e12
+    if sg_main is not None:
+        # dominant kernel: the surrogate (tensor cores: 3 hidden 128 x 128 layers and the 16-row output
+        # layer per pair), timed alone with CUDA events on one lane at a mid-range frequency
+        flops = 2.0 * (3 * 128 * 128 + 128 * 16)
+        sg_ms, sg_pairs, conc_ms = surrogate_kernel_time(hb, local, geom, case, betas, sg_main, tol_main)
+        ach = flops * sg_pairs / (sg_ms * 1e-3) / 1e12
         peak = PEAKS.get("bf16_tflops")
         line["roofline"] = {"kernel": "k_green_sg", "bound": "tensor", "unit": "TFLOP/s", "achieved": ach,
                             "peak": peak, "frac": ach / peak if peak else None, "traffic": SG_DRAM_BYTES_PER_LAUNCH,
                             "peak_source": "of measured: dense bf16 cuBLAS burst (MEASURED_PEAKS.json); the kernel "
-                                           "runs FP16 mma.sync",
-                            "launch_ms": tm["green_surrogate"], "pairs_per_launch": tm["pairs_surrogate"],
-                            "flops_per_pair": flops}
+                                           "runs tcgen05.mma kind::f16 (FP16 operands, FP32 accumulation)",
+                            "launch_ms": sg_ms, "launch_ms_in_timed_region": tm["green_surrogate"] or None,
+                            "pairs_per_launch": sg_pairs, "flops_per_pair": flops,
+                            "timing": "mean of 5 launches on one lane (nothing else running), CUDA events on the "
+                                      "launching stream"}
     else:
         eig_ms = tm["green_eigene"]
         peak = hb.measure_fp64_peak(local) if rank == 0 else None

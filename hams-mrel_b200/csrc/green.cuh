@@ -281,23 +281,27 @@ __device__ inline void pidcock_images(double r, double zf, double zp, double h, 
   gz = (-s2 + q2) / (h * h);
 }
 
+// Propagating mode and logarithmic terms of PIDCOCK, FinGreen3D.f90:581-591.
+__device__ inline void pidcock_head(double r, double zfh, double zph, double wk, double h, cplx g[3]) {
+  const double pi = 3.141592653589793, ga = 0.5772156649015328;
+  double nm0 = h / 2.0 * (1.0 + sinh(2.0 * wk * h) / (2.0 * wk * h));
+  double czp = cosh(wk * zph);
+  double p0 = pi / nm0 * cosh(wk * zfh) * czp;
+  double dp0 = wk * pi / nm0 * sinh(wk * zfh) * czp;
+  double j0, j1, y0, y1;
+  jy01b(wk * r, j0, j1, y0, y1);
+  g[0] = cmk(-p0 * y0 + 2.0 / h * (ga + log(r / 4.0 / h)), p0 * j0);
+  g[1] = cmk(wk * p0 * y1 + 2.0 / (r * h), -wk * p0 * j1);
+  g[2] = cmk(-dp0 * y0, dp0 * j0);
+}
+
 // PIDCOCK, FinGreen3D.f90:558-660 (0.0005 <= R/h < 0.05)
 template <class MD, int N>
 __device__ inline void pidcock(double r, double zf, double zp, double v, double wk, const double* __restrict__ wvn,
                                double h, cplx g[3], SeriesScratchN<N>& sc, const MD& md, int* overflow) {
-  const double pi = 3.141592653589793, ga = 0.5772156649015328;
+  const double pi = 3.141592653589793;
   double zfh = zf + h, zph = zp + h;
-  {
-    double nm0 = h / 2.0 * (1.0 + sinh(2.0 * wk * h) / (2.0 * wk * h));
-    double czp = cosh(wk * zph);
-    double p0 = pi / nm0 * cosh(wk * zfh) * czp;
-    double dp0 = wk * pi / nm0 * sinh(wk * zfh) * czp;
-    double j0, j1, y0, y1;
-    jy01b(wk * r, j0, j1, y0, y1);
-    g[0] = cmk(-p0 * y0 + 2.0 / h * (ga + log(r / 4.0 / h)), p0 * j0);
-    g[1] = cmk(wk * p0 * y1 + 2.0 / (r * h), -wk * p0 * j1);
-    g[2] = cmk(-dp0 * y0, dp0 * j0);
-  }
+  pidcock_head(r, zfh, zph, wk, h, g);
   double rhp = fabs(r / h);
   int nt = (int)(HAMS_F4(-1010.10) * rhp + HAMS_F4(100.50));
   if (nt > N) {  // outside the branch's range of R/h

@@ -1,16 +1,25 @@
 // green_sg.cu -- far-field finite-depth Green functions from the MLP
-// surrogate (surrogate.h), fused with the pair algebra of the assembly.
+// surrogate (surrogate.h), fused with the pair algebra of the assembly, on
+// the fifth-generation tensor cores.
 //
-// One warp evaluates 16 panel pairs at a time.  The first layer (4 inputs)
-// runs in FP32 on the CUDA cores; the three 128 x 128 hidden layers and the
-// output layer run on the tensor cores as mma.sync m16n8k16 (FP16 operands,
-// FP32 accumulation) with the pairs as the M dimension, so each layer's
-// accumulator fragments, after bias and SiLU, are repacked in registers as
-// the next layer's A fragments.  The weights of a block live in shared
-// memory.  Lanes 0-15 then finish their pair in FP64: the exact propagating
-// mode (FinGreen3D.f90:311-322), the surrogate's evanescent part, the point
-// source terms by the near/far flag, and A, S as the series kernels store
-// them.
+// A CTA runs kWG warpgroups; each takes tiles of 128 panel pairs, one pair
+// per thread.  The first layer (4 inputs) runs in FP32 on the CUDA cores;
+// the three 128 x 128 hidden layers and the output layer run as
+// tcgen05.mma (FP16 operands, FP32 accumulation, M = 128 pairs) issued by
+// one thread of the warpgroup, with the activations of the tile and all
+// weights in shared memory in the canonical K-major layout and the
+// accumulator in tensor memory.  After each layer the warpgroup reads its
+// 128 x 128 accumulator back with tcgen05.ld (thread t owns TMEM lane t =
+// pair t), adds the bias, applies SiLU, and writes the FP16 activations over
+// the tile for the next layer.  While one warpgroup runs its epilogue the
+// other's MMAs run.  Each thread then finishes its pair in FP64: the exact
+// propagating mode (FinGreen3D.f90:311-322), the surrogate's evanescent part,
+// the point-source terms by the near/far flag, and A, S as the series kernels
+// store them.
+//
+// Every wait on a tensor-core completion barrier is bounded; a wait that
+// gives up sets bit 2 of the error word, the warpgroup stops, and the CTA
+// frees its tensor memory before it returns.
 #include <cuda_fp16.h>
 
 #include "kernels.cuh"
@@ -19,13 +28,91 @@
 
 namespace {
 
-__device__ __forceinline__ void mma16816(float c[4], const uint32_t a[4], uint32_t b0, uint32_t b1) {
-  asm volatile(
-      "mma.sync.aligned.m16n8k16.row.col.f32.f16.f16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
-      "{%0,%1,%2,%3};\n"
-      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
-      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+constexpr int kWG = 3;                 // warpgroups per CTA, one 128-pair tile in flight each
+constexpr int kThreads = 128 * kWG;
+constexpr int kCols = kWG <= 2 ? 256 : 512;  // TMEM columns (power of two): 128 f32 columns per warpgroup
+constexpr int kOffAct = kSgHalves * 2;                    // activation tiles, one per warpgroup
+constexpr int kOffW0 = kOffAct + kWG * kSgOperandBytes;   // first layer, f32
+constexpr int kOffBias = kOffW0 + sg::kWidth * sg::kIn * 4;
+constexpr int kOffBar = kOffBias + ((kSgBias * 4 + 15) / 16) * 16;  // one mbarrier per warpgroup
+constexpr int kOffTmem = kOffBar + 8 * kWG;                          // TMEM base written by tcgen05.alloc
+constexpr int kSmemBytes = kOffTmem + 16;
+static_assert(kCols >= 128 * kWG, "tensor memory for the accumulators");
+static_assert(kSmemBytes <= 227 * 1024, "shared memory per CTA");
+
+// instruction descriptor of kind::f16: FP16 A and B, FP32 D, both K-major,
+// M = 128, N = n
+constexpr uint32_t idesc_f16(int n) { return (1u << 4) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(128 >> 4) << 24); }
+constexpr uint32_t kIdescHidden = idesc_f16(128), kIdescOut = idesc_f16(kSgOutRows);
+
+// shared-memory matrix descriptor of a canonical K-major operand without
+// swizzle (sg_core_off): K-direction core matrices 128 B apart (leading byte
+// offset), 8-row groups 2048 B apart (stride byte offset), version 1
+__device__ __forceinline__ uint64_t sdesc(uint32_t saddr) {
+  return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)(128 >> 4) << 16) | ((uint64_t)(2048 >> 4) << 32) |
+         (1ull << 46);
 }
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void umma_f16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                         uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem_d),
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate));
+}
+
+__device__ __forceinline__ void umma_commit(uint32_t bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
+}
+
+// bounded wait for the phase `parity` of the mbarrier to complete
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+  for (int it = 0; it < (1 << 22); ++it) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(done)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void proxy_fence() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void wg_sync(int id) { asm volatile("bar.sync %0, 128;" ::"r"(id) : "memory"); }
+// OR of p over the 128 threads of a warpgroup (a barrier as well)
+__device__ __forceinline__ bool wg_any(int id, bool p) {
+  uint32_t r;
+  asm volatile(
+      "{\n\t.reg .pred q, s;\n\tsetp.ne.u32 q, %1, 0;\n\tbarrier.red.or.pred s, %2, 128, q;\n\t"
+      "selp.u32 %0, 1, 0, s;\n\t}\n"
+      : "=r"(r)
+      : "r"((uint32_t)p), "r"(id)
+      : "memory");
+  return r != 0;
+}
+
+// 16 consecutive f32 columns of this thread's TMEM lane
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&v)[16]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+      "%15}, [%16];"
+      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+        "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+      : "r"(taddr));
+}
+__device__ __forceinline__ void tmem_ld4(uint32_t taddr, uint32_t (&v)[4]) {
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0, %1, %2, %3}, [%4];"
+               : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3])
+               : "r"(taddr));
+}
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
 __device__ __forceinline__ uint32_t pack2(float lo, float hi) {
   __half2 h = __floats2half2_rn(lo, hi);
@@ -40,45 +127,56 @@ __device__ __forceinline__ float silu(float z) {
   return 0.5f * z * (1.0f + t);
 }
 
-// Four 8 x 8 FP16 matrices from shared memory (one row address per lane).
-__device__ __forceinline__ void ldsm_x4(const __half* row, uint32_t& r0, uint32_t& r1, uint32_t& r2, uint32_t& r3) {
-  unsigned a = (unsigned)__cvta_generic_to_shared(row);
-  asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];\n"
-               : "=r"(r0), "=r"(r1), "=r"(r2), "=r"(r3)
-               : "r"(a));
-}
-
 }  // namespace
 
-__global__ void __launch_bounds__(128, 2) k_green_sg(DevGeom g, WaveDev w, SgDev sp, hams::ModeTab mt, double K,
-                                                     const uint32_t* __restrict__ pairs, long long count,
-                                                     const double* __restrict__ rs, const double* __restrict__ rd,
-                                                     double2* __restrict__ A, double2* __restrict__ S) {
-  extern __shared__ __align__(16) unsigned char smem[];
-  __half* sW = reinterpret_cast<__half*>(smem);                        // kSgHalves
-  float* sW0 = reinterpret_cast<float*>(smem + kSgHalves * 2);         // 128 x 4, column-major
-  float* sB = sW0 + sg::kWidth * sg::kIn;                              // biases
+__global__ void __launch_bounds__(kThreads, 1) k_green_sg(DevGeom g, WaveDev w, SgDev sp, hams::ModeTab mt, double K,
+                                                          const uint32_t* __restrict__ pairs, long long count,
+                                                          const double* __restrict__ rs, const double* __restrict__ rd,
+                                                          double2* __restrict__ A, double2* __restrict__ S, int* err) {
+  extern __shared__ __align__(1024) unsigned char smem[];
+  const float* sW0 = reinterpret_cast<const float*>(smem + kOffW0);  // 128 x 4, column-major
+  const float* sB = reinterpret_cast<const float*>(smem + kOffBias);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + kOffBar);
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(smem + kOffTmem);
+  const int tid = threadIdx.x, warp = tid >> 5, wg = warp >> 2, t = tid & 127;
   {
     const uint4* src = reinterpret_cast<const uint4*>(sp.wh);
-    uint4* dst = reinterpret_cast<uint4*>(sW);
-    for (int e = threadIdx.x; e < kSgHalves / 8; e += blockDim.x) dst[e] = src[e];
-    for (int e = threadIdx.x; e < sg::kWidth * sg::kIn; e += blockDim.x) sW0[e] = sp.w0[e];
-    for (int e = threadIdx.x; e < kSgBias; e += blockDim.x) sB[e] = sp.bias[e];
+    uint4* dst = reinterpret_cast<uint4*>(smem);
+    for (int e = tid; e < kSgHalves / 8; e += kThreads) dst[e] = src[e];
+    float* w0 = reinterpret_cast<float*>(smem + kOffW0);
+    float* b = reinterpret_cast<float*>(smem + kOffBias);
+    for (int e = tid; e < sg::kWidth * sg::kIn; e += kThreads) w0[e] = sp.w0[e];
+    for (int e = tid; e < kSgBias; e += kThreads) b[e] = sp.bias[e];
   }
+  if (tid == 0) {
+    for (int k = 0; k < kWG; ++k) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&bars[k])));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)),
+                 "r"(kCols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  tc_fence_before();
   __syncthreads();
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int gq = lane >> 2, tq = lane & 3;
+  tc_fence_after();
+  const uint32_t tbase = *reinterpret_cast<volatile uint32_t*>(tslot);
+  const uint32_t tacc = tbase + (uint32_t)(128 * wg);                   // this warpgroup's accumulator
+  const uint32_t tld = tacc + ((uint32_t)(32 * (warp & 3)) << 16);     // + this warp's 32 lanes
+  unsigned char* act = smem + kOffAct + wg * kSgOperandBytes;
+  const uint32_t act_sa = smem_u32(act), w_sa = smem_u32(smem), bar = smem_u32(&bars[wg]);
+  const int bar_id = 1 + wg;
+  uint32_t phase = 0;
   const double h = w.h;
-  const long long ngroups = (count + 15) / 16;
-  for (long long grp = (long long)blockIdx.x * 4 + warp; grp < ngroups; grp += (long long)gridDim.x * 4) {
-    // pair of this lane (lanes 16-31 repeat lanes 0-15)
-    const long long t = grp * 16 + (lane & 15);
-    const bool live = t < count;
+  const long long ntiles = (count + 127) / 128;
+  for (long long tile = (long long)blockIdx.x * kWG + wg; tile < ntiles; tile += (long long)gridDim.x * kWG) {
+    const long long tp = tile * 128 + t;
+    const bool live = tp < count;
     size_t p = 0;
     int i = 0, j = 0;
     double xp = 0, yp = 0, zp = -0.25 * h, xq = 0.1 * h, yq = 0, zq = -0.25 * h;
     if (live) {
-      p = pairs[t];
+      p = pairs[tp];
       i = (int)(p % (size_t)g.tn);
       j = (int)(p / (size_t)g.tn);
       xp = g.fxyz[i];
@@ -93,83 +191,81 @@ __global__ void __launch_bounds__(128, 2) k_green_sg(DevGeom g, WaveDev w, SgDev
     const double X = rr / h;
     float f[sg::kIn];
     sg::features(X, (zq + h) / h, (zp + h) / h, K, f);
-    // inputs of rows gq and gq + 8 of the 16 x 4 input tile
-    float fa[sg::kIn], fb[sg::kIn];
-    for (int k = 0; k < sg::kIn; ++k) {
-      fa[k] = __shfl_sync(0xffffffffu, f[k], gq);
-      fb[k] = __shfl_sync(0xffffffffu, f[k], gq + 8);
-    }
-    // layer 0 in FP32, straight into A fragments
-    uint32_t a[8][4];
+    // layer 0 in FP32 into row t of the activation tile
+#pragma unroll 2
+    for (int q = 0; q < 16; ++q) {
+      uint32_t hv[4];
 #pragma unroll
-    for (int kt = 0; kt < 8; ++kt) {
-#pragma unroll
-      for (int hh = 0; hh < 2; ++hh) {
-        const int o = 16 * kt + 2 * tq + 8 * hh;
-        float va0 = sB[o], va1 = sB[o + 1], vb0 = sB[o], vb1 = sB[o + 1];
+      for (int e = 0; e < 4; ++e) {
+        const int o = 8 * q + 2 * e;
+        float v0 = sB[o], v1 = sB[o + 1];
 #pragma unroll
         for (int k = 0; k < sg::kIn; ++k) {
-          const float w0 = sW0[o + sg::kWidth * k], w1 = sW0[o + 1 + sg::kWidth * k];
-          va0 = fmaf(w0, fa[k], va0);
-          va1 = fmaf(w1, fa[k], va1);
-          vb0 = fmaf(w0, fb[k], vb0);
-          vb1 = fmaf(w1, fb[k], vb1);
+          v0 = fmaf(sW0[o + sg::kWidth * k], f[k], v0);
+          v1 = fmaf(sW0[o + 1 + sg::kWidth * k], f[k], v1);
         }
-        a[kt][2 * hh] = pack2(silu(va0), silu(va1));
-        a[kt][2 * hh + 1] = pack2(silu(vb0), silu(vb1));
+        hv[e] = pack2(silu(v0), silu(v1));
       }
+      *reinterpret_cast<uint4*>(act + sg_core_off(t, 8 * q)) = make_uint4(hv[0], hv[1], hv[2], hv[3]);
     }
-    // hidden layers 1..3 on the tensor cores
+    // layers 1..3 (N = 128) and the output layer (N = 16, three columns used)
+    float y[3] = {0.0f, 0.0f, 0.0f};
+    bool ok = true;
+    for (int l = 1; l <= sg::kHidden; ++l) {
+      proxy_fence();
+      tc_fence_before();
+      wg_sync(bar_id);
+      if (t == 0) {
+        tc_fence_after();
+        const uint32_t wb = w_sa + (uint32_t)((l - 1) * kSgOperandBytes);
+        const uint32_t id = l < sg::kHidden ? kIdescHidden : kIdescOut;
+#pragma unroll
+        for (int s = 0; s < 8; ++s) umma_f16(tacc, sdesc(act_sa + 256 * s), sdesc(wb + 256 * s), id, s > 0);
+        umma_commit(bar);
+      }
+      const bool done = mbar_wait(bar, phase);
+      phase ^= 1u;
+      if (wg_any(bar_id, !done)) {
+        ok = false;
+        break;
+      }
+      tc_fence_after();
+      if (l < sg::kHidden) {
+        const float* bl = sB + l * sg::kWidth;
 #pragma unroll 1
-    for (int l = 1; l < sg::kHidden; ++l) {
-      const __half* Wl = sW + (size_t)(l - 1) * sg::kWidth * kSgPadK;
-      float c[16][4];
+        for (int c = 0; c < 128; c += 32) {
+          uint32_t v0[16], v1[16];
+          tmem_ld16(tld + c, v0);
+          tmem_ld16(tld + c + 16, v1);
+          tmem_wait_ld();
+          uint32_t hv[16];
 #pragma unroll
-      for (int nt = 0; nt < 16; ++nt) c[nt][0] = c[nt][1] = c[nt][2] = c[nt][3] = 0.0f;
-      // lane L addresses row L % 8 of matrix L / 8: (n-tile nt + m / 2, k half m % 2)
-      const int lm = lane >> 3, lr = lane & 7;
+          for (int e = 0; e < 8; ++e) {
+            hv[e] = pack2(silu(__uint_as_float(v0[2 * e]) + bl[c + 2 * e]),
+                          silu(__uint_as_float(v0[2 * e + 1]) + bl[c + 2 * e + 1]));
+            hv[8 + e] = pack2(silu(__uint_as_float(v1[2 * e]) + bl[c + 16 + 2 * e]),
+                              silu(__uint_as_float(v1[2 * e + 1]) + bl[c + 16 + 2 * e + 1]));
+          }
 #pragma unroll
-      for (int kt = 0; kt < 8; ++kt) {
-#pragma unroll
-        for (int nt = 0; nt < 16; nt += 2) {
-          uint32_t b00, b01, b10, b11;
-          ldsm_x4(Wl + (size_t)(8 * (nt + (lm >> 1)) + lr) * kSgPadK + 16 * kt + 8 * (lm & 1), b00, b01, b10, b11);
-          mma16816(c[nt], a[kt], b00, b01);
-          mma16816(c[nt + 1], a[kt], b10, b11);
+          for (int q = 0; q < 4; ++q)
+            *reinterpret_cast<uint4*>(act + sg_core_off(t, c + 8 * q)) =
+                make_uint4(hv[4 * q], hv[4 * q + 1], hv[4 * q + 2], hv[4 * q + 3]);
         }
-      }
-      const float* bl = sB + l * sg::kWidth;
-#pragma unroll
-      for (int nt = 0; nt < 16; ++nt) {
-        const int o = 8 * nt + 2 * tq;
-        const uint32_t lo = pack2(silu(c[nt][0] + bl[o]), silu(c[nt][1] + bl[o + 1]));
-        const uint32_t hi = pack2(silu(c[nt][2] + bl[o]), silu(c[nt][3] + bl[o + 1]));
-        a[nt / 2][(nt & 1) * 2] = lo;
-        a[nt / 2][(nt & 1) * 2 + 1] = hi;
+      } else {
+        uint32_t v[4];
+        tmem_ld4(tld, v);
+        tmem_wait_ld();
+        const float* bo = sB + sg::kHidden * sg::kWidth;
+        for (int k = 0; k < 3; ++k) y[k] = __uint_as_float(v[k]) + bo[k];
       }
     }
-    // output layer: one n-tile, columns 0-2 used
-    float co[4] = {0.0f, 0.0f, 0.0f, 0.0f};
-    {
-      const __half* Wo = sW + (size_t)(sg::kHidden - 1) * sg::kWidth * kSgPadK;
-#pragma unroll
-      for (int kt = 0; kt < 8; ++kt) {
-        const __half* row = Wo + (size_t)gq * kSgPadK + 16 * kt + 2 * tq;
-        mma16816(co, a[kt], *reinterpret_cast<const uint32_t*>(row), *reinterpret_cast<const uint32_t*>(row + 8));
-      }
+    if (!ok) {
+      if (t == 0) atomicOr(err, 2);
+      break;
     }
-    // outputs of pair L (lane L < 16): row L % 8 of the tile, upper half for L >= 8
-    const int src = 4 * (lane & 7);
-    const float r0a = __shfl_sync(0xffffffffu, co[0], src), r0b = __shfl_sync(0xffffffffu, co[2], src);
-    const float r1a = __shfl_sync(0xffffffffu, co[1], src), r1b = __shfl_sync(0xffffffffu, co[3], src);
-    const float r2a = __shfl_sync(0xffffffffu, co[0], src + 1), r2b = __shfl_sync(0xffffffffu, co[2], src + 1);
-    const bool up = (lane & 15) >= 8;
-    const float* bo = sB + sg::kHidden * sg::kWidth;
-    const double y0 = (double)((up ? r0b : r0a) + bo[0]), y1 = (double)((up ? r1b : r1a) + bo[1]),
-                 y2 = (double)((up ? r2b : r2a) + bo[2]);
-    if (lane < 16 && live) {
-      const double t0 = sp.mean[0] + sp.scale[0] * y0, t1 = sp.mean[1] + sp.scale[1] * y1,
-                   t2 = sp.mean[2] + sp.scale[2] * y2;
+    if (live) {
+      const double t0 = sp.mean[0] + sp.scale[0] * (double)y[0], t1 = sp.mean[1] + sp.scale[1] * (double)y[1],
+                   t2 = sp.mean[2] + sp.scale[2] * (double)y[2];
       // propagating mode (FinGreen3D.f90:311-322) from the per-frequency factors
       hams::cplx fg[3];
       double rk[3];
@@ -192,27 +288,35 @@ __global__ void __launch_bounds__(128, 2) k_green_sg(DevGeom g, WaveDev w, SgDev
       grn4 G = hams::finish_green(fg, xpq, ypq, zq, zp, rr, r, r1, flag);
       store_pair(g, p, i, j, G, rs, rd, A, S);
     }
+    __syncwarp();
   }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tbase), "r"(kCols));
 }
 
 int launch_green_sg(cudaStream_t st, int sms, DevGeom g, WaveDev w, const SgDev& sp, const hams::ModeTab& mt, double K,
-                    const uint32_t* pairs,
-                    long long count, const double* rs, const double* rd, double2* A, double2* S) {
+                    const uint32_t* pairs, long long count, const double* rs, const double* rd, double2* A,
+                    double2* S, int* err) {
   if (count <= 0) return 0;
-  if (cudaFuncSetAttribute(k_green_sg, cudaFuncAttributeMaxDynamicSharedMemorySize, kSgSmem) != cudaSuccess) return 1;
-  long long groups = (count + 15) / 16;
-  long long blocks = std::min<long long>(2LL * sms, (groups + 3) / 4);
-  k_green_sg<<<(unsigned)blocks, 128, kSgSmem, st>>>(g, w, sp, mt, K, pairs, count, rs, rd, A, S);
+  if (cudaFuncSetAttribute(k_green_sg, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes) != cudaSuccess)
+    return 1;
+  const long long tiles = (count + 127) / 128;
+  const long long blocks = std::min<long long>(sms, (tiles + kWG - 1) / kWG);  // persistent: one CTA per SM
+  k_green_sg<<<(unsigned)blocks, kThreads, kSmemBytes, st>>>(g, w, sp, mt, K, pairs, count, rs, rd, A, S, err);
   return cudaGetLastError() == cudaSuccess ? 0 : 1;
 }
 
 void pack_surrogate(const float* P, std::vector<__half>& wh, std::vector<float>& w0, std::vector<float>& bias) {
+  // layer l's weights as the B operand (N = outputs, K = inputs), rows past
+  // the output layer's three left zero
   wh.assign(kSgHalves, __float2half(0.0f));
   for (int l = 1; l < sg::kLayers; ++l) {
     const int fi = sg::layer_in(l), fo = sg::layer_out(l);
-    __half* dst = wh.data() + (size_t)(l - 1) * sg::kWidth * kSgPadK;
+    __half* dst = wh.data() + (size_t)(l - 1) * (kSgOperandBytes / 2);
     for (int o = 0; o < fo; ++o)
-      for (int k = 0; k < fi; ++k) dst[(size_t)o * kSgPadK + k] = __float2half(P[sg::w_off(l) + o + fo * k]);
+      for (int k = 0; k < fi; ++k) dst[sg_core_off(o, k) / 2] = __float2half(P[sg::w_off(l) + o + fo * k]);
   }
   w0.assign(P + sg::w_off(0), P + sg::w_off(0) + sg::kWidth * sg::kIn);
   bias.assign(kSgBias, 0.0f);

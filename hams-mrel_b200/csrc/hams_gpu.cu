@@ -552,12 +552,13 @@ struct hams_ctx {
   cudaEvent_t ev[6] = {};
   cudaEvent_t evb[6] = {};
   cudaEvent_t evf = nullptr;
-  static constexpr int kTimings = 18;
+  static constexpr int kTimings = 19;
   double last_ms[kTimings] = {};
   std::atomic<long long> launches{0};   // kernels of this library
   std::atomic<long long> lib_calls{0};  // cuBLAS / cuSOLVER / CUB calls
   cudaEvent_t marks[8] = {};
   int refine_sweeps = 0;
+  double ir_rate = 0.0;  // largest residual reduction factor of one refinement sweep
   // batch lanes: contexts that share this one's geometry and pair data (views)
   // and own their stream, handles and per-frequency buffers
   std::vector<hams_ctx*> lanes;
@@ -565,6 +566,7 @@ struct hams_ctx {
   // MLP surrogate of far-field pairs (hams_ctx_set_surrogate)
   int sg_on = 0;
   double sg_far = 3.0;
+  double sg_kmin = sg::kKmin, sg_kmax = sg::kKmax;  // frequencies (K = k0 h tanh k0 h) given to the surrogate
   DBuf<uint16_t> sg_wh;
   DBuf<float> sg_w0, sg_bias;
   SgDev sgd{};
@@ -778,6 +780,8 @@ static int make_lane(hams_ctx* c, hams_ctx** out) {
     for (int b = 0; b <= kBins; ++b) l->bin_off[b] = c->bin_off[b];
     l->sg_on = c->sg_on;
     l->sg_far = c->sg_far;
+    l->sg_kmin = c->sg_kmin;
+    l->sg_kmax = c->sg_kmax;
     l->sgd = c->sgd;
     l->sms = c->sms;
     l->chunks_h = c->chunks_h;
@@ -874,9 +878,9 @@ static int assemble_dev(hams_ctx* c, const hams_wave* w, int nbeta) {
     const long long cs = c->bin_off[6] - c->bin_off[4];
     const double hh = c->opts.depth, K = wd.wk * hh * tanh(wd.wk * hh);
     if (cs > 0) {
-      if (!wd.limit && K >= sg::kKmin && K <= sg::kKmax) {
+      if (!wd.limit && K >= c->sg_kmin && K <= c->sg_kmax) {
         if (launch_green_sg(c->st, c->sms, c->g, wd, c->sgd, c->mt, K, c->pairs.p + c->bin_off[4], cs, c->rs.p,
-                            c->rd.p, c->A.p, c->S.p))
+                            c->rd.p, c->A.p, c->S.p, c->ovf.p))
           return fail(HAMS_ERR_CUDA, "surrogate kernel launch failed");
         c->launches += 1;
         c->sg_used = 1;
@@ -984,6 +988,7 @@ static int mixed_solve(hams_ctx* c, double2* M, const double2* rhs, int ldr, int
   std::vector<double> ratio(nrhs);
   double prev = 1e300;
   c->refine_sweeps = 0;
+  c->ir_rate = 0.0;
   for (int it = 0;; ++it) {
     // R = rhs - M_fp64 X   (M still holds the FP64 matrix)
     CU(cudaMemcpy2DAsync(c->R.p, (size_t)n * 16, rhs, (size_t)ldr * 16, (size_t)n * 16, nrhs, cudaMemcpyDeviceToDevice, c->st));
@@ -998,6 +1003,7 @@ static int mixed_solve(hams_ctx* c, double2* M, const double2* rhs, int ldr, int
     double worst = 0.0;
     for (double r : ratio) worst = std::max(worst, r);
     c->refine_sweeps = it;
+    if (it > 0 && prev > 0.0) c->ir_rate = std::max(c->ir_rate, worst / prev);
     if (!(worst == worst)) return fail(HAMS_ERR_NUMERIC, "non-finite residual in iterative refinement");
     if (worst <= tol) break;
     if (it >= maxit) return fail(HAMS_ERR_NUMERIC, "iterative refinement: %.3e after %d sweeps", worst, it);
@@ -1331,6 +1337,8 @@ static int solve_one(hams_ctx* c, const hams_wave* w, int nbeta, const double* b
   c->last_ms[16] = 0.0;
   if (c->opts.depth >= 0.0 && cudaEventElapsedTime(&ms, c->evb[4], c->evb[5]) == cudaSuccess) c->last_ms[16] = ms;
   c->last_ms[17] = c->sg_used ? (double)(c->bin_off[6] - c->bin_off[4]) : 0.0;
+  c->last_ms[18] = c->opts.precision == HAMS_PREC_MIXED ? c->ir_rate : 0.0;
+  if (ovf & 2) return fail(HAMS_ERR_CUDA, "surrogate kernel: a tensor-core completion wait gave up");
   if (ovf) return fail(HAMS_ERR_NUMERIC, "adaptive quadrature stack overflow in the LINTON branch");
   if (info > 0) return info;  // singular pivot, LAPACK style
   return 0;
@@ -1535,6 +1543,24 @@ extern "C" int hams_eval_green_static(hams_ctx* c, const hams_wave* w, int32_t n
   return 0;
 }
 
+extern "C" int hams_ctx_set_surrogate_range(hams_ctx* c, double kmin, double kmax) {
+  g_err.clear();
+  if (!c || c->is_lane) return fail(HAMS_ERR_ARG, "null context");
+  if (!(kmin >= sg::kKmin && kmax <= sg::kKmax && kmin <= kmax))
+    return fail(HAMS_ERR_ARG, "K range [%g, %g] is not inside the network's domain [%g, %g]", kmin, kmax, sg::kKmin,
+                sg::kKmax);
+  if (cudaSetDevice(c->dev) != cudaSuccess) return fail(HAMS_ERR_CUDA, "cudaSetDevice failed");
+  for (hams_ctx* l : c->lanes) CU(cudaStreamSynchronize(l->st));
+  CU(cudaStreamSynchronize(c->st));
+  c->sg_kmin = kmin;
+  c->sg_kmax = kmax;
+  for (hams_ctx* l : c->lanes) {
+    l->sg_kmin = kmin;
+    l->sg_kmax = kmax;
+  }
+  return 0;
+}
+
 extern "C" int hams_ctx_set_surrogate(hams_ctx* c, const float* params, int32_t nparams, double far_factor) {
   g_err.clear();
   if (!c || c->is_lane) return fail(HAMS_ERR_ARG, "null context");
@@ -1576,6 +1602,8 @@ extern "C" int hams_ctx_set_surrogate(hams_ctx* c, const float* params, int32_t 
     l->pairs.view(c->pairs);
     l->sg_on = c->sg_on;
     l->sg_far = c->sg_far;
+    l->sg_kmin = c->sg_kmin;
+    l->sg_kmax = c->sg_kmax;
     l->sgd = c->sgd;
     l->mt.nmode = nmode;
   }

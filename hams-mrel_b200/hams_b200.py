@@ -92,6 +92,7 @@ def load_library(path=LIB_PATH):
     P_flt = ctypes.POINTER(ctypes.c_float)
     lib.hams_surrogate_param_count.restype = c_int
     lib.hams_ctx_set_surrogate.argtypes = [ctypes.c_void_p, P_flt, c_int, c_dbl]
+    lib.hams_ctx_set_surrogate_range.argtypes = [ctypes.c_void_p, c_dbl, c_dbl]
     lib.hams_surrogate_samples.argtypes = [c_int, c_int, ctypes.c_uint64, c_int, P_dbl]
     lib.hams_surrogate_train.argtypes = [c_int, ctypes.POINTER(SgTrain), P_flt, P_dbl]
     lib.hams_surrogate_eval.argtypes = [c_int, P_flt, c_int, P_dbl, P_dbl]
@@ -227,23 +228,26 @@ class Context:
 
     def timings(self):
         """Stage times of the last solve (ms), per-branch Green kernel times and pair counts."""
-        ms = np.zeros(18)
-        load_library().hams_last_timings(self._h, _d(ms), 18)
+        ms = np.zeros(19)
+        load_library().hams_last_timings(self._h, _d(ms), 19)
         return dict(green=ms[0], rhs=ms[1], solve=ms[2], forces=ms[3], total=ms[4], green_linton=ms[5],
                     green_pidcock=ms[6], green_eigene=ms[7], green_eigen=ms[8], factor=ms[9], refine_sweeps=int(ms[10]),
                     iterations=int(ms[10]),
                     pairs_linton=int(ms[11]), pairs_pidcock=int(ms[12]), pairs_eigene=int(ms[13]),
                     pairs_eigen=int(ms[14]), lu_used=int(ms[15]), green_surrogate=ms[16],
-                    pairs_surrogate=int(ms[17]))
+                    pairs_surrogate=int(ms[17]), ir_rate=ms[18])
 
-    def set_surrogate(self, params, far_factor=3.0):
-        """Far pairs from the trained network (params float32), or the series again (params None)."""
+    def set_surrogate(self, params, far_factor=3.0, k_range=None):
+        """Far pairs from the trained network (params float32), or the series again (params None);
+        k_range (kmin, kmax): the frequencies, by K = k0 h tanh(k0 h), the network serves."""
         lib = load_library()
         if params is None:
             _check(lib.hams_ctx_set_surrogate(self._h, None, 0, 0.0))
             return
         self._sg = np.ascontiguousarray(params, dtype=np.float32)
         _check(lib.hams_ctx_set_surrogate(self._h, _f(self._sg), self._sg.size, float(far_factor)))
+        kmin, kmax = k_range if k_range is not None else (0.04, 40.0)
+        _check(lib.hams_ctx_set_surrogate_range(self._h, float(kmin), float(kmax)))
 
     def note(self):
         """What the last solve decided on its own (e.g. a fallback to the library LU), or ''."""

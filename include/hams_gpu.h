@@ -237,14 +237,25 @@ int hams_surrogate_grad(int32_t device, const float *params, int32_t n, const fl
  * series for all pairs.  Finite depth only. */
 int hams_ctx_set_surrogate(hams_ctx *ctx, const float *params, int32_t nparams, double far_factor);
 
+/* Frequencies the surrogate serves: those with K = k0 h tanh(k0 h) in
+ * [kmin, kmax] (inside the network's domain, 0.04 to 40, the default);
+ * other frequencies keep the series for all pairs.  Where the outputs are
+ * small differences of large terms (damping as w -> 0, excitation of deep
+ * bodies at short waves, the bands around irregular frequencies) the
+ * surrogate's error is amplified, and this range keeps those frequencies
+ * on the series. */
+int hams_ctx_set_surrogate_range(hams_ctx *ctx, double kmin, double kmax);
+
 /* Timing of the last solve in milliseconds: [0] Green/assembly kernels,
  * [1] right-hand sides, [2] factorisation + solves, [3] reductions,
  * [4] whole call, [5..8] Green kernels of the LINTON, PIDCOCK, EIGENE and
  * EIGEN branches (finite depth), [9] LU factorisation, [10] refinement
  * sweeps (mixed form) or GMRES iterations, [11..14] pairs in each branch, [15] the mixed
  * form's factorisation (HAMS_LU_*; -1 for FP64), [16] the surrogate kernel
- * (or the series standing in for it), [17] pairs the surrogate evaluated.
- * n is the capacity of ms (18 fills all). Returns the number written. */
+ * (or the series standing in for it), [17] pairs the surrogate evaluated,
+ * [18] the mixed form's largest residual reduction factor over one refinement
+ * sweep (about the condition number times the factorisation's error).
+ * n is the capacity of ms (19 fills all). Returns the number written. */
 int hams_last_timings(hams_ctx *ctx, double *ms, int32_t n);
 
 /* What the last solve of ctx decided on its own, e.g. the reason it fell back

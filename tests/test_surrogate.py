@@ -151,6 +151,17 @@ def test_surrogate_assembly_against_series_and_gain():
             assert rel(a, b) < 2e-3
         # the series left for the near pairs plus the network cost less than the series alone
         assert t["green_surrogate"] + t["green_eigene"] + t["green_eigen"] < series_ms[om]
+    # a frequency outside the surrogate's K range keeps the series for every pair: the same bits
+    # as the series path (K = 1.25 at 0.5 rad/s, 11.4 at 1.5 rad/s in 50 m)
+    ctx.set_surrogate(train_surrogate.load(), 3.0, k_range=(2.0, 40.0))
+    low = ctx.solve_frequency(hams_b200.wave_properties(0.5, 50.0, 9.81), betas)
+    assert ctx.timings()["pairs_surrogate"] == 0
+    for a, b in zip(low, ref[0.5]):
+        assert np.array_equal(a, b)
+    ctx.solve_frequency(hams_b200.wave_properties(1.5, 50.0, 9.81), betas)
+    assert ctx.timings()["pairs_surrogate"] > 0.5 * n_series
+    with pytest.raises(hams_b200.HamsError):
+        ctx.set_surrogate(train_surrogate.load(), 3.0, k_range=(0.01, 40.0))
     # switched off, the plain series path gives the same bits again
     ctx.set_surrogate(None)
     again = ctx.solve_frequency(hams_b200.wave_properties(1.5, 50.0, 9.81), betas)
