@@ -86,6 +86,7 @@ static int fail(int code, const char* fmt, ...) {
 #include "kernels.cuh"
 #include "lu_mixed.h"
 #include "green_sg.h"
+#include "hmatrix.h"
 #include "surrogate.h"
 
 // ---------------------------------------------------------------------------
@@ -519,6 +520,10 @@ struct hams_ctx {
   hams_opts opts{};
   int n = 0, nl = 0, tn = 0, nb = 0;
   std::vector<int> body_nelem;
+  std::vector<double> xyz_p;  // hull panel centres (n x 3), host copy for the H-matrix cluster tree
+  bool hm_ready = false;      // GMRES: cluster tree uploaded to hm
+  hmat::Dev hm;
+  DBuf<double2> hxp, hyp, hw;  // H-matrix product work arrays
   // geometry
   DBuf<double> xq, fxyz, ds, pnsz, nrm, vtx;
   DBuf<int> ncn, body, bstart;
@@ -604,6 +609,7 @@ extern "C" void hams_ctx_destroy(hams_ctx* c) {
   c->info.release(); c->ovf.release(); c->work.release(); c->work32.release(); c->luw.release(); c->perm.release();
   c->mt_pm.release(); c->mt_ac.release(); c->mt_fld.release(); c->mt_fldt.release(); c->mt_src.release();
   c->mt_srct.release();
+  hmat::free_dev(c->hm);
   for (auto& e : c->ev)
     if (e) cudaEventDestroy(e);
   for (auto& e : c->evb)
@@ -770,6 +776,7 @@ static int make_lane(hams_ctx* c, hams_ctx** out) {
   l->tn = c->tn;
   l->nb = c->nb;
   l->body_nelem = c->body_nelem;
+  l->xyz_p = c->xyz_p;
   int rc = ctx_handles(l);
   if (!rc) {
     l->xq.view(c->xq); l->fxyz.view(c->fxyz); l->ds.view(c->ds); l->pnsz.view(c->pnsz); l->nrm.view(c->nrm);
@@ -818,6 +825,7 @@ extern "C" int hams_ctx_create(const hams_geom* geo, const hams_opts* opts, hams
   c->tn = c->n + c->nl;
   c->nb = geo->nbody;
   c->body_nelem.assign(geo->body_nelem, geo->body_nelem + geo->nbody);
+  c->xyz_p.assign(geo->xyz_p, geo->xyz_p + (size_t)3 * geo->nelem);
   int rc = ctx_handles(c);
   if (!rc) rc = ctx_setup(c, geo);
   if (rc < 0) {
@@ -1027,7 +1035,9 @@ static int mixed_solve(hams_ctx* c, double2* M, const double2* rhs, int ldr, int
 // modified Gram-Schmidt one vector at a time, :399-406), the small
 // Hessenberg least-squares problems (Givens rotations) on the host.  A column
 // that misses the tolerance after gmres_maxit steps keeps its last iterate
-// and the solve's note says so (:475-480).
+// and the solve's note says so (:475-480).  Without lids the products (Krylov
+// steps and restart residuals) use the H-matrix of M (HMatrix.f90, as
+// AssbMatx[Multi].f90:284-288 do); the preconditioner is built from M itself.
 static int gmres_solve(hams_ctx* c, double2* M, const double2* rhs, int nrhs) {
   const int n = c->n, nb = c->nb;
   const int m = c->opts.gmres_restart > 0 ? c->opts.gmres_restart : 25;
@@ -1041,6 +1051,41 @@ static int gmres_solve(hams_ctx* c, double2* M, const double2* rhs, int nrhs) {
   TRY(c->gz.alloc((size_t)n * nrhs));
   TRY(c->gy.alloc((size_t)(m + 1) * nrhs));
   TRY(c->gnrm.alloc(nrhs));
+  const bool use_h = c->nl == 0 && c->opts.gmres_dense == 0;
+  if (use_h) {
+    if (!c->hm_ready) {
+      hmat::Tree t;
+      hmat::build_tree(c->xyz_p.data(), n, t);
+      if (hmat::upload(t, c->hm)) return fail(HAMS_ERR_NOMEM, "H-matrix: device allocation failed");
+      c->hm_ready = true;
+    }
+    const double aca = c->opts.aca_tol > 0.0 ? c->opts.aca_tol : hmat::kAcaTol;
+    if (hmat::compress(c->st, M, aca, c->hm)) return fail(HAMS_ERR_CUDA, "H-matrix: ACA launch failed");
+    c->launches += 1 + (c->hm.nlow > 0);
+    std::vector<int> hr(c->hm.nlow);
+    std::vector<long long> hoff;
+    if (c->hm.nlow > 0) CU(cudaMemcpyAsync(hr.data(), c->hm.rank, sizeof(int) * hr.size(), cudaMemcpyDeviceToHost, c->st));
+    CU(cudaStreamSynchronize(c->st));
+    const long long wsize = hmat::product_offsets(c->st, hr, nrhs, c->hm, hoff);
+    TRY(c->hw.alloc((size_t)wsize));
+    TRY(c->hxp.alloc((size_t)n * nrhs));
+    TRY(c->hyp.alloc((size_t)n * nrhs));
+    CU(cudaStreamSynchronize(c->st));  // hoff is read by the copy above
+  }
+  // Y (n x nrhs) = M X, with the H-matrix or the dense matrix
+  auto product = [&](const double2* Xin, double2* Y) -> int {
+    if (use_h) {
+      long long la = 0;
+      if (hmat::matvec(c->st, c->hm, Xin, Y, nrhs, c->hxp.p, c->hyp.p, c->hw.p, &la))
+        return fail(HAMS_ERR_CUDA, "H-matrix product launch failed");
+      c->launches += la;
+      return 0;
+    }
+    CUB_(cublasZgemm(c->blas, CUBLAS_OP_N, CUBLAS_OP_N, n, nrhs, n, &one, (cuDoubleComplex*)M, n,
+                     (const cuDoubleComplex*)Xin, n, &zero, (cuDoubleComplex*)Y, n));
+    c->lib_calls += 1;
+    return 0;
+  };
   // preconditioner: LU of each body's diagonal block, packed one after
   // another, or the diagonal of M with one body
   std::vector<size_t> boff(nb + 1, 0);
@@ -1122,9 +1167,7 @@ static int gmres_solve(hams_ctx* c, double2* M, const double2* rhs, int nrhs) {
       CU(cudaMemcpy2DAsync(c->gz.p, (size_t)n * 16, c->gv.p + (size_t)j * n, vs * 16, (size_t)n * 16, nrhs,
                            cudaMemcpyDeviceToDevice, c->st));
       TRY(precond(c->gz.p));
-      CUB_(cublasZgemm(c->blas, CUBLAS_OP_N, CUBLAS_OP_N, n, nrhs, n, &one, (cuDoubleComplex*)M, n,
-                       (cuDoubleComplex*)c->gz.p, n, &zero, (cuDoubleComplex*)c->gw.p, n));
-      c->lib_calls += 1;
+      TRY(product(c->gz.p, c->gw.p));
       for (size_t e = 0; e < hcol.size(); ++e) hcol[e] = 0.0;
       for (int pass = 0; pass < 2; ++pass) {  // classical Gram-Schmidt, twice
         CUB_(cublasZgemvStridedBatched(c->blas, CUBLAS_OP_C, n, j + 1, &one, (cuDoubleComplex*)c->gv.p, n, (long long)vs,
@@ -1201,9 +1244,9 @@ static int gmres_solve(hams_ctx* c, double2* M, const double2* rhs, int nrhs) {
     TRY(precond(c->gz.p));
     CUB_(cublasZaxpy(c->blas, n * nrhs, &one, (cuDoubleComplex*)c->gz.p, 1, (cuDoubleComplex*)c->X.p, 1));
     // true residual R = B - A X for the next cycle and the stop test
+    TRY(product(c->X.p, c->gz.p));
     CU(cudaMemcpyAsync(c->gw.p, rhs, (size_t)n * nrhs * 16, cudaMemcpyDeviceToDevice, c->st));
-    CUB_(cublasZgemm(c->blas, CUBLAS_OP_N, CUBLAS_OP_N, n, nrhs, n, &mone, (cuDoubleComplex*)M, n,
-                     (cuDoubleComplex*)c->X.p, n, &one, (cuDoubleComplex*)c->gw.p, n));
+    CUB_(cublasZaxpy(c->blas, n * nrhs, &mone, (cuDoubleComplex*)c->gz.p, 1, (cuDoubleComplex*)c->gw.p, 1));
     c->lib_calls += 3;
     if (iters >= maxit) {
       k_colnorm2<<<nrhs, 256, 0, c->st>>>(c->gw.p, n, c->gnrm.p);

@@ -55,8 +55,11 @@ enum { HAMS_LU_BLOCK_TF32 = 0, HAMS_LU_BLOCK_EMU = 1, HAMS_LU_LIBRARY = 2 };
  * side from zero, all right-hand sides advanced together (one matrix product
  * per iteration); FP64 in every precision form.  A solve that misses the
  * tolerance keeps its last iterate and says so in hams_last_note, as the
- * reference warns and goes on (:475-480).  With lids (IRSP = 1) it
- * iterates on the normal equations (AssbMatx_irr.f90:494-498). */
+ * reference warns and goes on (:475-480).  Without lids its products use the
+ * H-matrix of the influence matrix (HMatrix.f90: cluster tree of the panel
+ * centres, ACA-compressed admissible blocks), as the reference's do; with
+ * lids (IRSP = 1) it iterates on the normal equations with dense products
+ * (AssbMatx_irr.f90:494-498). */
 enum { HAMS_SOLVER_LU = 1, HAMS_SOLVER_GMRES = 2 };
 
 /* Numerical form of a solve. */
@@ -105,7 +108,12 @@ typedef struct hams_opts {
   int32_t gmres_restart;/* GMRES restart length (<=0: 25, IterativeSolvers.f90:56) */
   int32_t gmres_maxit;  /* GMRES iterations over all restarts (<=0: 100, :58)    */
   double gmres_tol; /* GMRES relative residual target (<=0: 1e-4, :57)          */
-  int32_t reserved[4];
+  double aca_tol;   /* GMRES: ACA tolerance of the H-matrix blocks (<=0: 1e-4,
+                       HMatrix.f90:60)                                          */
+  int32_t gmres_dense;/* GMRES: 0 products with the H-matrix (the reference's
+                       choice without lids, AssbMatx[Multi].f90:284-288), 1 with
+                       the dense matrix; with lids always dense (:494-498)      */
+  int32_t reserved[3];
 } hams_opts;
 
 /* One frequency after CalWaveProperts (ImplementSubs.f90:40): V = w^2/g

@@ -1,14 +1,18 @@
 """GMRES solver (HAMS_SOLVER_GMRES) through the C ABI.
 
-Against the oracle's direct solve at a tight tolerance (1e-8 relative
-Frobenius on added mass, damping, excitation; the lid case 1e-5 as its
-normal equations square the condition number), and at the reference's
-defaults (restart 25, tolerance 1e-4, 100 steps) against the GMRES
-restatement of oracle/gmres_ref.py on the same assembled systems: the
+With dense products: against the oracle's direct solve at a tight tolerance
+(1e-8 relative Frobenius on added mass, damping, excitation; the lid case
+1e-5 as its normal equations square the condition number), and at the
+reference's defaults (restart 25, tolerance 1e-4, 100 steps) against the
+GMRES restatement of oracle/gmres_ref.py on the same assembled systems: the
 iteration count equals the restatement's largest per-column count (+-1, the
-last step can fall either side of the tolerance), and the forces stay within
-the reference's own GMRES-vs-LU test bounds (test_integration_gmres.f90:48-101:
-1e-3 added mass, 5e-2 damping).
+last step can fall either side of the tolerance).
+
+With H-matrix products (the reference's choice without lids): at the
+reference's defaults the forces stay within the reference's own
+GMRES-vs-LU test bounds (test_integration_gmres.f90:48-101: 1e-3 added mass,
+5e-2 damping); with ACA at 1e-8 and GMRES at 1e-10 within 1e-5 of the direct
+solve, which bounds the H-matrix's own error.
 """
 import os
 import sys
@@ -63,7 +67,7 @@ def test_gmres_tight_matches_direct_solve(name, precision):
     make, h = CASES[name]
     oc, geom, _ = make()
     ctx = hams_b200.Context(geom, h, rho=1025.0, g=9.81, precision=precision, solver=hams_b200.SOLVER_GMRES,
-                            gmres_restart=40, gmres_maxit=400, gmres_tol=1e-11)
+                            gmres_restart=40, gmres_maxit=400, gmres_tol=1e-11, gmres_dense=1)
     betas = np.radians([0.0, 60.0])
     for omega in (0.4, 1.6):
         am, bd, ex = ctx.solve_frequency(hams_b200.wave_properties(omega, h, 9.81), betas)
@@ -78,7 +82,7 @@ def test_gmres_tight_matches_direct_solve(name, precision):
 def test_gmres_defaults_follow_the_restatement(name):
     make, h = CASES[name]
     oc, geom, cnt = make()
-    ctx = hams_b200.Context(geom, h, rho=1025.0, g=9.81, solver=hams_b200.SOLVER_GMRES)
+    ctx = hams_b200.Context(geom, h, rho=1025.0, g=9.81, solver=hams_b200.SOLVER_GMRES, gmres_dense=1)
     betas = np.radians([0.0, 60.0])
     for omega in (0.4, 1.6):
         w = hams_b200.wave_properties(omega, h, 9.81)
@@ -90,6 +94,24 @@ def test_gmres_defaults_follow_the_restatement(name):
         oam, obd, oex, _ = oc.solve(oc.wave(omega), betas)
         assert rel(am, oam) < 1e-3 and rel(bd, obd) < 5e-2 and rel(ex, oex) < 1e-3
     ctx.close()
+
+
+@pytest.mark.parametrize("name", ["array", "single"])
+def test_gmres_hmatrix(name):
+    make, h = CASES[name]
+    oc, geom, _ = make()
+    betas = np.radians([0.0, 60.0])
+    ref = {om: oc.solve(oc.wave(om), betas) for om in (0.4, 1.6)}
+    for kw, bound in ((dict(), (1e-3, 5e-2, 1e-3)),
+                      (dict(aca_tol=1e-8, gmres_tol=1e-10, gmres_restart=40, gmres_maxit=400), (1e-5,) * 3)):
+        ctx = hams_b200.Context(geom, h, rho=1025.0, g=9.81, solver=hams_b200.SOLVER_GMRES, **kw)
+        for om in (0.4, 1.6):
+            am, bd, ex = ctx.solve_frequency(hams_b200.wave_properties(om, h, 9.81), betas)
+            assert ctx.note() == "", ctx.note()
+            oam, obd, oex, _ = ref[om]
+            assert rel(am, oam) < bound[0] and rel(bd, obd) < bound[1] and rel(ex, oex) < bound[2], \
+                (kw, om, rel(am, oam), rel(bd, obd), rel(ex, oex))
+        ctx.close()
 
 
 def test_gmres_missed_tolerance_keeps_iterate_and_notes():
