@@ -68,7 +68,22 @@ EIGENE_DRAM_BYTES_PER_LAUNCH = None
 SG_DRAM_BYTES_PER_LAUNCH = None
 
 
-def build_case():
+# A coarser copy of the array (3,240 panels, 10.2 M far pairs) that profilers
+# capture in full in a minute; never a bench line.
+PROFILE_WORKLOAD = "3x3 cylinder array R=4 T=8 spacing 20 m, 9 x 360 quad panels (profiling case), depth 50 m"
+
+
+def build_case(profile_case=False):
+    if profile_case:
+        bodies, centres = [], []
+        for iy in range(3):
+            for ix in range(3):
+                bodies.append(meshgen.cylinder(4.0, 8.0, 30, 8, 4, 20.0 * ix, 20.0 * iy))
+                centres.append((20.0 * ix, 20.0 * iy, 0.0))
+        base = meshgen.case_c2()
+        case = dict(base, name="c2-coarse", bodies=bodies, centres=centres)
+        xyz, ncn, ncon, cnt = meshgen.combine(bodies)
+        return case, xyz, ncn, ncon, cnt, np.array(centres, dtype=np.float64)
     case = meshgen.case_c2()
     xyz, ncn, ncon, cnt = meshgen.combine(case["bodies"])
     return case, xyz, ncn, ncon, cnt, np.array(case["centres"], dtype=np.float64)
@@ -325,7 +340,7 @@ def gpu_arm(args):
     def max_over_ranks(x):
         return shard.max_over_ranks(x, dist if ws > 1 else None, device="cuda")
 
-    case, xyz, ncn, ncon, cnt, xr = build_case()
+    case, xyz, ncn, ncon, cnt, xr = build_case(args.profile_case)
     geom = hb.prepare_geometry(xyz, ncn, ncon, cnt, xr)
     betas = np.radians(case["betas_deg"])
     allom = case["omegas"]
@@ -375,7 +390,8 @@ def gpu_arm(args):
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": FORMS[args.form][2], "data": "synthetic",
-            "config": {"workload": WORKLOAD, "form": args.form, "panels": int(ncn.size),
+            "config": {"workload": PROFILE_WORKLOAD if args.profile_case else WORKLOAD, "form": args.form,
+                       "panels": int(ncn.size),
                        "rhs_per_step": 6 * int(cnt.size) + len(betas),
                        "l2": "no flush: the 5400x5400 complex system (0.47 GB) and pair tables exceed the 126 MB L2",
                        "parallelism": f"frequency shards x{ws}, {LANES} frequencies in flight per GPU",
@@ -442,6 +458,8 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=None,
                     help="CPU work per baseline sample (default 8 s; 3 s per step of --impl reference)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--profile-case", action="store_true",
+                    help="the coarser 3,240-panel array, for profiler captures (not a bench line)")
     args = ap.parse_args()
     if args.impl == "reference":
         reference_arm(args)

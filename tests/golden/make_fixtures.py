@@ -13,6 +13,9 @@ Decks copied (reference path -> fixture name):
   test/data/config1                       -> config1   (3 bodies x 234 panels, h = 70 m)
   examples/example2_multi_bodies_wave_fields -> example2 (10 bodies x 234, h = 14.5 m)
   examples/example5_single_body           -> example5  (1 body, 234 panels + 383 lid panels)
+  examples/example3_multi_bodies_gen_mod  -> example3  (2 bodies x 234 panels with lids, a generalized
+                                                        mode; its expected files hold the first of the
+                                                        deck's 10 frequencies only)
 Only the HAMS-format outputs (OAMASS/ODAMPING/OEXFOR) are kept as expected data.
 """
 import os
@@ -25,6 +28,8 @@ DECKS = {
                  "examples/example2_multi_bodies_wave_fields/Output/Hams_format"),
     "example5": ("examples/example5_single_body/Input",
                  "examples/example5_single_body/Output/Hams_format"),
+    "example3": ("examples/example3_multi_bodies_gen_mod/Input",
+                 "examples/example3_multi_bodies_gen_mod/Output/Hams_format"),
 }
 OUTPUTS = [f"{k}{m}.txt" for k in ("OAMASS", "ODAMPING", "OEXFOR") for m in range(1, 7)]
 

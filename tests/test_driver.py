@@ -26,7 +26,7 @@ RUN = os.path.join(REPO, "hams-mrel_b200", "hams_b200_run")
 GOLDEN = os.path.join(HERE, "golden")
 
 CASES = [("config1", 1e-6, 5e-4, 2e-7, 1e-7), ("example2", 2e-5, 1e-4, 1e-5, 1e-7),
-         ("example5", 1e-4, 3e-2, 1e-5, 1e-5)]
+         ("example5", 1e-4, 3e-2, 1e-5, 1e-5), ("example3", 1e-4, 1e-4, 1e-4, 1e-5)]
 
 
 def _load(path):
@@ -68,9 +68,12 @@ def test_driver_reproduces_reference_files(tmp_path, deck, tol_a, tol_b, tol_x, 
             head, got = _load(tmp_path / "gpu" / "Hams_format" / f"{kind}{m}.txt")
             rhead, ref = _load(os.path.join(GOLDEN, deck, "expected", f"{kind}{m}.txt"))
             ohead, orc = _load(tmp_path / "cpu" / f"{kind}{m}.txt")
-            assert head == rhead == ohead
-            assert np.linalg.norm(got - ref) / np.linalg.norm(ref) < tol, f"{deck} {kind}{m} vs reference"
+            assert head == ohead
             assert np.linalg.norm(got - orc) / np.linalg.norm(orc) < tol_oracle, f"{deck} {kind}{m} vs oracle"
+            # the frequencies the expected file holds (example3 keeps the first of its deck's)
+            keep = [k for k, h in enumerate(head) if h in rhead]
+            assert [head[k] for k in keep] == rhead
+            assert np.linalg.norm(got[keep] - ref) / np.linalg.norm(ref) < tol, f"{deck} {kind}{m} vs reference"
 
 
 @pytest.mark.gpu

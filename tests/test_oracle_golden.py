@@ -14,6 +14,9 @@ Observed with the oracle (relative Frobenius, worst of the six files):
   config1  (3 x 234 panels, h=70 m, omega 0.05-0.07):  A 3.4e-7, B 1.3e-4, X 3.0e-8
   example2 (10 x 234 panels, h=14.5 m, T=0.5, 1 s):   A 4.9e-6, B 2.4e-5, X 3.3e-6
   example5 (1 x 234 + 383 lid panels, h=70 m):        A 1.9e-5, B 9.0e-3, X 3.0e-6
+  example3 (2 x 234 panels with lids, a generalized mode, 36 headings; its
+            expected files hold the first of the deck's 10 frequencies):
+                                                      A 3.7e-5, B 1.8e-5, X 2.7e-5
 The Wynn-epsilon extrapolation of the EIGENE/PIDCOCK series turns a one-ulp
 difference of sin/cos/exp/log into up to 1e-3 in single Green values; the
 oracle evaluates those with correctly rounded functions, as the reference's
@@ -33,13 +36,15 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 GOLDEN = os.path.join(HERE, "golden")
 
 # (deck, tol A, tol B, tol X, minimum fraction of significant entries printed identically per A/B/X)
-# Observed fractions: config1 0.977/0.912/0.968, example2 0.73/0.67/0.63, example5 0.79/0.63/0.71.
+# Observed fractions: config1 0.977/0.912/0.968, example2 0.73/0.67/0.63, example5 0.79/0.63/0.71,
+# example3 0.63/0.55/0.60.
 # The epsilon-accelerated series use correctly rounded sin/cos/exp/log (detmath.h); with
 # glibc's versions config1 prints identically for 0.92/0.79/0.90 only.
 CASES = [
     ("config1", 1e-6, 5e-4, 2e-7, (0.95, 0.88, 0.94)),
     ("example2", 2e-5, 1e-4, 1e-5, (0.70, 0.63, 0.60)),
     ("example5", 1e-4, 3e-2, 1e-5, (0.76, 0.60, 0.68)),
+    ("example3", 1e-4, 1e-4, 1e-4, (0.60, 0.50, 0.57)),
 ]
 
 
@@ -57,8 +62,10 @@ def test_oracle_reproduces_reference_outputs(tmp_path, oracle, deck, tol_a, tol_
                             ("OEXFOR", tol_x, min_same[2])):
         same = total = 0
         for m in range(1, 7):
-            got = _load(tmp_path / f"{kind}{m}.txt")
             ref = _load(os.path.join(exp, f"{kind}{m}.txt"))
+            heads = {tuple(row[:2]) for row in ref}
+            # the frequencies the expected file holds (example3 keeps the first of its deck's)
+            got = [row for row in _load(tmp_path / f"{kind}{m}.txt") if tuple(row[:2]) in heads]
             assert len(got) == len(ref)
             g = np.array([[float(x) for x in r[2:]] for r in got])
             r = np.array([[float(x) for x in row[2:]] for row in ref])
@@ -71,6 +78,7 @@ def test_oracle_reproduces_reference_outputs(tmp_path, oracle, deck, tol_a, tol_
             tr = np.array([row[2:] for row in ref])
             same += int((tg == tr)[sig].sum())
             total += int(sig.sum())
+        print(deck, kind, f"{same / total:.3f} of significant entries printed identically")
         assert same / total >= frac, f"{deck} {kind}: {same}/{total} significant entries printed identically"
 
 
