@@ -34,7 +34,7 @@ import meshgen  # noqa: E402
 METRIC = "freq-solves/s @5.4k panels: surrogate+mixed vs plain FP64 GPU @≤1e-4 rel err"
 UNIT = "freq-solves/s"
 RHO, G = 1025.0, 9.81
-LANES = 4  # frequencies in flight in hams_solve_batch (the library's default)
+LANES = 8  # frequencies in flight in hams_solve_batch (the library's default)
 SG_FAR = 3.0  # surrogate pairs: centre distance beyond 3 source-panel sizes
 # Frequencies the surrogate serves, by K = k0 h tanh(k0 h): on this array the
 # damping below 0.26 rad/s (K < 0.3) and the excitation above 2.05 rad/s
@@ -64,8 +64,11 @@ WORKLOAD = "3x3 cylinder array R=4 T=8 spacing 20 m, 5400 quad panels, depth 50 
 # (profiles/k_green_series_eigene_c2_array.md).
 EIGENE_FP64_FLOPS_PER_PAIR = None
 EIGENE_DRAM_BYTES_PER_LAUNCH = None
-# DRAM bytes of one launch of the surrogate kernel on this workload (ncu), or None
-SG_DRAM_BYTES_PER_LAUNCH = None
+# DRAM bytes of one launch of the surrogate kernel on this workload: ncu's
+# dram__bytes_read.sum + dram__bytes_write.sum on the 3,240-panel profiling
+# case (642.0 MB for 10,233,540 pairs, 62.7 B per pair) scaled to the
+# 28,496,520 pairs of a full launch (profiles/k_green_sg_c2_array.md)
+SG_DRAM_BYTES_PER_LAUNCH = 62.73 * 28_496_520
 
 
 # A coarser copy of the array (3,240 panels, 10.2 M far pairs) that profilers
@@ -419,7 +422,8 @@ def gpu_arm(args):
                             "peak": peak, "frac": ach / peak if peak else None, "traffic": SG_DRAM_BYTES_PER_LAUNCH,
                             "peak_source": "of measured: dense bf16 cuBLAS burst (MEASURED_PEAKS.json); the kernel "
                                            "runs tcgen05.mma kind::f16 (FP16 operands, FP32 accumulation)",
-                            "launch_ms": sg_ms, "launch_ms_in_timed_region": tm["green_surrogate"] or None,
+                            "launch_ms": sg_ms,
+                            "launch_ms_in_timed_region": tm["green_surrogate"] if tm["pairs_surrogate"] else None,
                             "pairs_per_launch": sg_pairs, "flops_per_pair": flops,
                             "timing": "mean of 5 launches on one lane (nothing else running), CUDA events on the "
                                       "launching stream"}

@@ -1396,7 +1396,7 @@ extern "C" int hams_solve_frequency(hams_ctx* c, const hams_wave* w, int32_t nbe
 }
 
 // Frequencies in flight at once in hams_solve_batch when opts.batch_lanes is 0.
-constexpr int kDefaultLanes = 4;
+constexpr int kDefaultLanes = 8;
 
 extern "C" int hams_solve_batch(hams_ctx* c, int32_t nfreq, const hams_wave* waves, int32_t nbeta, const double* beta,
                                 double* amas, double* bdmp, double* exfc) {

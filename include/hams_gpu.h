@@ -103,7 +103,7 @@ typedef struct hams_opts {
   double refine_tol;/* mixed: relative residual target of the refinement (<=0: 1e-12) */
   int32_t refine_max;/* mixed: refinement sweeps (<=0: 30)                       */
   int32_t lu_kind;  /* mixed: HAMS_LU_BLOCK_TF32 (0), HAMS_LU_BLOCK_EMU, HAMS_LU_LIBRARY */
-  int32_t batch_lanes;/* hams_solve_batch: frequencies in flight (<=0: 4)          */
+  int32_t batch_lanes;/* hams_solve_batch: frequencies in flight (<=0: 8)          */
   int32_t solver;   /* HAMS_SOLVER_LU (0 or 1) or HAMS_SOLVER_GMRES (2), ISOLV     */
   int32_t gmres_restart;/* GMRES restart length (<=0: 25, IterativeSolvers.f90:56) */
   int32_t gmres_maxit;  /* GMRES iterations over all restarts (<=0: 100, :58)    */
