@@ -18,11 +18,13 @@
 
 #include <cctype>
 #include <cmath>
+#include <complex>
 #include <cstdint>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <fstream>
+#include <iomanip>
 #include <sstream>
 #include <stdexcept>
 #include <string>
@@ -154,6 +156,10 @@ struct Deck {
   std::vector<double> xyz, xyz_p, ds, pnsz, dxyz, ixyz_p;
   std::vector<int> ncn, ncon, body_nelem;
   int inelem = 0;
+  double refl = 1.0;             // reference body length (REFL)
+  std::vector<double> xfp;       // field points (nfp,3) column-major
+  int nfp = 0;
+  bool separate = false;         // separate_wamit_diffraction_radiation_files
 };
 
 Deck load(const std::string& dir) {
@@ -210,7 +216,7 @@ Deck load(const std::string& dir) {
     const std::string l = r.next();
     for (int k = 0; k < 3; ++k) d.xr[b + nb * k] = fortran_real(field(l, 28 + 12 * k, 12), 3);
   }
-  read_f(r, 26, 30, 15);  // reference body length (not used by this path)
+  d.refl = read_f(r, 26, 30, 15);
   d.isol = read_i(r, 26, 16);
   d.irsp = read_i(r, 23, 16);
   read_i(r, 23, 16);  // NTHREAD
@@ -219,6 +225,25 @@ Deck load(const std::string& dir) {
       d.isolv = (int)std::strtol(field(*l, 26, 16).c_str(), nullptr, 10);
       r.next();
     }
+  // field points and the WAMIT output option (InputFiles.f90:190-220)
+  r.next();
+  r.next();
+  if (const std::string* l = r.peek())
+    if (l->find("field_points") != std::string::npos) {
+      d.nfp = read_i(r, 27, 16);
+      if (d.nfp < 0) throw std::runtime_error("negative number of field points");
+      d.xfp.assign(3 * (size_t)d.nfp, 0.0);
+      for (int i = 0; i < d.nfp; ++i) {
+        auto v = read_list(r, 3);
+        for (int k = 0; k < 3; ++k) d.xfp[i + (size_t)d.nfp * k] = v[k];
+      }
+      r.next();
+      r.next();
+      if (const std::string* o = r.peek())
+        if (o->find("separate") != std::string::npos || o->find("Separate") != std::string::npos)
+          d.separate = std::strtol(field(*o, 50, 16).c_str(), nullptr, 10) != 0;
+    }
+  if (d.nbody == 1) d.separate = false;
 
   // meshes, bodies stacked in order, local coordinates rotated and shifted
   std::vector<Mesh> hull(nb), lid(nb);
@@ -345,6 +370,40 @@ std::string fmt_e(int w, int dg, double v) {
   return out;
 }
 
+// Fortran ESw.d (one digit before the point, two-digit exponent).
+std::string fmt_es(int w, int dg, double v) {
+  char out[64];
+  std::snprintf(out, sizeof(out), "%*.*E", w, dg, v);
+  return out;
+}
+
+typedef std::complex<double> zc;
+
+// WamitNondimensMulti (PressureElevationMulti.f90:353-399): pressure or
+// elevation of a radiation mode md (1..6) or of a diffraction/incident field
+// (md = 0) in WAMIT's nondimensional form and sign convention.
+zc wamit_nondim(zc vcp, bool pressure, bool radiation, int md, bool limit, double rho, double g, double amp,
+                double refl, double w1) {
+  const double nfac = pressure ? (limit ? rho * amp : rho * g * amp) : amp;
+  zc nv;
+  if (!radiation) {
+    nv = vcp / nfac;
+  } else {
+    const int mexp = md <= 3 ? 0 : 1;
+    nv = limit ? vcp / nfac * amp / std::pow(refl, mexp + 1) : vcp / nfac * zc(0.0, -w1) * amp / std::pow(refl, mexp);
+  }
+  if (std::abs(nv) < 1.E-15) nv = 0.0;
+  return radiation ? zc(nv.real(), -nv.imag()) : zc(-nv.imag(), -nv.real());
+}
+
+// Pressure (i w rho phi) or elevation (i w / g phi) of a potential
+// (CalPressureMulti / CalElevationMulti, :305-348), rho phi and phi at the
+// zero and infinite frequency limits.
+zc pressure_or_elevation(zc pot, bool pressure, bool limit, double rho, double g, double w1) {
+  if (pressure) return limit ? rho * pot : zc(0.0, w1 * rho) * pot;
+  return limit ? pot : zc(0.0, w1 / g) * pot;
+}
+
 std::vector<float> read_params(const std::string& path) {
   std::ifstream f(path, std::ios::binary);
   if (!f) throw std::runtime_error("cannot open " + path);
@@ -352,6 +411,99 @@ std::vector<float> read_params(const std::string& path) {
   f.read(reinterpret_cast<char*>(p.data()), p.size() * sizeof(float));
   if (f.gcount() != (std::streamsize)(p.size() * sizeof(float))) throw std::runtime_error(path + ": short parameter file");
   return p;
+}
+
+// Output frequency of a wave (CalWaveProperts OUFR, ImplementSubs.f90:139-149).
+double out_freq(const hams_wave& w, int ouft) {
+  switch (ouft) {
+    case 1: return w.v;
+    case 2: return w.wk;
+    case 4: return w.tp;
+    case 5: return w.wl;
+    default: return w.w1;
+  }
+}
+
+// WAMIT-format field-point files (OutputPressureElevation_*Multi,
+// PressureElevationMulti.f90:404-590, and the single-body writers of
+// PressureElevation.f90:391-461): per frequency the radiation lines, then per
+// heading the diffraction lines and (several bodies) the incident-wave lines.
+// Points below the free surface give pressures, points on it elevations.
+void write_field_points(const std::string& out, const Deck& d, const std::vector<hams_wave>& waves,
+                        const std::vector<std::vector<zc>>& fpot, const hams_opts& o) {
+  const std::string wd = out + "/Wamit_format";
+  mkdir(out.c_str(), 0755);
+  mkdir(wd.c_str(), 0755);
+  const int nb = d.nbody, ndof = 6 * nb, nbeta = (int)d.wvhd.size(), nfp = d.nfp;
+  const bool multi = nb > 1;
+  std::ofstream main_f, dif_f, inc_f;
+  std::vector<std::ofstream> rad_f;
+  if (d.separate) {
+    dif_f.open(wd + "/PressureElevationDiffraction.6p");
+    rad_f.resize(nb);
+    for (int b = 0; b < nb; ++b) rad_f[b].open(wd + "/PressureElevationRadiation_" + std::to_string(b + 1) + ".6p");
+  } else {
+    main_f.open(wd + "/PressureElevation.6p");
+  }
+  if (multi) inc_f.open(wd + "/PressureElevationIncidence.6p");
+  std::ofstream& dif = d.separate ? dif_f : main_f;
+  const double kPi = 3.141592653589793;
+  for (size_t k = 0; k < fpot.size(); ++k) {
+    const hams_wave& w = waves[k];
+    const bool limit = std::fabs(w.tp + 1.0) < 1.E-6 || std::fabs(w.tp) < 1.E-6;
+    const double oufr = out_freq(w, d.ouft);
+    auto at = [&](int f, int col) { return fpot[k][f + (size_t)nfp * col]; };
+    auto field = [&](int f, int col, bool radiation, int md) {
+      const bool pressure = std::fabs(d.xfp[f + 2 * (size_t)nfp]) > 1.E-6;
+      const zc v = pressure_or_elevation(at(f, col), pressure, limit, o.rho, o.g, w.w1);
+      return wamit_nondim(v, pressure, radiation, md, limit, o.rho, o.g, o.amp, d.refl, w.w1);
+    };
+    // radiation
+    for (int f = 0; f < nfp; ++f) {
+      if (!multi) {
+        if (!(std::fabs(d.xfp[f + 2 * (size_t)nfp]) > 1.E-6)) continue;  // single body: submerged points only
+        main_f << fmt_es(14, 6, oufr) << std::setw(10) << f + 1;
+        for (int md = 1; md <= 6; ++md) {
+          const zc v = field(f, md - 1, true, md);
+          main_f << fmt_es(14, 6, v.real()) << fmt_es(14, 6, v.imag());
+        }
+        main_f << '\n';
+        continue;
+      }
+      if (!d.separate) main_f << fmt_es(14, 6, oufr) << std::setw(10) << f + 1;
+      for (int b = 0; b < nb; ++b) {
+        std::ostringstream line;
+        for (int md = 1; md <= 6; ++md) {
+          const zc v = field(f, 6 * b + md - 1, true, md);
+          line << fmt_es(14, 6, v.real()) << fmt_es(14, 6, v.imag());
+        }
+        if (d.separate)
+          rad_f[b] << fmt_es(14, 6, oufr) << std::setw(10) << f + 1 << line.str() << '\n';
+        else
+          main_f << (b == 0 ? "" : std::string(24, ' ')) << line.str() << '\n';
+      }
+    }
+    // diffraction and incident wave, per heading
+    for (int ib = 0; ib < nbeta; ++ib) {
+      const double bdeg = (d.wvhd[ib] * kPi / 180.0) * 180.0 / kPi;
+      for (int f = 0; f < nfp; ++f) {
+        const zc v = field(f, ndof + ib, false, 0);
+        dif << fmt_es(14, 6, oufr) << fmt_es(14, 6, bdeg) << std::setw(10) << f + 1;
+        if (multi)
+          dif << fmt_es(14, 6, v.real()) << fmt_es(14, 6, v.imag()) << '\n';
+        else
+          dif << fmt_es(14, 6, std::abs(v)) << fmt_es(14, 6, std::atan2(v.imag(), v.real()) * 180.0 / kPi)
+              << fmt_es(14, 6, v.real()) << fmt_es(14, 6, v.imag()) << '\n';
+      }
+      if (multi)
+        for (int f = 0; f < nfp; ++f) {
+          const zc v = field(f, ndof + nbeta + ib, false, 0);
+          inc_f << fmt_es(14, 6, oufr) << fmt_es(14, 6, bdeg) << std::setw(10) << f + 1 << fmt_es(14, 6, std::abs(v))
+                << fmt_es(14, 6, std::atan2(v.imag(), v.real()) * 180.0 / kPi) << fmt_es(14, 6, v.real())
+                << fmt_es(14, 6, v.imag()) << '\n';
+        }
+    }
+  }
 }
 
 int usage() {
@@ -415,6 +567,8 @@ int main(int argc, char** argv) {
       if (hams_ctx_set_surrogate(ctx, p.data(), (int32_t)p.size(), far))
         throw std::runtime_error(std::string("surrogate: ") + hams_last_error());
     }
+    if (d.nfp > 0 && hams_ctx_set_field_points(ctx, d.nfp, d.xfp.data()))
+      throw std::runtime_error(std::string("field points: ") + hams_last_error());
     std::vector<hams_wave> waves(nf);
     for (int k = 0; k < nf; ++k)
       if (hams_wave_properties(d.inft, d.wvnb[k], d.h, g, d.sybo == 1 && k < 2 ? k + 1 : 0, &waves[k]))
@@ -424,6 +578,12 @@ int main(int argc, char** argv) {
     std::vector<double> amas((size_t)nf * ndof * ndof), bdmp(amas.size()), exfc(2 * (size_t)nf * std::max(nbeta, 1) * ndof);
     int rc = hams_solve_batch(ctx, nf, waves.data(), nbeta, beta.data(), amas.data(), bdmp.data(), exfc.data());
     if (rc >= 0 && *hams_last_note(ctx)) std::fprintf(stderr, "hams_b200_run: %s\n", hams_last_note(ctx));
+    // field-point potentials of every frequency: (nfp, 6nb + 2 nbeta) each
+    const size_t fpn = (size_t)d.nfp * (ndof + 2 * nbeta);
+    std::vector<std::vector<zc>> fpot(d.nfp > 0 && rc >= 0 ? nf : 0, std::vector<zc>(fpn));
+    for (int k = 0; k < (int)fpot.size(); ++k)
+      if (hams_field_potentials(ctx, k, reinterpret_cast<double*>(fpot[k].data())))
+        throw std::runtime_error(std::string("field potentials: ") + hams_last_error());
     hams_ctx_destroy(ctx);
     if (rc < 0) throw std::runtime_error(std::string("solve: ") + hams_last_error());
     if (rc > 0) std::fprintf(stderr, "hams_b200_run: singular pivot %d\n", rc);
@@ -458,6 +618,7 @@ int main(int argc, char** argv) {
           }
       }
     }
+    if (d.nfp > 0) write_field_points(out, d, waves, fpot, o);
     std::printf("hams_b200_run: %d frequencies, %d headings, %d panels, %d bodies -> %s\n", nf, nbeta, d.nelem, nb,
                 hd.c_str());
   } catch (const std::exception& e) {

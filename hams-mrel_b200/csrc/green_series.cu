@@ -8,6 +8,7 @@
 // transcendental functions inside them come from detmath.h.  The remaining
 // kernels (hams_gpu.cu) keep fused multiply-adds.
 #include "kernels.cuh"
+#include "rankine.cuh"
 
 // 128 threads and at most 64 registers per thread (8 blocks per SM): the
 // series are latency-bound, and the extra resident warps outweigh the few
@@ -131,6 +132,74 @@ __global__ void k_eval_green(int npts, const double* __restrict__ pts, const int
   for (int k = 0; k < 4; ++k) out[t + (size_t)k * npts] = make_double2(G.g[k].re, G.g[k].im);
 }
 
+
+// Source (S) and normal-dipole (D) influence of every hull panel J at field
+// point f, the terms CalPotentialMulti sums (PressureElevationMulti.f90:81-137):
+// S = FLAG*SIJ + G ds, D = (FLAG*DIJ + grad G ds) . n_J, with the Rankine
+// integrals at the field point (SGLINTBD_MULTI_QUAD2/TRI2,
+// SingularIntgrMulti.f90:454-776) and FLAG = (distance <= 50 PNSZ_J).
+__global__ void k_field_pairs(DevGeom g, WaveDev w, const double* __restrict__ wvn, int nfp,
+                              const double* __restrict__ xfp, double2* __restrict__ Sf, double2* __restrict__ Df,
+                              int* ovf) {
+  const int f = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y;
+  if (f >= nfp) return;
+  const double xp = xfp[f], yp = xfp[f + nfp], zp = xfp[f + 2 * (size_t)nfp];
+  const double xq = g.xq[j], yq = g.xq[j + g.n], zq = g.xq[j + 2 * g.n];
+  const double dist = sqrt((xp - xq) * (xp - xq) + (yp - yq) * (yp - yq) + (zp - zq) * (zp - zq));
+  const int flag = dist <= 50.0 * g.pnsz[j] ? 1 : 0;
+  const double xf[3] = {xp, yp, zp};
+  hams::rk4 r;
+  if (g.ncn[j] == 3) {
+    double q[3][3];
+    for (int v = 0; v < 3; ++v)
+      for (int c = 0; c < 3; ++c) q[v][c] = g.vtx[(size_t)j * 12 + v * 3 + c];
+    r = hams::sglint_tri(xf, q);
+  } else {
+    double q[4][3];
+    for (int v = 0; v < 4; ++v)
+      for (int c = 0; c < 3; ++c) q[v][c] = g.vtx[(size_t)j * 12 + v * 3 + c];
+    r = hams::sglint_quad(xf, q);
+  }
+  grn4 G;
+  if (w.limit) {
+    G = hams::green_limit(w.limit == 2, xq, xp, yq, yp, zq, zp, flag);
+  } else if (w.h < 0.0) {
+    G = hams::infgreen3d(xq, xp, yq, yp, zq, zp, w.v, flag);
+  } else {
+    int o = 0;
+    const double rr = sqrt((xq - xp) * (xq - xp) + (yq - yp) * (yq - yp));
+    switch (hams::fin_branch(rr, w.h)) {
+      case hams::kLinton: G = hams::fingreen3d<hams::kLinton>(xq, xp, yq, yp, zq, zp, w.v, wvn, w.h, flag, (void*)nullptr, &o); break;
+      case hams::kPidcock: {
+        hams::SeriesScratchN<hams::kPidcockMax> sc;
+        G = hams::fingreen3d<hams::kPidcock>(xq, xp, yq, yp, zq, zp, w.v, wvn, w.h, flag, &sc, &o);
+        break;
+      }
+      case hams::kEigenE: {
+        hams::SeriesScratchN<hams::kEigenEMax> sc;
+        G = hams::fingreen3d<hams::kEigenE>(xq, xp, yq, yp, zq, zp, w.v, wvn, w.h, flag, &sc, &o);
+        break;
+      }
+      default: G = hams::fingreen3d<hams::kEigen>(xq, xp, yq, yp, zq, zp, w.v, wvn, w.h, flag, (void*)nullptr, &o); break;
+    }
+    if (o) atomicOr(ovf, 1);
+  }
+  const double ds = g.ds[j], n1 = g.nrm[j], n2 = g.nrm[j + g.n], n3 = g.nrm[j + 2 * g.n];
+  double sre = G.g[0].re * ds, sim = G.g[0].im * ds;
+  double dre = (G.g[1].re * n1 + G.g[2].re * n2 + G.g[3].re * n3) * ds;
+  double dim = (G.g[1].im * n1 + G.g[2].im * n2 + G.g[3].im * n3) * ds;
+  if (flag) {
+    sre = r.s + G.g[0].re * ds;
+    dre = (r.dx + G.g[1].re * ds) * n1 + (r.dy + G.g[2].re * ds) * n2 + (r.dz + G.g[3].re * ds) * n3;
+  }
+  Sf[f + (size_t)nfp * j] = make_double2(sre, sim);
+  Df[f + (size_t)nfp * j] = make_double2(dre, dim);
+}
+
+void launch_field_pairs(cudaStream_t st, DevGeom g, WaveDev w, const double* wvn, int nfp, const double* xfp,
+                        double2* Sf, double2* Df, int* ovf) {
+  k_field_pairs<<<dim3((nfp + 127) / 128, g.n), 128, 0, st>>>(g, w, wvn, nfp, xfp, Sf, Df, ovf);
+}
 
 void launch_eval_green(unsigned blocks, cudaStream_t st, int npts, const double* pts, const int* flag, WaveDev w,
                        const double* wvn, double2* out, int* ovf) {

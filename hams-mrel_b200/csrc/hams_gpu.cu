@@ -257,6 +257,46 @@ __device__ __forceinline__ cplx vinp(const IncWave& q, double x, double y, doubl
   return e * (dum * cosh(q.wk0 * (z + q.h)));
 }
 
+// Boundary values of the field-point potentials (CalPotentialMulti,
+// PressureElevationMulti.f90:161-230): column 6b+m the generalized normal m
+// on the panels of body b (FACTOR_NORMAL), column 6nb+k minus the incident
+// normal velocity of heading k.
+__global__ void k_field_bc(DevGeom g, int nbeta, const double2* __restrict__ wd, double2* __restrict__ bc) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x, col = blockIdx.y;
+  if (j >= g.n) return;
+  double2 v = make_double2(0.0, 0.0);
+  if (col < 6 * g.nb) {
+    if (g.body[j] == col / 6) v.x = g.nrm[j + (size_t)(col % 6) * g.n];
+  } else {
+    const double2 q = wd[j + (size_t)(col - 6 * g.nb) * g.n];
+    v = make_double2(-q.x, -q.y);
+  }
+  bc[j + (size_t)g.n * col] = v;
+}
+
+// out (nfp, ncol + nbeta): the summed potentials over 2 pi or 4 pi, the
+// incident potential added to the diffraction columns of the total-potential
+// solution (PressureElevationMulti.f90:253-266), then the incident potential
+// alone per heading (CalPotentialIncMulti, :277-300).
+__global__ void k_field_finish(int nfp, int ncol, int nrad, int nbeta, const double* __restrict__ xfp,
+                               const double* __restrict__ sld, IncWave q, const double* __restrict__ beta, int add_inc,
+                               const double2* __restrict__ pot, double2* __restrict__ out) {
+  const int f = blockIdx.x * blockDim.x + threadIdx.x, col = blockIdx.y;
+  if (f >= nfp) return;
+  cplx inc = hams::cmk(0.0, 0.0);
+  const int k = col < ncol ? col - nrad : col - ncol;
+  if (add_inc && (col >= ncol || col >= nrad)) inc = vinp(q, xfp[f], xfp[f + nfp], xfp[f + 2 * (size_t)nfp], beta[k]);
+  double2 v;
+  if (col < ncol) {
+    const double2 p = pot[f + (size_t)nfp * col];
+    v = make_double2(p.x / sld[f], p.y / sld[f]);
+    if (col >= nrad) v = make_double2(v.x + inc.re, v.y + inc.im);
+  } else {
+    v = make_double2(inc.re, inc.im);
+  }
+  out[f + (size_t)nfp * col] = v;
+}
+
 // w(J,beta) = grad(phi_I)(x_J) . n_J for every source panel and heading
 __global__ void k_dbc_weights(DevGeom g, WaveDev w, IncWave q, const double* __restrict__ beta, int nbeta,
                               double2* __restrict__ wd) {
@@ -521,6 +561,16 @@ struct hams_ctx {
   int n = 0, nl = 0, tn = 0, nb = 0;
   std::vector<int> body_nelem;
   std::vector<double> xyz_p;  // hull panel centres (n x 3), host copy for the H-matrix cluster tree
+  std::vector<double> vtx_h, pnsz_h, nrm_h;  // host copies for the field points' on-body test
+  std::vector<int> ncn_h;
+  // field points (hams_ctx_set_field_points): coordinates, 2 pi / 4 pi per
+  // point, and the potentials of the last solve (host) or of each frequency
+  // of the last batch
+  int nfp = 0;
+  DBuf<double> fp_x, fp_sld;
+  DBuf<double2> fp_S, fp_D, fp_bc, fp_pot, fp_out;
+  std::vector<double> fp_last;
+  std::vector<std::vector<double>> fp_batch;
   bool hm_ready = false;      // GMRES: cluster tree uploaded to hm
   hmat::Dev hm;
   DBuf<double2> hxp, hyp, hw;  // H-matrix product work arrays
@@ -683,6 +733,10 @@ static int ctx_setup(hams_ctx* c, const hams_geom* geo) {
   TRY(c->xq.alloc(3 * (size_t)n)); TRY(c->fxyz.alloc(3 * (size_t)tn)); TRY(c->ds.alloc(n)); TRY(c->pnsz.alloc(n));
   TRY(c->nrm.alloc(6 * (size_t)n)); TRY(c->vtx.alloc(12 * (size_t)n)); TRY(c->ncn.alloc(n)); TRY(c->body.alloc(n));
   TRY(c->bstart.alloc(nb + 1));
+  c->vtx_h = vtx;
+  c->ncn_h.assign(geo->ncn, geo->ncn + n);
+  c->pnsz_h.assign(geo->pnsz, geo->pnsz + n);
+  c->nrm_h.assign(geo->dxyz, geo->dxyz + 6 * (size_t)n);
   CU(cudaMemcpyAsync(c->xq.p, xq.data(), 3 * (size_t)n * 8, cudaMemcpyHostToDevice, c->st));
   CU(cudaMemcpyAsync(c->fxyz.p, fx.data(), 3 * (size_t)tn * 8, cudaMemcpyHostToDevice, c->st));
   CU(cudaMemcpyAsync(c->ds.p, geo->ds, (size_t)n * 8, cudaMemcpyHostToDevice, c->st));
@@ -777,6 +831,11 @@ static int make_lane(hams_ctx* c, hams_ctx** out) {
   l->nb = c->nb;
   l->body_nelem = c->body_nelem;
   l->xyz_p = c->xyz_p;
+  l->nfp = c->nfp;
+  if (c->nfp > 0) {
+    l->fp_x.view(c->fp_x);
+    l->fp_sld.view(c->fp_sld);
+  }
   int rc = ctx_handles(l);
   if (!rc) {
     l->xq.view(c->xq); l->fxyz.view(c->fxyz); l->ds.view(c->ds); l->pnsz.view(c->pnsz); l->nrm.view(c->nrm);
@@ -1341,6 +1400,40 @@ static int forces_dev(hams_ctx* c, const hams_wave* w, int nbeta) {
   return launch_check(c);
 }
 
+// Potentials at the field points from the solved panel potentials X
+// (CalPotentialMulti, PressureElevationMulti.f90:55-272): the influence of
+// every panel at every point (k_field_pairs), then
+// POT = (S_f BC - D_f X) / (2 pi or 4 pi) as two complex GEMMs, the incident
+// potential added for the total-potential solution; copied to fp_last.
+static int field_dev(hams_ctx* c, const hams_wave* w, int nbeta) {
+  const int n = c->n, nfp = c->nfp, nrad = 6 * c->nb, ncol = nrad + nbeta;
+  const cuDoubleComplex one = make_cuDoubleComplex(1.0, 0.0), zero = make_cuDoubleComplex(0.0, 0.0),
+                        mone = make_cuDoubleComplex(-1.0, 0.0);
+  WaveDev wd = wave_dev(c, w);
+  TRY(c->fp_S.alloc((size_t)nfp * n));
+  TRY(c->fp_D.alloc((size_t)nfp * n));
+  TRY(c->fp_bc.alloc((size_t)n * ncol));
+  TRY(c->fp_pot.alloc((size_t)nfp * ncol));
+  TRY(c->fp_out.alloc((size_t)nfp * (ncol + nbeta)));
+  launch_field_pairs(c->st, c->g, wd, c->wvn.p, nfp, c->fp_x.p, c->fp_S.p, c->fp_D.p, c->ovf.p);
+  k_field_bc<<<dim3((n + 127) / 128, ncol), 128, 0, c->st>>>(c->g, nbeta, c->wd.p, c->fp_bc.p);
+  TRY(launch_check(c, 2));
+  CUB_(cublasZgemm(c->blas, CUBLAS_OP_N, CUBLAS_OP_N, nfp, ncol, n, &one, (cuDoubleComplex*)c->fp_S.p, nfp,
+                   (cuDoubleComplex*)c->fp_bc.p, n, &zero, (cuDoubleComplex*)c->fp_pot.p, nfp));
+  CUB_(cublasZgemm(c->blas, CUBLAS_OP_N, CUBLAS_OP_N, nfp, ncol, n, &mone, (cuDoubleComplex*)c->fp_D.p, nfp,
+                   (cuDoubleComplex*)c->X.p, n, &one, (cuDoubleComplex*)c->fp_pot.p, nfp));
+  c->lib_calls += 2;
+  IncWave q = inc_params(wd, c->opts.amp, c->opts.g, c->opts.xw[0], c->opts.xw[1]);
+  const int add_inc = c->opts.isol == 1 && !wd.limit;
+  k_field_finish<<<dim3((nfp + 127) / 128, ncol + nbeta), 128, 0, c->st>>>(nfp, ncol, nrad, nbeta, c->fp_x.p,
+                                                                            c->fp_sld.p, q, c->beta.p, add_inc,
+                                                                            c->fp_pot.p, c->fp_out.p);
+  TRY(launch_check(c));
+  c->fp_last.resize(2 * (size_t)nfp * (ncol + nbeta));
+  CU(cudaMemcpyAsync(c->fp_last.data(), c->fp_out.p, c->fp_last.size() * 8, cudaMemcpyDeviceToHost, c->st));
+  return 0;
+}
+
 static int solve_one(hams_ctx* c, const hams_wave* w, int nbeta, const double* beta, double* amas, double* bdmp,
                      double* exfc) {
   const int ndof = 6 * c->nb;
@@ -1352,6 +1445,7 @@ static int solve_one(hams_ctx* c, const hams_wave* w, int nbeta, const double* b
   TRY(solve_dev(c, ndof + nbeta, &info));
   CU(cudaEventRecord(c->ev[3], c->st));
   TRY(forces_dev(c, w, nbeta));
+  if (c->nfp > 0) TRY(field_dev(c, w, nbeta));
   CU(cudaEventRecord(c->ev[4], c->st));
   double* o = c->outbuf.p;
   if (amas) CU(cudaMemcpyAsync(amas, o, (size_t)ndof * ndof * 8, cudaMemcpyDeviceToHost, c->st));
@@ -1389,6 +1483,7 @@ static int solve_one(hams_ctx* c, const hams_wave* w, int nbeta, const double* b
 
 extern "C" int hams_solve_frequency(hams_ctx* c, const hams_wave* w, int32_t nbeta, const double* beta, double* amas,
                                     double* bdmp, double* exfc) {
+  if (c) c->fp_batch.clear();
   g_err.clear();
   if (!c || !w || (nbeta > 0 && !beta)) return fail(HAMS_ERR_ARG, "null argument");
   if (cudaSetDevice(c->dev) != cudaSuccess) return fail(HAMS_ERR_CUDA, "cudaSetDevice failed");
@@ -1416,6 +1511,7 @@ extern "C" int hams_solve_batch(hams_ctx* c, int32_t nfreq, const hams_wave* wav
   for (int t = 0; t + 1 < L; ++t) lane.push_back(c->lanes[t]);
   std::vector<int> rc_of(nfreq, 0), lane_rc(L, 0);
   std::vector<std::string> lane_err(L), note_of(nfreq);
+  c->fp_batch.assign(c->nfp > 0 ? nfreq : 0, std::vector<double>());
   // lane t solves frequencies t, t + L, ... on its own stream and host thread
   auto run = [&](int t) {
     if (cudaSetDevice(c->dev) != cudaSuccess) {
@@ -1433,6 +1529,7 @@ extern "C" int hams_solve_batch(hams_ctx* c, int32_t nfreq, const hams_wave* wav
       }
       rc_of[k] = rc;
       note_of[k] = lane[t]->note;
+      if (c->nfp > 0) c->fp_batch[k] = lane[t]->fp_last;
       // scatter into (nfreq, ...) column-major arrays with the frequency index leading
       for (size_t e = 0; e < (size_t)ndof * ndof; ++e) {
         if (amas) amas[k + e * nfreq] = a[e];
@@ -1661,6 +1758,79 @@ extern "C" int hams_last_timings(hams_ctx* c, double* ms, int32_t n) {
 }
 
 extern "C" const char* hams_last_note(hams_ctx* c) { return c ? c->note.c_str() : ""; }
+
+extern "C" int hams_ctx_set_field_points(hams_ctx* c, int32_t nfp, const double* xfp) {
+  g_err.clear();
+  if (!c || c->is_lane) return fail(HAMS_ERR_ARG, "null context");
+  if (nfp < 0 || (nfp > 0 && !xfp)) return fail(HAMS_ERR_ARG, "bad field points");
+  if (cudaSetDevice(c->dev) != cudaSuccess) return fail(HAMS_ERR_CUDA, "cudaSetDevice failed");
+  for (hams_ctx* l : c->lanes) CU(cudaStreamSynchronize(l->st));
+  CU(cudaStreamSynchronize(c->st));
+  c->nfp = nfp;
+  c->fp_last.clear();
+  c->fp_batch.clear();
+  if (nfp > 0) {
+    // 2 pi for a point on a hull panel (in its plane and inside its edges),
+    // 4 pi in the fluid (PressureElevationMulti.f90:203-252)
+    const int n = c->n;
+    std::vector<double> sld(nfp);
+    for (int f = 0; f < nfp; ++f) {
+      const double x[3] = {xfp[f], xfp[f + nfp], xfp[f + 2 * (size_t)nfp]};
+      bool onbody = false;
+      for (int j = 0; j < n && !onbody; ++j) {
+        const double* e = &c->nrm_h[j];
+        const double en[3] = {e[0], e[(size_t)n], e[2 * (size_t)n]};
+        const double tolp = std::max(1e-6, 1e-3 * c->pnsz_h[j]), tola = 1e-3 * c->pnsz_h[j] * c->pnsz_h[j];
+        const double* v0 = &c->vtx_h[(size_t)j * 12];
+        const double dpln = (x[0] - v0[0]) * en[0] + (x[1] - v0[1]) * en[1] + (x[2] - v0[2]) * en[2];
+        if (std::fabs(dpln) > tolp) continue;
+        double smin = 1e30, smax = -1e30;
+        const int nv = c->ncn_h[j];
+        for (int k = 0; k < nv; ++k) {
+          const double* a = &c->vtx_h[(size_t)j * 12 + 3 * k];
+          const double* b = &c->vtx_h[(size_t)j * 12 + 3 * ((k + 1) % nv)];
+          const double ev[3] = {b[0] - a[0], b[1] - a[1], b[2] - a[2]};
+          const double wv[3] = {x[0] - a[0], x[1] - a[1], x[2] - a[2]};
+          const double sv = (ev[1] * wv[2] - ev[2] * wv[1]) * en[0] + (ev[2] * wv[0] - ev[0] * wv[2]) * en[1] +
+                            (ev[0] * wv[1] - ev[1] * wv[0]) * en[2];
+          smin = std::min(smin, sv);
+          smax = std::max(smax, sv);
+        }
+        if (smin >= -tola || smax <= tola) onbody = true;
+      }
+      sld[f] = (onbody ? 2.0 : 4.0) * 3.141592653589793;
+    }
+    TRY(c->fp_x.alloc(3 * (size_t)nfp));
+    TRY(c->fp_sld.alloc(nfp));
+    CU(cudaMemcpy(c->fp_x.p, xfp, 3 * (size_t)nfp * 8, cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(c->fp_sld.p, sld.data(), (size_t)nfp * 8, cudaMemcpyHostToDevice));
+  }
+  for (hams_ctx* l : c->lanes) {
+    l->nfp = nfp;
+    l->fp_last.clear();
+    if (nfp > 0) {
+      l->fp_x.view(c->fp_x);
+      l->fp_sld.view(c->fp_sld);
+    }
+  }
+  return 0;
+}
+
+extern "C" int hams_field_potentials(hams_ctx* c, int32_t k, double* pot) {
+  g_err.clear();
+  if (!c || !pot) return fail(HAMS_ERR_ARG, "null argument");
+  const std::vector<double>* src = nullptr;
+  if (!c->fp_batch.empty()) {
+    if (k < 0 || k >= (int)c->fp_batch.size()) return fail(HAMS_ERR_ARG, "frequency %d not in the last batch", k);
+    src = &c->fp_batch[k];
+  } else {
+    if (k != 0) return fail(HAMS_ERR_ARG, "frequency %d: the last solve was a single frequency", k);
+    src = &c->fp_last;
+  }
+  if (src->empty()) return fail(HAMS_ERR_ARG, "no field potentials (no field points, or no solve since they were set)");
+  std::memcpy(pot, src->data(), src->size() * 8);
+  return 0;
+}
 
 extern "C" int64_t hams_launch_count(hams_ctx* c) {
   if (!c) return 0;

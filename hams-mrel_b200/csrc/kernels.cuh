@@ -60,3 +60,6 @@ void launch_mode_tables(cudaStream_t st, DevGeom g, WaveDev w, const double* wvn
                         double2* src, double2* srct, double* fld, double* fldt);
 void launch_eval_green(unsigned blocks, cudaStream_t st, int npts, const double* pts, const int* flag, WaveDev w,
                        const double* wvn, double2* out, int* ovf);
+// Influence of every hull panel at nfp field points xfp (nfp,3): Sf, Df (nfp x n).
+void launch_field_pairs(cudaStream_t st, DevGeom g, WaveDev w, const double* wvn, int nfp, const double* xfp,
+                        double2* Sf, double2* Df, int* ovf);

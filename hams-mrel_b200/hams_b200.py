@@ -93,6 +93,8 @@ def load_library(path=LIB_PATH):
     lib.hams_surrogate_param_count.restype = c_int
     lib.hams_ctx_set_surrogate.argtypes = [ctypes.c_void_p, P_flt, c_int, c_dbl]
     lib.hams_ctx_set_surrogate_range.argtypes = [ctypes.c_void_p, c_dbl, c_dbl]
+    lib.hams_ctx_set_field_points.argtypes = [ctypes.c_void_p, c_int, P_dbl]
+    lib.hams_field_potentials.argtypes = [ctypes.c_void_p, c_int, P_dbl]
     lib.hams_surrogate_samples.argtypes = [c_int, c_int, ctypes.c_uint64, c_int, P_dbl]
     lib.hams_surrogate_train.argtypes = [c_int, ctypes.POINTER(SgTrain), P_flt, P_dbl]
     lib.hams_surrogate_eval.argtypes = [c_int, P_flt, c_int, P_dbl, P_dbl]
@@ -250,6 +252,22 @@ class Context:
         _check(lib.hams_ctx_set_surrogate(self._h, _f(self._sg), self._sg.size, float(far_factor)))
         kmin, kmax = k_range if k_range is not None else (0.04, 40.0)
         _check(lib.hams_ctx_set_surrogate_range(self._h, float(kmin), float(kmax)))
+
+    def set_field_points(self, xfp):
+        """Field points (nfp, 3) whose potentials every later solve evaluates (None: off)."""
+        if xfp is None or len(xfp) == 0:
+            self._fp = None
+            _check(load_library().hams_ctx_set_field_points(self._h, 0, None))
+            return
+        self._fp = np.asfortranarray(xfp, dtype=np.float64)
+        _check(load_library().hams_ctx_set_field_points(self._h, self._fp.shape[0], _d(self._fp)))
+
+    def field_potentials(self, nbeta, k=0):
+        """(nfp, 6 nb + 2 nbeta) complex potentials of frequency k of the last batch (0 after a single
+        solve): radiation modes, diffraction per heading, incident per heading."""
+        out = np.zeros((self._fp.shape[0], self.ndof + 2 * nbeta), dtype=np.complex128, order="F")
+        _check(load_library().hams_field_potentials(self._h, int(k), out.ctypes.data_as(P_dbl)))
+        return out
 
     def note(self):
         """What the last solve decided on its own (e.g. a fallback to the library LU), or ''."""

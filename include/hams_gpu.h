@@ -266,6 +266,26 @@ int hams_ctx_set_surrogate_range(hams_ctx *ctx, double kmin, double kmax);
  * n is the capacity of ms (19 fills all). Returns the number written. */
 int hams_last_timings(hams_ctx *ctx, double *ms, int32_t n);
 
+/* Field points (ControlFile Number_of_field_points, InputFiles.f90:193-203):
+ * every later solve of ctx also evaluates the potentials at these nfp points
+ * xfp (nfp,3) from the solved panel potentials (CalPotentialMulti,
+ * PressureElevationMulti.f90:55-272): the influence of every hull panel at
+ * each point (Rankine integral at the point, SGLINTBD_MULTI_QUAD2/TRI2, plus
+ * the wave Green function), divided by 2 pi for a point on a hull panel and
+ * 4 pi in the fluid.  nfp = 0 switches them off. */
+int hams_ctx_set_field_points(hams_ctx *ctx, int32_t nfp, const double *xfp);
+
+/* The field-point potentials of frequency k of the last hams_solve_batch
+ * (k = 0 after hams_solve_frequency): pot (nfp, 6nb + 2 nbeta) complex,
+ * column-major -- the radiation potential of each body mode (unit velocity,
+ * columns 6b+m), the diffraction potential of each heading (scattered plus
+ * incident for ISOL = 1, as CalPotentialMulti adds VINP), then the incident
+ * potential alone of each heading (CalPotentialIncMulti, :277-300).
+ * Pressure is i w rho times a potential, elevation i w / g times it (rho and
+ * 1 at the zero and infinite frequency limits), CalPressureMulti /
+ * CalElevationMulti :305-348. */
+int hams_field_potentials(hams_ctx *ctx, int32_t k, double *pot);
+
 /* What the last solve of ctx decided on its own, e.g. the reason it fell back
  * from the block LU to the library LU, or a GMRES solve that missed its
  * tolerance; after hams_solve_batch each frequency's note, prefixed by its

@@ -16,7 +16,9 @@ Decks copied (reference path -> fixture name):
   examples/example3_multi_bodies_gen_mod  -> example3  (2 bodies x 234 panels with lids, a generalized
                                                         mode; its expected files hold the first of the
                                                         deck's 10 frequencies only)
-Only the HAMS-format outputs (OAMASS/ODAMPING/OEXFOR) are kept as expected data.
+Only the HAMS-format outputs (OAMASS/ODAMPING/OEXFOR) are kept as expected data, plus
+example2's WAMIT-format field-point files (PressureElevation.6p,
+PressureElevationIncidence.6p: 100 points on the free surface).
 """
 import os
 import shutil
@@ -32,6 +34,8 @@ DECKS = {
                  "examples/example3_multi_bodies_gen_mod/Output/Hams_format"),
 }
 OUTPUTS = [f"{k}{m}.txt" for k in ("OAMASS", "ODAMPING", "OEXFOR") for m in range(1, 7)]
+WAMIT = {"example2": ("examples/example2_multi_bodies_wave_fields/Output/Wamit_format",
+                      ["PressureElevation.6p", "PressureElevationIncidence.6p"])}
 
 
 def main(ref_root: str) -> None:
@@ -46,7 +50,11 @@ def main(ref_root: str) -> None:
             shutil.copyfile(os.path.join(src_in, f), os.path.join(dst_in, f))
         for f in OUTPUTS:
             shutil.copyfile(os.path.join(ref_root, exp, f), os.path.join(dst_exp, f))
-        print(f"{name}: {len(os.listdir(dst_in))} input files, {len(OUTPUTS)} expected files")
+        if name in WAMIT:
+            src, files = WAMIT[name]
+            for f in files:
+                shutil.copyfile(os.path.join(ref_root, src, f), os.path.join(dst_exp, f))
+        print(f"{name}: {len(os.listdir(dst_in))} input files, {len(os.listdir(dst_exp))} expected files")
 
 
 if __name__ == "__main__":

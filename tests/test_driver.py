@@ -92,3 +92,35 @@ def test_driver_gmres_deck(tmp_path):
             rhead, ref = _load(os.path.join(GOLDEN, "config1", "expected", f"{kind}{m}.txt"))
             assert head == rhead
             assert np.linalg.norm(got - ref) / np.linalg.norm(ref) < tol, f"GMRES {kind}{m} vs reference LU"
+
+
+def _load_6p(path):
+    """Header tokens (frequency, heading, point index) and values of a WAMIT .6p file: lines of
+    14 (frequency, point, 12 radiation values), 12 (the next body's radiation values), 5
+    (frequency, heading, point, diffraction re, im) or 7 (frequency, heading, point, modulus,
+    phase, re, im) fields."""
+    heads, vals = [], []
+    for line in open(path):
+        t = line.split()
+        if not t:
+            continue
+        nh = {14: 2, 12: 0, 5: 3, 7: 3}[len(t)]
+        heads.append(t[:nh])
+        vals.extend(float(x) for x in t[nh:])
+    return heads, np.array(vals)
+
+
+@pytest.mark.gpu
+def test_driver_field_points_example2(tmp_path):
+    """example2's 100 free-surface points: the WAMIT-format elevation files (radiation of every
+    body mode, diffraction and incident wave of every heading) against the reference's
+    (PressureElevationMulti.f90); the incident-wave file is analytic and matches as printed."""
+    inp = os.path.join(GOLDEN, "example2", "input")
+    r = subprocess.run([RUN, inp, str(tmp_path / "gpu")], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    for name, tol in (("PressureElevation.6p", 2e-4), ("PressureElevationIncidence.6p", 1e-6)):
+        got_h, got = _load_6p(tmp_path / "gpu" / "Wamit_format" / name)
+        ref_h, ref = _load_6p(os.path.join(GOLDEN, "example2", "expected", name))
+        assert got_h == ref_h, name
+        err = np.linalg.norm(got - ref) / np.linalg.norm(ref)
+        assert err < tol, f"{name}: relative Frobenius {err:.2e}"

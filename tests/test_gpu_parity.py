@@ -226,3 +226,27 @@ def test_array_of_cylinders_finite_depth():
         am, bd, ex = ctx.solve_frequency(hams_b200.wave_properties(omega, 50.0, 9.81), betas)
         oam, obd, oex, _ = oc.solve(oc.wave(omega), betas)
         assert rel(am, oam) < 1e-7 and rel(bd, obd) < 1e-7 and rel(ex, oex) < 1e-7
+
+
+def test_field_points_on_the_hull_return_the_panel_potentials():
+    """At a hull panel's centre (on the body: divided by 2 pi) the field-point potential is the
+    boundary integral equation of that panel's row, so it must equal the solved panel potential:
+    radiation columns directly, diffraction columns once the incident potential (the last columns)
+    is taken off.  In the fluid (4 pi) the result differs."""
+    d, ctx = deck_context("config1")
+    betas = np.radians(d["wvhd"])
+    rows = np.array([0, 117, 300, 555, d["xyz_p"].shape[0] - 1])
+    ctx.set_field_points(d["xyz_p"][rows])
+    w = hams_b200.wave_properties(d["wvnb"][1], d["h"], 9.80665)
+    ctx.solve_frequency(w, betas)
+    pot = ctx.field_potentials(len(betas))
+    a, b, dd = ctx.assemble(w, betas)
+    x = np.linalg.solve(a, np.concatenate([b, dd], axis=1))
+    nd = 6 * d["body_nelem"].size
+    nb = len(betas)
+    assert rel(pot[:, :nd], x[rows, :nd]) < 1e-9
+    assert rel(pot[:, nd:nd + nb] - pot[:, nd + nb:], x[rows, nd:]) < 1e-9
+    lifted = d["xyz_p"][rows] + 0.5 * d["dxyz"][rows, :3]  # half a metre off the hull along its normal
+    ctx.set_field_points(lifted)
+    ctx.solve_frequency(w, betas)
+    assert rel(ctx.field_potentials(len(betas))[:, :nd], x[rows, :nd]) > 1e-3
