@@ -16,6 +16,7 @@
 // (rho 1000, g 9.80665, unit amplitude, wave reference point at the origin).
 #include <sys/stat.h>
 
+#include <algorithm>
 #include <cctype>
 #include <cmath>
 #include <complex>
@@ -506,6 +507,182 @@ void write_field_points(const std::string& out, const Deck& d, const std::vector
   }
 }
 
+// Hydrostatic_k.in / Hydrostatic.in (ReadHydroStatic[Multi],
+// HydroStaticMulti.f90:68-118): centre of gravity, then the 6 x 6 mass,
+// external linear damping, external quadratic damping, hydrostatic restoring
+// and external restoring matrices of one body.
+struct Hydro {
+  double m[6][6], blin[6][6], bqdr[6][6], crs[6][6], kstf[6][6];
+};
+
+Hydro read_hydro(const std::string& path) {
+  Lines r(path);
+  Hydro h{};
+  r.next();
+  read_list(r, 3);
+  double(*mats[5])[6] = {h.m, h.blin, h.bqdr, h.crs, h.kstf};
+  for (auto* a : mats) {
+    r.next();
+    for (int i = 0; i < 6; ++i) {
+      auto v = read_list(r, 6);
+      for (int j = 0; j < 6; ++j) a[i][j] = v[j];
+    }
+  }
+  return h;
+}
+
+// A x = b for a small complex system by Gaussian elimination with partial
+// pivoting on |re| + |im| (ZGESV's choice); b is overwritten with x.
+void small_solve(int n, std::vector<zc> a, std::vector<zc>& b) {
+  std::vector<int> piv(n);
+  for (int k = 0; k < n; ++k) {
+    int p = k;
+    double best = -1.0;
+    for (int i = k; i < n; ++i) {
+      const zc v = a[i + (size_t)n * k];
+      const double m = std::fabs(v.real()) + std::fabs(v.imag());
+      if (m > best) {
+        best = m;
+        p = i;
+      }
+    }
+    if (p != k) {
+      for (int j = 0; j < n; ++j) std::swap(a[k + (size_t)n * j], a[p + (size_t)n * j]);
+      std::swap(b[k], b[p]);
+    }
+    const zc d = a[k + (size_t)n * k];
+    if (d == zc(0.0, 0.0)) continue;  // singular: the reference's ZGESV leaves INFO > 0 unchecked
+    for (int i = k + 1; i < n; ++i) {
+      const zc l = a[i + (size_t)n * k] / d;
+      if (l == zc(0.0, 0.0)) continue;
+      for (int j = k + 1; j < n; ++j) a[i + (size_t)n * j] -= l * a[k + (size_t)n * j];
+      b[i] -= l * b[k];
+    }
+  }
+  for (int k = n - 1; k >= 0; --k) {
+    zc s = b[k];
+    for (int j = k + 1; j < n; ++j) s -= a[k + (size_t)n * j] * b[j];
+    b[k] = s / a[k + (size_t)n * k];
+  }
+}
+
+// Motion amplitudes of all bodies for one frequency and heading
+// (SolveMotion[Multi], SolveMotionMulti.f90:46-150): block-diagonal body
+// matrices, (-w^2 (M + A) + i w (B + Blin [+ Bq w |x|]) + C + K) x = -Im X - i Re X,
+// the quadratic damping iterated until the summed relative change is below 1e-6.
+std::vector<zc> solve_motion(int nb, const std::vector<Hydro>& hy, double w1, const double* amas, const double* bdmp,
+                             size_t stride, const std::vector<zc>& exfc) {
+  const int n = 6 * nb;
+  auto blk = [&](double(Hydro::*mat)[6][6], int i, int j) {
+    return i / 6 == j / 6 ? (hy[i / 6].*mat)[i % 6][j % 6] : 0.0;
+  };
+  double norm = 0.0;
+  for (int i = 0; i < n; ++i)
+    for (int j = 0; j < n; ++j) norm = std::max(norm, std::fabs(blk(&Hydro::bqdr, i, j)));
+  auto system = [&](const std::vector<zc>* x) {
+    std::vector<zc> a((size_t)n * n);
+    for (int i = 0; i < n; ++i)
+      for (int j = 0; j < n; ++j) {
+        const size_t e = (size_t)i + (size_t)n * j;
+        double damp = bdmp[e * stride] + blk(&Hydro::blin, i, j);
+        if (x) damp += blk(&Hydro::bqdr, i, j) * w1 * std::abs((*x)[j]);
+        a[e] = -w1 * w1 * (blk(&Hydro::m, i, j) + amas[e * stride]) + zc(0.0, w1) * damp + blk(&Hydro::crs, i, j) +
+               blk(&Hydro::kstf, i, j);
+      }
+    return a;
+  };
+  std::vector<zc> rhs(n);
+  for (int i = 0; i < n; ++i) rhs[i] = zc(-exfc[i].imag(), -exfc[i].real());
+  std::vector<zc> x = rhs;
+  small_solve(n, system(nullptr), x);
+  if (norm >= 1.0E-6) {
+    double rerr = 100.0;
+    while (rerr > 1.0E-6) {
+      std::vector<zc> x1 = rhs;
+      small_solve(n, system(&x), x1);
+      rerr = 0.0;
+      for (int j = 0; j < n; ++j)
+        if (std::abs(x1[j]) > 0.0) rerr += std::abs(x1[j] - x[j]) / std::abs(x1[j]);
+      x = x1;
+    }
+  }
+  return x;
+}
+
+// WAMIT-format force and motion files (RFORCE[_MULTI] / EFORCE[_MULTI],
+// PotentWavForceMulti.f90:122,206-215, ReorderAmssDamp :235-346,
+// SolveMotion[Multi], the hydrostatic listing HydroStaticMulti.f90:98-111):
+// AmssDamp.1 row-major per frequency, ExcForce.3 and Motion.4 per heading.
+// The excitation phase is printed as the reference does, converted to
+// degrees twice (ATAN2D(...)*180/PI).
+void write_wamit_forces(const std::string& out, const std::string& in, const Deck& d,
+                        const std::vector<hams_wave>& waves, const std::vector<double>& amas,
+                        const std::vector<double>& bdmp, const std::vector<double>& exfc, const hams_opts& o) {
+  const std::string wd = out + "/Wamit_format";
+  mkdir(out.c_str(), 0755);
+  mkdir(wd.c_str(), 0755);
+  const int nb = d.nbody, ndof = 6 * nb, nf = (int)waves.size(), nbeta = (int)d.wvhd.size();
+  const double kPi = 3.141592653589793;
+  std::vector<Hydro> hy;
+  for (int b = 0; b < nb; ++b) {
+    const std::string f = in + (nb == 1 ? "/Hydrostatic.in" : "/Hydrostatic_" + std::to_string(b + 1) + ".in");
+    if (!exists(f)) {
+      hy.clear();
+      break;
+    }
+    hy.push_back(read_hydro(f));
+  }
+  if (!hy.empty()) {
+    std::ofstream hs(wd + "/Hydrostat.hst");
+    for (int i = 0; i < ndof; ++i)
+      for (int j = 0; j < ndof; ++j) {
+        const double v = i / 6 == j / 6 ? hy[i / 6].crs[i % 6][j % 6] / (o.rho * o.g) : 0.0;
+        hs << std::setw(6) << i + 1 << std::setw(6) << j + 1 << "  " << fmt_es(14, 6, v) << '\n';
+      }
+  }
+  std::ofstream ad(wd + "/AmssDamp.1"), ef(wd + "/ExcForce.3");
+  std::ofstream mo;
+  if (!hy.empty()) mo.open(wd + "/Motion.4");
+  const size_t sf = (size_t)nf;
+  for (int k = 0; k < nf; ++k) {
+    const hams_wave& w = waves[k];
+    const bool limit = std::fabs(w.tp + 1.0) < 1.E-6 || std::fabs(w.tp) < 1.E-6;
+    const double oufr = out_freq(w, d.ouft);
+    for (int i = 0; i < ndof; ++i)
+      for (int j = 0; j < ndof; ++j) {
+        const size_t e = k + sf * ((size_t)i + (size_t)ndof * j);
+        ad << fmt_es(14, 6, oufr) << std::setw(6) << i + 1 << std::setw(6) << j + 1 << fmt_es(14, 6, amas[e] / o.rho);
+        if (!limit) ad << fmt_es(14, 6, bdmp[e] / (o.rho * w.w1));
+        ad << '\n';
+      }
+    for (int ib = 0; ib < nbeta; ++ib) {
+      const double bdeg = (d.wvhd[ib] * kPi / 180.0) * 180.0 / kPi;
+      std::vector<zc> x(ndof);
+      for (int m = 0; m < ndof; ++m) {
+        const size_t e = k + sf * (ib + (size_t)nbeta * m);
+        x[m] = zc(exfc[2 * e], exfc[2 * e + 1]);
+      }
+      if (!limit)
+        for (int m = 0; m < ndof; ++m) {
+          const double s = o.rho * o.g * o.amp, re = x[m].real() / s, im = x[m].imag() / s;
+          const double nrel = -im, nimg = -re;
+          ef << fmt_es(14, 6, oufr) << fmt_es(14, 6, bdeg) << std::setw(6) << m + 1 << fmt_es(14, 6, std::abs(x[m]) / s)
+             << fmt_es(14, 6, std::atan2(nimg, nrel) * 180.0 / kPi * 180.0 / kPi) << fmt_es(14, 6, nrel)
+             << fmt_es(14, 6, nimg) << '\n';
+        }
+      if (hy.empty() || limit) continue;
+      const std::vector<zc> u = solve_motion(nb, hy, w.w1, &amas[k], &bdmp[k], sf, x);
+      for (int m = 0; m < ndof; ++m) {
+        const double nfac = o.amp / std::pow(d.refl, m % 6 < 3 ? 2 : 3);
+        const double nrel = u[m].real() / nfac, nimg = u[m].imag() / nfac;
+        mo << fmt_es(14, 6, oufr) << fmt_es(14, 6, bdeg) << std::setw(6) << m + 1
+           << fmt_es(14, 6, std::sqrt(nrel * nrel + nimg * nimg)) << fmt_es(14, 6, std::atan2(nimg, nrel) * 180.0 / kPi)
+           << fmt_es(14, 6, nrel) << fmt_es(14, 6, nimg) << '\n';
+      }
+    }
+  }
+}
+
 int usage() {
   std::fprintf(stderr,
                "usage: hams_b200_run <inputdir> <outputdir> [--mixed] [--surrogate FILE] [--far F] [--lanes N] "
@@ -618,6 +795,7 @@ int main(int argc, char** argv) {
           }
       }
     }
+    write_wamit_forces(out, in, d, waves, amas, bdmp, exfc, o);
     if (d.nfp > 0) write_field_points(out, d, waves, fpot, o);
     std::printf("hams_b200_run: %d frequencies, %d headings, %d panels, %d bodies -> %s\n", nf, nbeta, d.nelem, nb,
                 hd.c_str());

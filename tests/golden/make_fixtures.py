@@ -17,8 +17,9 @@ Decks copied (reference path -> fixture name):
                                                         mode; its expected files hold the first of the
                                                         deck's 10 frequencies only)
 Only the HAMS-format outputs (OAMASS/ODAMPING/OEXFOR) are kept as expected data, plus
-example2's WAMIT-format field-point files (PressureElevation.6p,
-PressureElevationIncidence.6p: 100 points on the free surface).
+the WAMIT-format force, motion and hydrostatic files of example2, example3 and example5
+and example2's field-point files (PressureElevation.6p, PressureElevationIncidence.6p:
+100 points on the free surface).
 """
 import os
 import shutil
@@ -34,8 +35,11 @@ DECKS = {
                  "examples/example3_multi_bodies_gen_mod/Output/Hams_format"),
 }
 OUTPUTS = [f"{k}{m}.txt" for k in ("OAMASS", "ODAMPING", "OEXFOR") for m in range(1, 7)]
+FORCES = ["AmssDamp.1", "ExcForce.3", "Motion.4", "Hydrostat.hst"]
 WAMIT = {"example2": ("examples/example2_multi_bodies_wave_fields/Output/Wamit_format",
-                      ["PressureElevation.6p", "PressureElevationIncidence.6p"])}
+                      FORCES + ["PressureElevation.6p", "PressureElevationIncidence.6p"]),
+         "example3": ("examples/example3_multi_bodies_gen_mod/Output/Wamit_format", FORCES),
+         "example5": ("examples/example5_single_body/Output/Wamit_format", FORCES)}
 
 
 def main(ref_root: str) -> None:
