@@ -47,9 +47,10 @@ SG_K_RANGE = (0.3, 21.5)
 def _peaks():
     try:
         with open(os.path.join(REPO, "MEASURED_PEAKS.json")) as f:
-            return json.load(f)
+            return dict(json.load(f), source="of measured")
     except (OSError, ValueError):
-        return {"bf16_tflops": 1590.0, "hbm_gbs": 6650.0}  # earlier measurement on this pool (fallback)
+        # an earlier measurement on this pool, used when the measured file is absent
+        return {"bf16_tflops": 1590.0, "hbm_gbs": 6650.0, "source": "of fallback"}
 
 
 PEAKS = _peaks()
@@ -64,11 +65,11 @@ WORKLOAD = "3x3 cylinder array R=4 T=8 spacing 20 m, 5400 quad panels, depth 50 
 # (profiles/k_green_series_eigene_c2_array.md).
 EIGENE_FP64_FLOPS_PER_PAIR = None
 EIGENE_DRAM_BYTES_PER_LAUNCH = None
-# DRAM bytes of one launch of the surrogate kernel on this workload: ncu's
-# dram__bytes_read.sum + dram__bytes_write.sum on the 3,240-panel profiling
-# case (642.0 MB for 10,233,540 pairs, 62.7 B per pair) scaled to the
-# 28,496,520 pairs of a full launch (profiles/k_green_sg_c2_array.md)
-SG_DRAM_BYTES_PER_LAUNCH = 62.73 * 28_496_520
+# DRAM bytes per pair of the surrogate kernel: ncu's dram__bytes_read.sum +
+# dram__bytes_write.sum on the 3,240-panel profiling case (642.0 MB for
+# 10,233,540 pairs), scaled to a full launch by its pair count
+# (profiles/k_green_sg_c2_array.md)
+SG_DRAM_BYTES_PER_PAIR = 62.73
 
 
 # A coarser copy of the array (3,240 panels, 10.2 M far pairs) that profilers
@@ -244,10 +245,11 @@ def rel(a, b):
 
 
 def run_form(hb, dev, geom, case, prec, omegas, betas, warmup, steps, barrier, want_results, sampler=None, sg=None,
-             tol=0.0):
+             tol=0.0, blocks=0):
     """K frequencies through hams_solve_batch (frequencies in flight on several streams), timed
     between two events on the context's stream."""
-    ctx = hb.Context(geom, case["depth"], rho=RHO, g=G, precision=prec, device=dev, refine_tol=tol)
+    ctx = hb.Context(geom, case["depth"], rho=RHO, g=G, precision=prec, device=dev, refine_tol=tol,
+                     body_blocks=blocks)
     if sg is not None:
         ctx.set_surrogate(sg, SG_FAR, SG_K_RANGE)
     waves = [hb.wave_properties(om, case["depth"], G) for om in omegas]
@@ -270,10 +272,10 @@ def run_form(hb, dev, geom, case, prec, omegas, betas, warmup, steps, barrier, w
     return dict(ms=ms, launches=launches, lib_calls=libcalls, timings=tm, results=results, clocks=clocks)
 
 
-def surrogate_kernel_time(hb, dev, geom, case, betas, sg, tol, reps=5):
+def surrogate_kernel_time(hb, dev, geom, case, betas, sg, tol, blocks=0, reps=5):
     """Average duration of the surrogate kernel alone (one lane), CUDA events on its stream."""
     ctx = hb.Context(geom, case["depth"], rho=RHO, g=G, precision=hb.PREC_MIXED, device=dev, refine_tol=tol,
-                     batch_lanes=1)
+                     batch_lanes=1, body_blocks=blocks)
     ctx.set_surrogate(sg, SG_FAR, SG_K_RANGE)
     w = hb.wave_properties(1.2, case["depth"], G)
     ctx.solve_frequency(w, betas)
@@ -287,7 +289,8 @@ def surrogate_kernel_time(hb, dev, geom, case, betas, sg, tol, reps=5):
     return float(np.mean(ms)), int(pairs), None
 
 
-def e2e_form(hb, dev, case, xyz, ncn, ncon, cnt, xr, prec, omegas, betas, steps, barrier, sg=None, tol=0.0):
+def e2e_form(hb, dev, case, xyz, ncn, ncon, cnt, xr, prec, omegas, betas, steps, barrier, sg=None, tol=0.0,
+             blocks=0):
     """Deck through the C ABI from host buffers: geometry, context, K frequencies."""
     import torch
 
@@ -295,7 +298,8 @@ def e2e_form(hb, dev, case, xyz, ncn, ncon, cnt, xr, prec, omegas, betas, steps,
     barrier()
     t = time.perf_counter()
     geom = hb.prepare_geometry(xyz, ncn, ncon, cnt, xr)
-    ctx = hb.Context(geom, case["depth"], rho=RHO, g=G, precision=prec, device=dev, refine_tol=tol)
+    ctx = hb.Context(geom, case["depth"], rho=RHO, g=G, precision=prec, device=dev, refine_tol=tol,
+                     body_blocks=blocks)
     if sg is not None:
         ctx.set_surrogate(sg, SG_FAR, SG_K_RANGE)
     ctx.solve_batch([hb.wave_properties(omegas[s % len(omegas)], case["depth"], G) for s in range(steps)], betas)
@@ -311,12 +315,15 @@ def e2e_form(hb, dev, case, xyz, ncn, ncon, cnt, xr, prec, omegas, betas, steps,
     return el, int(round(h2d)), int(d2h)
 
 
-# forms: precision, surrogate on, dtype, refinement target.  The surrogate form's
-# accuracy is set by the network (~1e-5 in the outputs), so its refinement
-# stops at a relative residual of 1e-7.
-FORMS = {"surrogate": ("mixed", True, "f64 near + f16/f32 MLP far, c64 LU + f64 refinement", 1e-7),
-         "mixed": ("mixed", False, "f64, c64 LU + f64 refinement", 1e-12),
-         "fp64": ("fp64", False, "f64", 0.0)}
+# forms: precision, surrogate on, dtype, refinement target, identical body
+# blocks computed once.  The surrogate form's accuracy is set by the network
+# (~1e-5 in the outputs), so its refinement stops at a relative residual of
+# 1e-7; it also computes the Green functions of each of the 25 distinct
+# (field, source) body blocks of the array once (hams_opts.body_blocks).  The
+# plain forms compute every pair, as the reference does.
+FORMS = {"surrogate": ("mixed", True, "f64 near + f16/f32 MLP far, c64 LU + f64 refinement", 1e-7, 1),
+         "mixed": ("mixed", False, "f64, c64 LU + f64 refinement", 1e-12, 0),
+         "fp64": ("fp64", False, "f64", 0.0, 0)}
 
 
 def gpu_arm(args):
@@ -357,20 +364,20 @@ def gpu_arm(args):
     prec = {"mixed": hb.PREC_MIXED, "fp64": hb.PREC_FP64}
 
     def form_args(name):
-        pr, on, _, tol = FORMS[name]
-        return prec[pr], (sgp if on else None), tol
+        pr, on, _, tol, blocks = FORMS[name]
+        return prec[pr], (sgp if on else None), tol, blocks
 
     sampler = ClockSampler(local)
-    p_main, sg_main, tol_main = form_args(args.form)
+    p_main, sg_main, tol_main, blk_main = form_args(args.form)
     run_form(hb, local, geom, case, p_main, np.concatenate([om_warm, om_rank]), betas, args.warmup, 0, barrier,
-             False, sg=sg_main, tol=tol_main)  # warm the library and caches on this deck
+             False, sg=sg_main, tol=tol_main, blocks=blk_main)  # warm the library and caches on this deck
     runs = {args.form: run_form(hb, local, geom, case, p_main, om_rank, betas, args.warmup, args.steps, barrier, True,
-                                sampler, sg=sg_main, tol=tol_main)}
+                                sampler, sg=sg_main, tol=tol_main, blocks=blk_main)}
     for other in FORMS:
         if other != args.form and not args.only_form:
-            pr, sg, tol = form_args(other)
+            pr, sg, tol, blocks = form_args(other)
             runs[other] = run_form(hb, local, geom, case, pr, om_rank, betas, args.warmup, args.steps, barrier, True,
-                                   sg=sg, tol=tol)
+                                   sg=sg, tol=tol, blocks=blocks)
     main = runs[args.form]
     ms = max_over_ranks(main["ms"])
     forms = {}
@@ -386,7 +393,7 @@ def gpu_arm(args):
         if err is not None:
             forms[name]["rel_err_median"] = med
     e2e_s, h2d, d2h = e2e_form(hb, local, case, xyz, ncn, ncon, cnt, xr, p_main, om_rank, betas, args.steps,
-                               barrier, sg=sg_main, tol=tol_main)
+                               barrier, sg=sg_main, tol=tol_main, blocks=blk_main)
     e2e_s = max_over_ranks(e2e_s)
 
     value = ws * args.steps / (ms * 1e-3)
@@ -400,7 +407,10 @@ def gpu_arm(args):
                        "parallelism": f"frequency shards x{ws}, {LANES} frequencies in flight per GPU",
                        "frequencies": "K solves per rank spread evenly over the 40-frequency sweep",
                        "surrogate": (f"far pairs beyond {SG_FAR} panel sizes, frequencies with K = k0 h tanh(k0 h) in "
-                                     f"[{SG_K_RANGE[0]}, {SG_K_RANGE[1]}]") if sg_main is not None else None},
+                                     f"[{SG_K_RANGE[0]}, {SG_K_RANGE[1]}]") if sg_main is not None else None,
+                       "body_blocks": ("Green functions of the 25 distinct (field body, source body) blocks of the "
+                                       "81 computed, the others copied (identical translated cylinders)")
+                                      if blk_main else None},
             "clocks": main["clocks"], "gpu_launches": main["launches"], "library_calls": main["lib_calls"],
             "e2e": {"value": ws * args.steps / e2e_s, "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h,
@@ -415,12 +425,13 @@ def gpu_arm(args):
         # dominant kernel: the surrogate (tensor cores: 3 hidden 128 x 128 layers and the 16-row output
         # layer per pair), timed alone with CUDA events on one lane at a mid-range frequency
         flops = 2.0 * (3 * 128 * 128 + 128 * 16)
-        sg_ms, sg_pairs, conc_ms = surrogate_kernel_time(hb, local, geom, case, betas, sg_main, tol_main)
+        sg_ms, sg_pairs, conc_ms = surrogate_kernel_time(hb, local, geom, case, betas, sg_main, tol_main, blk_main)
         ach = flops * sg_pairs / (sg_ms * 1e-3) / 1e12
         peak = PEAKS.get("bf16_tflops")
         line["roofline"] = {"kernel": "k_green_sg", "bound": "tensor", "unit": "TFLOP/s", "achieved": ach,
-                            "peak": peak, "frac": ach / peak if peak else None, "traffic": SG_DRAM_BYTES_PER_LAUNCH,
-                            "peak_source": "of measured: dense bf16 cuBLAS burst (MEASURED_PEAKS.json); the kernel "
+                            "peak": peak, "frac": ach / peak if peak else None, "traffic": SG_DRAM_BYTES_PER_PAIR * sg_pairs,
+                            "peak_source": PEAKS["source"] + ": dense bf16 cuBLAS burst (MEASURED_PEAKS.json, else the "
+                                           "pool's earlier 1,590 TFLOP/s); the kernel "
                                            "runs tcgen05.mma kind::f16 (FP16 operands, FP32 accumulation)",
                             "launch_ms": sg_ms,
                             "launch_ms_in_timed_region": tm["green_surrogate"] if tm["pairs_surrogate"] else None,

@@ -1,7 +1,7 @@
 // driver.cpp -- hams_b200_run: a HAMS-MREL deck through the B200 library.
 //
 //   hams_b200_run <inputdir> <outputdir> [--mixed] [--surrogate FILE] [--far F]
-//                 [--lanes N] [--device D]
+//                 [--body-blocks] [--lanes N] [--device D]
 //
 // Reads the reference's input deck -- ControlFile.in (ReadControlFile,
 // src/InputFiles.f90:46-224), HullMesh[_k].pnl and, with IRSP = 1,
@@ -685,8 +685,8 @@ void write_wamit_forces(const std::string& out, const std::string& in, const Dec
 
 int usage() {
   std::fprintf(stderr,
-               "usage: hams_b200_run <inputdir> <outputdir> [--mixed] [--surrogate FILE] [--far F] [--lanes N] "
-               "[--device D]\n");
+               "usage: hams_b200_run <inputdir> <outputdir> [--mixed] [--surrogate FILE] [--far F] [--body-blocks] "
+               "[--lanes N] [--device D]\n");
   return 2;
 }
 
@@ -695,7 +695,7 @@ int usage() {
 int main(int argc, char** argv) {
   if (argc < 3) return usage();
   const std::string in = argv[1], out = argv[2];
-  int precision = HAMS_PREC_FP64, lanes = 0, device = 0;
+  int precision = HAMS_PREC_FP64, lanes = 0, device = 0, body_blocks = 0;
   std::string sgfile;
   double far = 3.0;
   for (int a = 3; a < argc; ++a) {
@@ -703,6 +703,7 @@ int main(int argc, char** argv) {
     if (s == "--mixed") precision = HAMS_PREC_MIXED;
     else if (s == "--surrogate" && a + 1 < argc) sgfile = argv[++a];
     else if (s == "--far" && a + 1 < argc) far = std::atof(argv[++a]);
+    else if (s == "--body-blocks") body_blocks = 1;
     else if (s == "--lanes" && a + 1 < argc) lanes = std::atoi(argv[++a]);
     else if (s == "--device" && a + 1 < argc) device = std::atoi(argv[++a]);
     else return usage();
@@ -736,6 +737,7 @@ int main(int argc, char** argv) {
     o.precision = precision;
     o.device = device;
     o.batch_lanes = lanes;
+    o.body_blocks = body_blocks;
     o.solver = d.isolv == 2 ? HAMS_SOLVER_GMRES : HAMS_SOLVER_LU;
     hams_ctx* ctx = nullptr;
     if (hams_ctx_create(&geo, &o, &ctx)) throw std::runtime_error(std::string("context: ") + hams_last_error());

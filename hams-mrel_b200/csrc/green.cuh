@@ -75,7 +75,11 @@ __device__ inline double limes(int n, double* s, double* a) {
   // from the same operands in the same order, so every entry and the
   // returned value are bit-identical; old s(i+1) and new a(i) are carried
   // in registers.  When the s loop of a column would be empty the a loop's
-  // values are never read again, so that column is skipped.
+  // values are never read again, so that column is skipped.  Steps go in
+  // pairs: the two new a entries depend on the previous column only, so
+  // their reciprocals (and then the two s reciprocals) are independent and
+  // overlap; the maximum test then runs in the reference's order, and an
+  // early return discards the second step's stores, which nothing reads.
   double rl = s[n], amax = 0.0;
   for (int i = 0; i <= n; ++i) a[i] = 0.0;
   for (int k = 1;; ++k) {
@@ -84,19 +88,41 @@ __device__ inline double limes(int n, double* s, double* a) {
     double s_i = s[0], s_i1 = s[1];
     double an_i = (s_i1 != s_i) ? a[1] + 1.0 / (s_i1 - s_i) : a[1];
     a[0] = an_i;
-    for (int i = 0; i <= m; ++i) {
-      double s_i2 = s[i + 2], a_i2 = a[i + 2];
-      double an_i1 = (s_i2 != s_i1) ? a_i2 + 1.0 / (s_i2 - s_i1) : a_i2;
+    int i = 0;
+    for (; i < m; i += 2) {
+      const double s_i2 = s[i + 2], a_i2 = a[i + 2], s_i3 = s[i + 3], a_i3 = a[i + 3];
+      const double an_i1 = (s_i2 != s_i1) ? a_i2 + 1.0 / (s_i2 - s_i1) : a_i2;
+      const double an_i2 = (s_i3 != s_i2) ? a_i3 + 1.0 / (s_i3 - s_i2) : a_i3;
+      const double sn_i = (an_i1 != an_i) ? s_i1 + 1.0 / (an_i1 - an_i) : s_i1;
+      const double sn_i1 = (an_i2 != an_i1) ? s_i2 + 1.0 / (an_i2 - an_i1) : s_i2;
       a[i + 1] = an_i1;
-      double sn_i = (an_i1 != an_i) ? s_i1 + 1.0 / (an_i1 - an_i) : s_i1;
+      a[i + 2] = an_i2;
+      s[i] = sn_i;
+      s[i + 1] = sn_i1;
+      if (fabs(an_i) > amax) {
+        amax = fabs(an_i);
+        rl = sn_i;
+        if (s_i1 == sn_i) return rl;
+      }
+      if (fabs(an_i1) > amax) {
+        amax = fabs(an_i1);
+        rl = sn_i1;
+        if (s_i2 == sn_i1) return rl;
+      }
+      s_i1 = s_i3;
+      an_i = an_i2;
+    }
+    if (i == m) {  // odd number of steps: the last one alone
+      const double s_i2 = s[i + 2], a_i2 = a[i + 2];
+      const double an_i1 = (s_i2 != s_i1) ? a_i2 + 1.0 / (s_i2 - s_i1) : a_i2;
+      a[i + 1] = an_i1;
+      const double sn_i = (an_i1 != an_i) ? s_i1 + 1.0 / (an_i1 - an_i) : s_i1;
       s[i] = sn_i;
       if (fabs(an_i) > amax) {
         amax = fabs(an_i);
         rl = sn_i;
         if (s_i1 == sn_i) return rl;
       }
-      s_i1 = s_i2;
-      an_i = an_i1;
     }
   }
   return rl;
@@ -295,13 +321,11 @@ __device__ inline void pidcock_head(double r, double zfh, double zph, double wk,
   g[2] = cmk(-dp0 * y0, dp0 * j0);
 }
 
-// PIDCOCK, FinGreen3D.f90:558-660 (0.0005 <= R/h < 0.05)
+// The epsilon-extrapolated mode-difference sums of PIDCOCK (FinGreen3D.f90:597-632)
 template <class MD, int N>
-__device__ inline void pidcock(double r, double zf, double zp, double v, double wk, const double* __restrict__ wvn,
-                               double h, cplx g[3], SeriesScratchN<N>& sc, const MD& md, int* overflow) {
+__device__ inline void pidcock_sums(double r, double h, const double* __restrict__ wvn, SeriesScratchN<N>& sc,
+                                    const MD& md, int* overflow, double l[3]) {
   const double pi = 3.141592653589793;
-  double zfh = zf + h, zph = zp + h;
-  pidcock_head(r, zfh, zph, wk, h, g);
   double rhp = fabs(r / h);
   int nt = (int)(HAMS_F4(-1010.10) * rhp + HAMS_F4(100.50));
   if (nt > N) {  // outside the branch's range of R/h
@@ -325,14 +349,30 @@ __device__ inline void pidcock(double r, double zf, double zp, double v, double 
     sc.s1[i - 1] = sc.s1[i - 2] + (-um * am * k1 + umt * amt * k1t);
     sc.s2[i - 1] = sc.s2[i - 2] + (dam * k0 - damt * k0t);
   }
-  double l0 = limes(nt - 1, sc.s0, sc.a);
-  double l1 = limes(nt - 1, sc.s1, sc.a);
-  double l2 = limes(nt - 1, sc.s2, sc.a);
+  l[0] = limes(nt - 1, sc.s0, sc.a);
+  l[1] = limes(nt - 1, sc.s1, sc.a);
+  l[2] = limes(nt - 1, sc.s2, sc.a);
+}
+
+// PIDCOCK's wave term from its three extrapolated sums: head + 4 l + images
+// (FinGreen3D.f90:634-642), before the point-source terms are removed.
+__device__ inline void pidcock_assemble(double r, double zf, double zp, double h, const double l[3], cplx g[3]) {
   double gs, gr, gz;
   pidcock_images(r, zf, zp, h, gs, gr, gz);
-  g[0].re = g[0].re + 4.0 * l0 + gs;
-  g[1].re = g[1].re + 4.0 * l1 + gr;
-  g[2].re = g[2].re + 4.0 * l2 + gz;
+  g[0].re = g[0].re + 4.0 * l[0] + gs;
+  g[1].re = g[1].re + 4.0 * l[1] + gr;
+  g[2].re = g[2].re + 4.0 * l[2] + gz;
+}
+
+// PIDCOCK, FinGreen3D.f90:558-660 (0.0005 <= R/h < 0.05)
+template <class MD, int N>
+__device__ inline void pidcock(double r, double zf, double zp, double v, double wk, const double* __restrict__ wvn,
+                               double h, cplx g[3], SeriesScratchN<N>& sc, const MD& md, int* overflow) {
+  double zfh = zf + h, zph = zp + h;
+  pidcock_head(r, zfh, zph, wk, h, g);
+  double l[3];
+  pidcock_sums(r, h, wvn, sc, md, overflow, l);
+  pidcock_assemble(r, zf, zp, h, l, g);
   remove_rankine(r, zf, zp, g);
 }
 

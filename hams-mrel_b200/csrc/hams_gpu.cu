@@ -121,12 +121,13 @@ __global__ void k_rankine(DevGeom g, double* __restrict__ rs, double* __restrict
   rd[p] = r.dx * g.nrm[j] + r.dy * g.nrm[j + g.n] + r.dz * g.nrm[j + 2 * g.n];
 }
 
-// Sort key of a pair: branch (2 bits) and epsilon-table length (8 bits).
 // Sort key of a pair: branch << 8 | series length.  With the surrogate on,
 // EIGENE / EIGEN pairs farther apart than far x the source panel's size and
-// inside the network's domain go to bins 4 (EIGENE) and 5 (EIGEN).
-__global__ void k_pair_keys(DevGeom g, double h, int sg_on, double far, uint32_t* __restrict__ keys,
-                            uint32_t* __restrict__ idx) {
+// inside the network's domain go to bins 4 (EIGENE) and 5 (EIGEN).  Pairs of
+// a body block copied from an identical one (copied[field body + nb x source
+// body], hams_opts.body_blocks) go to bin 6, which no Green kernel reads.
+__global__ void k_pair_keys(DevGeom g, double h, int sg_on, double far, const unsigned char* __restrict__ copied,
+                            uint32_t* __restrict__ keys, uint32_t* __restrict__ idx) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   int j = blockIdx.y;
   if (i >= g.tn) return;
@@ -140,6 +141,7 @@ __global__ void k_pair_keys(DevGeom g, double h, int sg_on, double far, uint32_t
     bool far_pair = sqrt(dx * dx + dy * dy + dz * dz) > far * g.pnsz[j];
     if (far_pair && sg::in_domain(rr / h, (zq + h) / h, (zp + h) / h, sg::kKmin)) b = b == hams::kEigenE ? 4 : 5;
   }
+  if (copied && i < g.n && copied[g.body[i] + g.nb * g.body[j]]) b = 6;
   keys[p] = (uint32_t)(b << 8) | (uint32_t)(nt & 0xff);
   idx[p] = (uint32_t)p;
 }
@@ -176,12 +178,13 @@ __global__ void __launch_bounds__(128, BR == hams::kEigen ? 8 : 1) k_green_fin(D
   store_pair(g, p, i, j, G, rs, rd, A, S);
 }
 
-__global__ void __launch_bounds__(128) k_green_inf(DevGeom g, WaveDev w, const double* __restrict__ rs,
-                                                   const double* __restrict__ rd, double2* __restrict__ A,
-                                                   double2* __restrict__ S) {
+__global__ void __launch_bounds__(128) k_green_inf(DevGeom g, WaveDev w, const unsigned char* __restrict__ copied,
+                                                   const double* __restrict__ rs, const double* __restrict__ rd,
+                                                   double2* __restrict__ A, double2* __restrict__ S) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   int j = blockIdx.y;
   if (i >= g.tn) return;
+  if (copied && i < g.n && copied[g.body[i] + g.nb * g.body[j]]) return;  // filled by k_copy_blocks
   size_t p = (size_t)i + (size_t)j * g.tn;
   int flag = near_flag(g, i, j);
   double xp = g.fxyz[i], yp = g.fxyz[i + g.tn], zp = g.fxyz[i + 2 * g.tn];
@@ -189,6 +192,24 @@ __global__ void __launch_bounds__(128) k_green_inf(DevGeom g, WaveDev w, const d
   grn4 G = w.limit ? hams::green_limit(w.limit == 2, xq, xp, yq, yp, zq, zp, flag)
                    : hams::infgreen3d(xq, xp, yq, yp, zq, zp, w.v, flag);
   store_pair(g, p, i, j, G, rs, rd, A, S);
+}
+
+// Body blocks of identical body pairs (hams_opts.body_blocks): blk holds 6
+// ints per block -- destination first row and column, source first row and
+// column, rows, columns -- and block z copies its A and S entries, one
+// source column per blockIdx.y, after the Green kernels have filled the
+// source block.
+__global__ void __launch_bounds__(256) k_copy_blocks(const int* __restrict__ blk, int tn, double2* __restrict__ A,
+                                                     double2* __restrict__ S) {
+  const int* b = blk + 6 * blockIdx.z;
+  const int nj = b[5], ni = b[4];
+  for (int j = blockIdx.y; j < nj; j += gridDim.y) {
+    const size_t d0 = (size_t)b[0] + (size_t)(b[1] + j) * tn, s0 = (size_t)b[2] + (size_t)(b[3] + j) * tn;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ni; i += gridDim.x * blockDim.x) {
+      A[d0 + i] = A[s0 + i];
+      S[d0 + i] = S[s0 + i];
+    }
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -514,7 +535,7 @@ __global__ void k_colnorm_ratio(const double2* __restrict__ r, const double2* __
 // ---------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------
-constexpr int kBins = 6;
+constexpr int kBins = 7;
 template <class T>
 struct DBuf {
   T* p = nullptr;
@@ -582,8 +603,15 @@ struct hams_ctx {
   DBuf<double> rs, rd;
   DBuf<uint32_t> pairs;
   // start offsets into pairs of bins 0-3 (branches LINTON, PIDCOCK, EIGENE,
-  // EIGEN), 4-5 (surrogate pairs of EIGENE, EIGEN); bin_off[6] = total
+  // EIGEN), 4-5 (surrogate pairs of EIGENE, EIGEN), 6 (pairs of copied body
+  // blocks); bin_off[7] = total
   long long bin_off[kBins + 1] = {};
+  // identical body blocks (hams_opts.body_blocks): per (field, source) body
+  // pair 1 when copied, and the copies (6 ints each, k_copy_blocks)
+  DBuf<unsigned char> blk_copied;
+  DBuf<int> blk_list;
+  int nblk = 0, blk_rows = 0, blk_cols = 0;
+  long long blk_pairs = 0;
   // chunks of source panels for the RHS reduction
   std::vector<int2> chunks_h;
   DBuf<int2> chunks;
@@ -607,7 +635,7 @@ struct hams_ctx {
   cudaEvent_t ev[6] = {};
   cudaEvent_t evb[6] = {};
   cudaEvent_t evf = nullptr;
-  static constexpr int kTimings = 19;
+  static constexpr int kTimings = 20;
   double last_ms[kTimings] = {};
   std::atomic<long long> launches{0};   // kernels of this library
   std::atomic<long long> lib_calls{0};  // cuBLAS / cuSOLVER / CUB calls
@@ -684,7 +712,8 @@ static int build_pairs(hams_ctx* c) {
   DBuf<uint32_t> keys, keys2, idx;
   TRY(keys.alloc(np)); TRY(keys2.alloc(np)); TRY(idx.alloc(np)); TRY(c->pairs.alloc(np));
   dim3 grid2((tn + 127) / 128, n);
-  k_pair_keys<<<grid2, 128, 0, c->st>>>(c->g, c->opts.depth, c->sg_on, c->sg_far, keys.p, idx.p);
+  k_pair_keys<<<grid2, 128, 0, c->st>>>(c->g, c->opts.depth, c->sg_on, c->sg_far, c->nblk ? c->blk_copied.p : nullptr,
+                                         keys.p, idx.p);
   TRY(launch_check(c));
   size_t tmp = 0;
   cub::DeviceRadixSort::SortPairs(nullptr, tmp, keys.p, keys2.p, idx.p, c->pairs.p, np, 0, 11, c->st);
@@ -755,6 +784,38 @@ static int ctx_setup(hams_ctx* c, const hams_geom* geo) {
   dim3 grid2((tn + 127) / 128, n);
   k_rankine<<<grid2, 128, 0, c->st>>>(c->g, c->rs.p, c->rd.p);
   TRY(launch_check(c));
+
+  // identical body blocks: which (field, source) body blocks are copies
+  c->nblk = 0;
+  c->blk_pairs = 0;
+  if (c->opts.body_blocks && nb > 1 && c->nl == 0) {
+    std::vector<int32_t> rep((size_t)nb * nb);
+    if (hams_body_blocks(geo, 1e-9, rep.data()) < 0) return fail(HAMS_ERR_ARG, "body blocks: bad geometry");
+    std::vector<unsigned char> copied((size_t)nb * nb, 0);
+    std::vector<int> lst;
+    for (int k = 0; k < nb * nb; ++k) {
+      if (rep[k] == k) continue;
+      const int b1 = k % nb, b2 = k / nb, c1 = rep[k] % nb, c2 = rep[k] / nb;
+      copied[k] = 1;
+      const int ni = bst[b1 + 1] - bst[b1], nj = bst[b2 + 1] - bst[b2];
+      lst.insert(lst.end(), {bst[b1], bst[b2], bst[c1], bst[c2], ni, nj});
+      c->blk_rows = std::max(c->blk_rows, ni);
+      c->blk_cols = std::max(c->blk_cols, nj);
+      c->blk_pairs += (long long)ni * nj;
+      ++c->nblk;
+    }
+    if (c->nblk > 65535) {  // one grid z index per copy: keep every block instead
+      c->nblk = 0;
+      c->blk_pairs = 0;
+    }
+    if (c->nblk) {
+      TRY(c->blk_copied.alloc(copied.size()));
+      TRY(c->blk_list.alloc(lst.size()));
+      CU(cudaMemcpyAsync(c->blk_copied.p, copied.data(), copied.size(), cudaMemcpyHostToDevice, c->st));
+      CU(cudaMemcpyAsync(c->blk_list.p, lst.data(), lst.size() * 4, cudaMemcpyHostToDevice, c->st));
+      CU(cudaStreamSynchronize(c->st));
+    }
+  }
 
   // branch-sorted pair list (finite depth)
   if (c->opts.depth >= 0.0) TRY(build_pairs(c));
@@ -842,6 +903,8 @@ static int make_lane(hams_ctx* c, hams_ctx** out) {
     l->vtx.view(c->vtx); l->ncn.view(c->ncn); l->body.view(c->body); l->bstart.view(c->bstart);
     l->rs.view(c->rs); l->rd.view(c->rd); l->pairs.view(c->pairs); l->chunks.view(c->chunks);
     l->chunk_body.view(c->chunk_body);
+    l->blk_copied.view(c->blk_copied); l->blk_list.view(c->blk_list);
+    l->nblk = c->nblk; l->blk_rows = c->blk_rows; l->blk_cols = c->blk_cols; l->blk_pairs = c->blk_pairs;
     l->g = c->g;
     for (int b = 0; b <= kBins; ++b) l->bin_off[b] = c->bin_off[b];
     l->sg_on = c->sg_on;
@@ -918,7 +981,8 @@ static int assemble_dev(hams_ctx* c, const hams_wave* w, int nbeta) {
   CU(cudaEventRecord(c->ev[0], c->st));
   if (c->opts.depth < 0.0) {
     dim3 grid((tn + 127) / 128, n);
-    k_green_inf<<<grid, 128, 0, c->st>>>(c->g, wd, c->rs.p, c->rd.p, c->A.p, c->S.p);
+    k_green_inf<<<grid, 128, 0, c->st>>>(c->g, wd, c->nblk ? c->blk_copied.p : nullptr, c->rs.p, c->rd.p, c->A.p,
+                                         c->S.p);
     TRY(launch_check(c));
   } else {
     if (!wd.limit) {
@@ -965,6 +1029,12 @@ static int assemble_dev(hams_ctx* c, const hams_wave* w, int nbeta) {
       }
     }
     CU(cudaEventRecord(c->evb[5], c->st));
+  }
+  if (c->nblk) {
+    dim3 grid((unsigned)std::min((c->blk_rows + 255) / 256, 4), (unsigned)std::min(c->blk_cols, 1024),
+              (unsigned)c->nblk);
+    k_copy_blocks<<<grid, 256, 0, c->st>>>(c->blk_list.p, c->tn, c->A.p, c->S.p);
+    TRY(launch_check(c));
   }
   CU(cudaEventRecord(c->ev[1], c->st));
   // right-hand sides
@@ -1475,6 +1545,7 @@ static int solve_one(hams_ctx* c, const hams_wave* w, int nbeta, const double* b
   if (c->opts.depth >= 0.0 && cudaEventElapsedTime(&ms, c->evb[4], c->evb[5]) == cudaSuccess) c->last_ms[16] = ms;
   c->last_ms[17] = c->sg_used ? (double)(c->bin_off[6] - c->bin_off[4]) : 0.0;
   c->last_ms[18] = c->opts.precision == HAMS_PREC_MIXED ? c->ir_rate : 0.0;
+  c->last_ms[19] = (double)c->blk_pairs;
   if (ovf & 2) return fail(HAMS_ERR_CUDA, "surrogate kernel: a tensor-core completion wait gave up");
   if (ovf) return fail(HAMS_ERR_NUMERIC, "adaptive quadrature stack overflow in the LINTON branch");
   if (info > 0) return info;  // singular pivot, LAPACK style

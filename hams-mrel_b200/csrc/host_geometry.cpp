@@ -9,7 +9,9 @@
 // (CalPanelChartLength :401), unit normal from the cross product of the
 // diagonals (CalTransNormals :74) and the rotational normals r x n about
 // each body's reference point (CalRotNormals :46).  It runs once per mesh.
+#include <algorithm>
 #include <cmath>
+#include <vector>
 
 #include "../../include/hams_gpu.h"
 
@@ -100,4 +102,116 @@ extern "C" int hams_prepare_geometry(int32_t ntnd, const double* xyz, int32_t ne
     i0 += body_nelem[b];
   }
   return HAMS_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Identical bodies (hams_body_blocks).  The finite- and infinite-depth Green
+// functions depend on the horizontal distance and the two depths of a pair
+// only, and the Rankine panel integrals on the panels' relative position, so
+// the (field body, source body) block of the collocation matrices is the same
+// for every pair of bodies with the same shapes and the same horizontal
+// offset.  Body b is a translate of an earlier body t when both have the same
+// panels in the same order, each with the same vertex count, and every
+// vertex, centre, area, longest edge and unit normal of b equals t's moved by
+// one horizontal offset (coordinates within tol times the mesh size; the
+// rotational normals are left out, they enter the right-hand sides only).
+// ---------------------------------------------------------------------------
+namespace {
+
+struct BodyShape {
+  int tmpl;        // the first body of which this one is a translate
+  double dx, dy;   // its horizontal offset from that body
+};
+
+std::vector<BodyShape> body_shapes(const hams_geom* g, double tol) {
+  const int nb = g->nbody, n = g->nelem;
+  std::vector<int> st(nb + 1, 0);
+  for (int b = 0; b < nb; ++b) st[b + 1] = st[b] + g->body_nelem[b];
+  double lo = 0.0, hi = 0.0;
+  for (int k = 0; k < 3; ++k)
+    for (int i = 0; i < n; ++i) {
+      lo = std::min(lo, g->xyz_p[i + (size_t)k * n]);
+      hi = std::max(hi, g->xyz_p[i + (size_t)k * n]);
+    }
+  const double eps = tol * std::max(1.0, hi - lo), eps_n = tol;
+  auto node = [&](int panel, int v, int k) {
+    return g->xyz[(g->ncon[panel + (size_t)v * n] - 1) + (size_t)k * g->ntnd];
+  };
+  std::vector<BodyShape> s(nb);
+  for (int b = 0; b < nb; ++b) {
+    s[b] = {b, 0.0, 0.0};
+    for (int t = 0; t < b; ++t) {
+      if (s[t].tmpl != t || st[t + 1] - st[t] != st[b + 1] - st[b]) continue;
+      const int m = st[b + 1] - st[b];
+      if (m == 0) continue;
+      const double dx = g->xyz_p[st[b]] - g->xyz_p[st[t]], dy = g->xyz_p[st[b] + n] - g->xyz_p[st[t] + n];
+      bool same = true;
+      for (int q = 0; q < m && same; ++q) {
+        const int i = st[b] + q, j = st[t] + q;
+        same = g->ncn[i] == g->ncn[j] && std::fabs(g->xyz_p[i] - g->xyz_p[j] - dx) <= eps &&
+               std::fabs(g->xyz_p[i + n] - g->xyz_p[j + n] - dy) <= eps &&
+               std::fabs(g->xyz_p[i + 2 * (size_t)n] - g->xyz_p[j + 2 * (size_t)n]) <= eps &&
+               std::fabs(g->ds[i] - g->ds[j]) <= eps * std::max(1.0, std::fabs(g->pnsz[j])) &&
+               std::fabs(g->pnsz[i] - g->pnsz[j]) <= eps;
+        for (int k = 0; k < 3 && same; ++k)
+          same = std::fabs(g->dxyz[i + (size_t)k * n] - g->dxyz[j + (size_t)k * n]) <= eps_n;
+        for (int v = 0; v < g->ncn[i] && same; ++v)
+          same = std::fabs(node(i, v, 0) - node(j, v, 0) - dx) <= eps &&
+                 std::fabs(node(i, v, 1) - node(j, v, 1) - dy) <= eps &&
+                 std::fabs(node(i, v, 2) - node(j, v, 2)) <= eps;
+      }
+      if (same) {
+        s[b] = {t, dx, dy};
+        break;
+      }
+    }
+  }
+  return s;
+}
+
+std::vector<int> body_block_reps(const hams_geom* g, double tol) {
+  const int nb = g->nbody;
+  std::vector<int> rep((size_t)nb * nb);
+  for (size_t k = 0; k < rep.size(); ++k) rep[k] = (int)k;
+  if (nb <= 1 || g->inelem > 0) return rep;
+  std::vector<BodyShape> s = body_shapes(g, tol);
+  double lo = 0.0, hi = 0.0;
+  for (int i = 0; i < 2 * g->nelem; ++i) {
+    lo = std::min(lo, g->xyz_p[i]);
+    hi = std::max(hi, g->xyz_p[i]);
+  }
+  const double eps = tol * std::max(1.0, hi - lo);
+  // block (b1 field, b2 source) = block (c1, c2) when the templates agree and
+  // the offset of b2 from b1 equals that of c2 from c1
+  for (int b2 = 0; b2 < nb; ++b2)
+    for (int b1 = 0; b1 < nb; ++b1) {
+      const size_t k = b1 + (size_t)nb * b2;
+      const double ox = s[b2].dx - s[b1].dx, oy = s[b2].dy - s[b1].dy;
+      for (size_t c = 0; c < k; ++c) {
+        if (rep[c] != (int)c) continue;
+        const int c1 = (int)(c % nb), c2 = (int)(c / nb);
+        if (s[c1].tmpl != s[b1].tmpl || s[c2].tmpl != s[b2].tmpl) continue;
+        if (std::fabs(s[c2].dx - s[c1].dx - ox) <= eps && std::fabs(s[c2].dy - s[c1].dy - oy) <= eps) {
+          rep[k] = (int)c;
+          break;
+        }
+      }
+    }
+  return rep;
+}
+
+}  // namespace
+
+extern "C" int hams_body_blocks(const hams_geom* g, double tol, int32_t* rep) {
+  if (!g || !rep || g->nbody < 1 || !g->body_nelem || !g->xyz_p || !g->ncn || !g->ncon || !g->xyz || !g->ds ||
+      !g->pnsz || !g->dxyz)
+    return -1;
+  if (!(tol > 0.0)) tol = 1e-9;
+  std::vector<int> r = body_block_reps(g, tol);
+  int distinct = 0;
+  for (size_t k = 0; k < r.size(); ++k) {
+    rep[k] = r[k];
+    distinct += r[k] == (int)k;
+  }
+  return distinct;
 }

@@ -39,7 +39,7 @@ class HamsOpts(ctypes.Structure):
                 ("irsp", c_int), ("precision", c_int), ("device", c_int), ("refine_tol", c_dbl),
                 ("refine_max", c_int), ("lu_kind", c_int), ("batch_lanes", c_int),
                 ("solver", c_int), ("gmres_restart", c_int), ("gmres_maxit", c_int), ("gmres_tol", c_dbl),
-                ("aca_tol", c_dbl), ("gmres_dense", c_int), ("reserved", c_int * 3)]
+                ("aca_tol", c_dbl), ("gmres_dense", c_int), ("body_blocks", c_int), ("reserved", c_int * 2)]
 
 
 class HamsWave(ctypes.Structure):
@@ -87,6 +87,7 @@ def load_library(path=LIB_PATH):
     lib.hams_mark.argtypes = [ctypes.c_void_p, c_int]
     lib.hams_mark_elapsed.argtypes = [ctypes.c_void_p, c_int, c_int, P_dbl]
     lib.hams_measure_fp64_peak.argtypes = [c_int, P_dbl]
+    lib.hams_body_blocks.argtypes = [ctypes.POINTER(HamsGeom), c_dbl, P_int]
     lib.hams_prepare_geometry.argtypes = [c_int, P_dbl, c_int, P_int, P_int, c_int, P_int, P_dbl, P_dbl, P_dbl, P_dbl,
                                           P_dbl]
     P_flt = ctypes.POINTER(ctypes.c_float)
@@ -142,6 +143,25 @@ def prepare_geometry(xyz, ncn, ncon, body_nelem, xr):
     return dict(xyz=xyz, ncn=ncn, ncon=ncon, xyz_p=xyz_p, ds=ds, pnsz=pnsz, dxyz=dxyz, body_nelem=bn)
 
 
+def body_blocks(geom, tol=1e-9):
+    """Blocks of identical body pairs (hams_body_blocks): rep (nbody, nbody), rep[b1, b2] = the
+    column-major index b1' + nbody b2' of the block that (field b1, source b2) copies (its own
+    index when computed in full), and the number of distinct blocks."""
+    lib = load_library()
+    keep = {k: np.asfortranarray(geom[k], dtype=np.int32 if k in ("ncn", "ncon", "body_nelem") else np.float64)
+            for k in ("xyz", "ncn", "ncon", "xyz_p", "ds", "pnsz", "dxyz", "body_nelem")}
+    nb = keep["body_nelem"].size
+    g = HamsGeom(nelem=keep["ncn"].size, ntnd=keep["xyz"].shape[0], nbody=nb, xyz=_d(keep["xyz"]),
+                 ncn=_i(keep["ncn"]), ncon=_i(keep["ncon"]), xyz_p=_d(keep["xyz_p"]), ds=_d(keep["ds"]),
+                 pnsz=_d(keep["pnsz"]), dxyz=_d(keep["dxyz"]), body_nelem=_i(keep["body_nelem"]),
+                 inelem=int(len(geom.get("ixyz_p", ()))), ixyz_p=None)
+    rep = np.zeros((nb, nb), dtype=np.int32, order="F")
+    distinct = lib.hams_body_blocks(ctypes.byref(g), float(tol), _i(rep))
+    if distinct < 0:
+        raise HamsError(distinct, "hams_body_blocks: null argument")
+    return rep, distinct
+
+
 class Context:
     """Device-resident geometry of one deck; solves frequencies on one GPU.
 
@@ -152,7 +172,7 @@ class Context:
     def __init__(self, geom, depth, rho=1000.0, g=9.80665, isol=1, irsp=0, precision=PREC_FP64, device=0,
                  xw=(0.0, 0.0), amp=1.0, refine_tol=0.0, refine_max=0, lu_kind=0,
                  batch_lanes=0, solver=SOLVER_LU, gmres_restart=0, gmres_maxit=0, gmres_tol=0.0, aca_tol=0.0,
-                 gmres_dense=0):
+                 gmres_dense=0, body_blocks=0):
         lib = load_library()
         self._keep = {}
         f = lambda k, dt: self._keep.setdefault(k, np.asfortranarray(geom[k], dtype=dt))
@@ -173,7 +193,7 @@ class Context:
                      precision=int(precision), device=int(device), refine_tol=float(refine_tol),
                      refine_max=int(refine_max), lu_kind=int(lu_kind), batch_lanes=int(batch_lanes), solver=int(solver),
                      gmres_restart=int(gmres_restart), gmres_maxit=int(gmres_maxit), gmres_tol=float(gmres_tol),
-                     aca_tol=float(aca_tol), gmres_dense=int(gmres_dense))
+                     aca_tol=float(aca_tol), gmres_dense=int(gmres_dense), body_blocks=int(body_blocks))
         o.xw[0], o.xw[1] = xw
         self.depth, self.g = float(depth), float(g)
         self._h = ctypes.c_void_p()
@@ -232,14 +252,14 @@ class Context:
 
     def timings(self):
         """Stage times of the last solve (ms), per-branch Green kernel times and pair counts."""
-        ms = np.zeros(19)
-        load_library().hams_last_timings(self._h, _d(ms), 19)
+        ms = np.zeros(20)
+        load_library().hams_last_timings(self._h, _d(ms), 20)
         return dict(green=ms[0], rhs=ms[1], solve=ms[2], forces=ms[3], total=ms[4], green_linton=ms[5],
                     green_pidcock=ms[6], green_eigene=ms[7], green_eigen=ms[8], factor=ms[9], refine_sweeps=int(ms[10]),
                     iterations=int(ms[10]),
                     pairs_linton=int(ms[11]), pairs_pidcock=int(ms[12]), pairs_eigene=int(ms[13]),
                     pairs_eigen=int(ms[14]), lu_used=int(ms[15]), green_surrogate=ms[16],
-                    pairs_surrogate=int(ms[17]), ir_rate=ms[18])
+                    pairs_surrogate=int(ms[17]), ir_rate=ms[18], pairs_copied=int(ms[19]))
 
     def set_surrogate(self, params, far_factor=3.0, k_range=None):
         """Far pairs from the trained network (params float32), or the series again (params None);

@@ -113,7 +113,11 @@ typedef struct hams_opts {
   int32_t gmres_dense;/* GMRES: 0 products with the H-matrix (the reference's
                        choice without lids, AssbMatx[Multi].f90:284-288), 1 with
                        the dense matrix; with lids always dense (:494-498)      */
-  int32_t reserved[3];
+  int32_t body_blocks;/* 1: compute the wave Green function of each distinct
+                       (field body, source body) block once and copy it to
+                       the blocks of identical body pairs (hams_body_blocks);
+                       without lids only.  0: every pair (the reference)     */
+  int32_t reserved[2];
 } hams_opts;
 
 /* One frequency after CalWaveProperts (ImplementSubs.f90:40): V = w^2/g
@@ -139,6 +143,19 @@ int hams_wave_properties(int32_t inft, double value, double depth, double g, int
 int hams_prepare_geometry(int32_t ntnd, const double *xyz, int32_t nelem, const int32_t *ncn, const int32_t *ncon,
                           int32_t nbody, const int32_t *body_nelem, const double *xr, double *xyz_p, double *ds,
                           double *pnsz, double *dxyz);
+
+/* Blocks of identical body pairs (hams_opts.body_blocks).  Body b is a
+ * translate of an earlier body t when they have the same panels in the same
+ * order and every vertex, centre, area, longest edge and unit normal of b is
+ * t's moved by one horizontal offset (within tol times the mesh size; tol <= 0:
+ * 1e-9).  The (field b1, source b2) block then equals the first block
+ * (c1, c2), in column-major order of k = b1 + nbody b2, whose bodies are
+ * translates of the same bodies with the same horizontal offset of c2 from
+ * c1: rep[k] receives that block's k (rep (nbody, nbody); rep[k] = k for a
+ * block computed in full).  Geometries with water-plane lids (inelem > 0)
+ * keep every block.  Host-only.  Returns the number of distinct blocks, or
+ * -1 on a null argument. */
+int hams_body_blocks(const hams_geom *geo, double tol, int32_t *rep);
 
 /* Uploads the geometry, evaluates the frequency-independent Rankine panel
  * integrals (SGLINTBD_*, SingularIntgr.f90:44,252) for every field/source
@@ -262,8 +279,9 @@ int hams_ctx_set_surrogate_range(hams_ctx *ctx, double kmin, double kmax);
  * form's factorisation (HAMS_LU_*; -1 for FP64), [16] the surrogate kernel
  * (or the series standing in for it), [17] pairs the surrogate evaluated,
  * [18] the mixed form's largest residual reduction factor over one refinement
- * sweep (about the condition number times the factorisation's error).
- * n is the capacity of ms (19 fills all). Returns the number written. */
+ * sweep (about the condition number times the factorisation's error),
+ * [19] pairs copied from identical body blocks (hams_opts.body_blocks).
+ * n is the capacity of ms (20 fills all). Returns the number written. */
 int hams_last_timings(hams_ctx *ctx, double *ms, int32_t n);
 
 /* Field points (ControlFile Number_of_field_points, InputFiles.f90:193-203):
