@@ -58,13 +58,14 @@ WORKLOAD = "3x3 cylinder array R=4 T=8 spacing 20 m, 5400 quad panels, depth 50 
            "headings 0/30/60/90 deg (54 rad + 4 dif RHS)"
 
 # FP64 operations per EIGENE panel pair of the series Green kernel, from the
-# executed-instruction counters of one ncu capture of that kernel on this
-# workload: dadd + dmul + 2 dfma (smsp__sass_thread_inst_executed_op_d*), and
-# its DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum).
-# Both belong to the kernel version they were captured from
+# executed-instruction counters of one ncu capture of that kernel on the
+# 3,240-panel profiling case: dadd + dmul + 2 dfma
+# (smsp__sass_thread_inst_executed_op_d*), and its DRAM bytes per pair
+# (dram__bytes_read.sum + dram__bytes_write.sum over the launch's 4,093,706
+# pairs), scaled to a full launch by its pair count
 # (profiles/k_green_series_eigene_c2_array.md).
-EIGENE_FP64_FLOPS_PER_PAIR = None
-EIGENE_DRAM_BYTES_PER_LAUNCH = None
+EIGENE_FP64_FLOPS_PER_PAIR = 44_410
+EIGENE_DRAM_BYTES_PER_PAIR = 2_381
 # DRAM bytes per pair of the surrogate kernel: ncu's dram__bytes_read.sum +
 # dram__bytes_write.sum on the 3,240-panel profiling case (642.0 MB for
 # 10,233,540 pairs), scaled to a full launch by its pair count
@@ -445,7 +446,7 @@ def gpu_arm(args):
                 "pairs_per_launch": tm["pairs_eigene"], "peak": peak,
                 "peak_source": "measured in this run: FP64 FMA loop on all SMs (no FP64 figure in "
                                "MEASURED_PEAKS.json)", "achieved": None, "frac": None,
-                "traffic": EIGENE_DRAM_BYTES_PER_LAUNCH}
+                "traffic": EIGENE_DRAM_BYTES_PER_PAIR * tm["pairs_eigene"]}
         if EIGENE_FP64_FLOPS_PER_PAIR and peak and eig_ms > 0:
             ach = EIGENE_FP64_FLOPS_PER_PAIR * tm["pairs_eigene"] / (eig_ms * 1e-3) / 1e12
             roof.update(achieved=ach, frac=ach / peak, flops_per_pair=EIGENE_FP64_FLOPS_PER_PAIR)

@@ -10,10 +10,12 @@ solves).  Every copied block equals its source block bit for bit, and the
 source blocks equal the fully computed ones bit for bit.  The fully computed
 copies differ from their source blocks only through the rounding of the
 translated coordinates; the epsilon extrapolation of the EIGENE / PIDCOCK
-series amplifies that to ~2e-6 of max(1, |G|) in single pairs (the CPU
-oracle shows the same for a pair and its translate), so the assembled
-matrices and right-hand sides agree to 1e-6 and the added mass, damping and
-excitation to 1e-6 (relative Frobenius).
+series amplifies that in single pairs -- the CPU oracle's own values for a
+pair and its translate differ by up to 2e-6 of max(1, |G|) at 0.3 rad/s and
+6e-5 at 2.0 rad/s -- and the assembled matrices differ by up to 2.4e-5
+(relative Frobenius, at 2.0 rad/s).  The bound here is 1e-4, the accuracy
+bar of the surrogate form that uses the blocks, for the matrices, the
+right-hand sides and the added mass, damping and excitation.
 """
 import os
 import sys
@@ -127,17 +129,17 @@ def test_copied_blocks_match_every_pair(depth):
             if r == k:
                 assert np.array_equal(blk(a1, k), blk(a0, k))
         # the right-hand sides are sums over S, so they see the copies too
-        assert rel(a1, a0) < 1e-6 and rel(b1, b0) < 1e-6 and rel(d1, d0) < 1e-6
+        assert rel(a1, a0) < 1e-4 and rel(b1, b0) < 1e-4 and rel(d1, d0) < 1e-4
         r0 = full.solve_frequency(w, betas)
         r1 = copy.solve_frequency(w, betas)
         assert copy.timings()["pairs_copied"] == (81 - distinct) * per * per
         assert full.timings()["pairs_copied"] == 0
         for x, y in zip(r1, r0):
-            assert rel(x, y) < 1e-6
+            assert rel(x, y) < 1e-4
     # batched lanes share the copy lists
     if depth > 0:
         for x, y in zip(copy.solve_batch(waves[:3], betas), full.solve_batch(waves[:3], betas)):
             for k in range(3):
-                assert rel(x[k], y[k]) < 1e-6
+                assert rel(x[k], y[k]) < 1e-4
     full.close()
     copy.close()
