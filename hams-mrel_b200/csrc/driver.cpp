@@ -161,6 +161,7 @@ struct Deck {
   std::vector<double> xfp;       // field points (nfp,3) column-major
   int nfp = 0;
   bool separate = false;         // separate_wamit_diffraction_radiation_files
+  bool genmod = false;           // some gen_mod_* file overrode the normals
 };
 
 Deck load(const std::string& dir) {
@@ -308,6 +309,7 @@ Deck load(const std::string& dir) {
       const std::string gp = dir + "/gen_mod_" + std::to_string(nb == 1 ? 1 : b + 1) + "_" + std::to_string(dof) + ".txt";
       std::ifstream f(gp);
       if (!f) continue;
+      d.genmod = true;
       std::string l;
       for (int i = 0; i < d.body_nelem[b] && std::getline(f, l); ++i) {
         for (char& c : l)
@@ -710,13 +712,19 @@ int main(int argc, char** argv) {
   }
   try {
     Deck d = load(in);
-    if (d.isx || d.isy) throw std::runtime_error("geometric symmetry (ISX/ISY != 0) is not built in the GPU path");
+    // a half mesh (ISX or ISY = 1) is unfolded by the library; generalized
+    // modes would need each mode's parity under the mirror, which the deck
+    // does not give
+    if ((d.isx || d.isy) && d.genmod)
+      throw std::runtime_error("generalized modes (gen_mod_*) with geometric symmetry (ISX/ISY = 1) are not supported");
     const int nb = d.nbody, ndof = 6 * nb, nf = (int)d.wvnb.size(), nbeta = (int)d.wvhd.size();
     const double g = 9.80665;
     hams_geom geo{};
     geo.nelem = d.nelem;
     geo.ntnd = d.ntnd;
     geo.nbody = nb;
+    geo.isx = d.isx;
+    geo.isy = d.isy;
     geo.xyz = d.xyz.data();
     geo.ncn = d.ncn.data();
     geo.ncon = d.ncon.data();

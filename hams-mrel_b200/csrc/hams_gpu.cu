@@ -656,6 +656,7 @@ struct hams_ctx {
   int sms = 148;
   int sg_used = 0;  // the last solve evaluated its far pairs with the surrogate
   std::string note;  // what the last solve changed on its own (fallbacks), or empty
+  bool unfolded = false;  // built from a half mesh (ISX or ISY = 1), see unfold_symmetry
 };
 
 static int launch_check(hams_ctx* c, int count = 1) {
@@ -926,6 +927,99 @@ static int make_lane(hams_ctx* c, hams_ctx** out) {
   return 0;
 }
 
+// Geometric symmetry (ISX = 1: the mesh holds the half x >= 0 of every body,
+// mirrored in the plane x = 0; ISY = 1: the half y >= 0, mirrored in y = 0).
+// The reference solves the symmetric and antisymmetric systems of the half
+// mesh (NSYS = 2: field points imaged with the SX/SY signs, A, B and D
+// combined with RXY, HAMS_Prog.f90 and CalGreenFuncMulti.f90).  Both
+// systems together are the full body's system in another basis, so here the
+// half mesh is unfolded into the full one: each body's panels followed by
+// their mirror images (nodes appended after the originals, vertex order
+// reversed so the normals stay outward), the mirrored centres, areas and
+// sizes, n' = M n and (r x n)' = -M (r x n) for the mirror M, which holds
+// for reference points on the symmetry plane (the plane the reference's
+// sign tables assume).  Water-plane panel centres are mirrored the same way
+// and appended.  The forces are then those of the full bodies, as the
+// reference reports them.
+struct Unfolded {
+  std::vector<double> xyz, xyz_p, ds, pnsz, dxyz, ixyz_p;
+  std::vector<int32_t> ncn, ncon, body_nelem;
+  hams_geom g{};
+};
+
+static void unfold_symmetry(const hams_geom* geo, Unfolded& u) {
+  const int n = geo->nelem, nt = geo->ntnd, nb = geo->nbody, n2 = 2 * n, nt2 = 2 * nt;
+  const int ax = geo->isx ? 0 : 1;  // the coordinate the mirror negates
+  u.xyz.resize((size_t)3 * nt2);
+  for (int k = 0; k < 3; ++k)
+    for (int i = 0; i < nt; ++i) {
+      const double v = geo->xyz[i + (size_t)k * nt];
+      u.xyz[i + (size_t)k * nt2] = v;
+      u.xyz[nt + i + (size_t)k * nt2] = k == ax ? -v : v;
+    }
+  u.ncn.resize(n2);
+  u.ncon.assign((size_t)4 * n2, 0);
+  u.xyz_p.resize((size_t)3 * n2);
+  u.ds.resize(n2);
+  u.pnsz.resize(n2);
+  u.dxyz.resize((size_t)6 * n2);
+  u.body_nelem.resize(nb);
+  // sign of each dxyz column under the mirror: n' = M n, (r x n)' = -M (r x n)
+  double sgn[6];
+  for (int k = 0; k < 3; ++k) {
+    sgn[k] = k == ax ? -1.0 : 1.0;
+    sgn[3 + k] = k == ax ? 1.0 : -1.0;
+  }
+  int src = 0, dst = 0;
+  for (int b = 0; b < nb; ++b) {
+    const int m = geo->body_nelem[b];
+    for (int half = 0; half < 2; ++half)
+      for (int q = 0; q < m; ++q, ++dst) {
+        const int i = src + q, nc = geo->ncn[i];
+        u.ncn[dst] = nc;
+        for (int v = 0; v < nc; ++v) {
+          // mirrored panels: vertices 0, nc-1, ..., 1 of the mirrored nodes
+          const int sv = half == 0 ? v : (v == 0 ? 0 : nc - v);
+          const int id = geo->ncon[i + (size_t)sv * n];
+          u.ncon[dst + (size_t)v * n2] = half == 0 ? id : id + nt;
+        }
+        for (int k = 0; k < 3; ++k) {
+          const double v = geo->xyz_p[i + (size_t)k * n];
+          u.xyz_p[dst + (size_t)k * n2] = half == 1 && k == ax ? -v : v;
+        }
+        u.ds[dst] = geo->ds[i];
+        u.pnsz[dst] = geo->pnsz[i];
+        for (int k = 0; k < 6; ++k) u.dxyz[dst + (size_t)k * n2] = (half == 1 ? sgn[k] : 1.0) * geo->dxyz[i + (size_t)k * n];
+      }
+    u.body_nelem[b] = 2 * m;
+    src += m;
+  }
+  u.g = *geo;
+  u.g.isx = u.g.isy = 0;
+  u.g.nelem = n2;
+  u.g.ntnd = nt2;
+  u.g.xyz = u.xyz.data();
+  u.g.ncn = u.ncn.data();
+  u.g.ncon = u.ncon.data();
+  u.g.xyz_p = u.xyz_p.data();
+  u.g.ds = u.ds.data();
+  u.g.pnsz = u.pnsz.data();
+  u.g.dxyz = u.dxyz.data();
+  u.g.body_nelem = u.body_nelem.data();
+  if (geo->inelem > 0 && geo->ixyz_p) {
+    const int nl = geo->inelem, nl2 = 2 * nl;
+    u.ixyz_p.resize((size_t)3 * nl2);
+    for (int k = 0; k < 3; ++k)
+      for (int i = 0; i < nl; ++i) {
+        const double v = geo->ixyz_p[i + (size_t)k * nl];
+        u.ixyz_p[i + (size_t)k * nl2] = v;
+        u.ixyz_p[nl + i + (size_t)k * nl2] = k == ax ? -v : v;
+      }
+    u.g.inelem = nl2;
+    u.g.ixyz_p = u.ixyz_p.data();
+  }
+}
+
 extern "C" int hams_ctx_create(const hams_geom* geo, const hams_opts* opts, hams_ctx** out) {
   g_err.clear();
   if (!geo || !opts || !out) return fail(HAMS_ERR_ARG, "null argument");
@@ -933,13 +1027,24 @@ extern "C" int hams_ctx_create(const hams_geom* geo, const hams_opts* opts, hams
   if (geo->nelem <= 0 || geo->nbody <= 0 || !geo->xyz || !geo->ncn || !geo->ncon || !geo->xyz_p || !geo->ds ||
       !geo->pnsz || !geo->dxyz || !geo->body_nelem)
     return fail(HAMS_ERR_ARG, "incomplete geometry");
-  if (geo->isx != 0 || geo->isy != 0)
-    return fail(HAMS_ERR_UNSUPPORTED, "geometric symmetry (ISX/ISY != 0) is not built in the GPU path");
+  if (geo->isx < 0 || geo->isx > 1 || geo->isy < 0 || geo->isy > 1)
+    return fail(HAMS_ERR_ARG, "ISX/ISY must be 0 or 1");
+  if (geo->isx && geo->isy) return fail(HAMS_ERR_UNSUPPORTED, "ISX = ISY = 1 (two symmetry planes) is not supported");
+  Unfolded unf;
+  if (geo->isx || geo->isy) {
+    for (int i = 0; i < geo->nelem; ++i)
+      if (geo->ncn[i] != 3 && geo->ncn[i] != 4)
+        return fail(HAMS_ERR_ARG, "panel %d has %d vertices (3 or 4 expected)", i + 1, geo->ncn[i]);
+    if (2.0 * geo->nelem * 2.0 * geo->nelem > 4294967295.0) return fail(HAMS_ERR_UNSUPPORTED, "unfolded mesh too large");
+    unfold_symmetry(geo, unf);
+    geo = &unf.g;
+  }
   if (opts->irsp == 1 && (geo->inelem <= 0 || !geo->ixyz_p)) return fail(HAMS_ERR_ARG, "irsp=1 needs water-plane panels");
   if (opts->precision != HAMS_PREC_FP64 && opts->precision != HAMS_PREC_MIXED)
     return fail(HAMS_ERR_ARG, "unknown precision %d", opts->precision);
   if (opts->solver < 0 || opts->solver > HAMS_SOLVER_GMRES) return fail(HAMS_ERR_ARG, "unknown solver %d", opts->solver);
   hams_ctx* c = new hams_ctx();
+  c->unfolded = geo == &unf.g;
   c->opts = *opts;
   c->dev = opts->device;
   c->n = geo->nelem;
@@ -1634,6 +1739,8 @@ extern "C" int hams_assemble(hams_ctx* c, const hams_wave* w, int32_t nbeta, con
                              double* brmat, double* bdmat) {
   g_err.clear();
   if (!c || !w || (nbeta > 0 && !beta)) return fail(HAMS_ERR_ARG, "null argument");
+  if (c->unfolded)
+    return fail(HAMS_ERR_UNSUPPORTED, "hams_assemble: the context holds the unfolded mesh of a half-mesh deck");
   if (cudaSetDevice(c->dev) != cudaSuccess) return fail(HAMS_ERR_CUDA, "cudaSetDevice failed");
   const int n = c->n, tn = c->tn, ndof = 6 * c->nb, nrhs = ndof + nbeta;
   TRY(c->beta.alloc(std::max(nbeta, 1)));

@@ -78,7 +78,10 @@ typedef struct hams_geom {
   int32_t nelem;               /* hull panels of all bodies (N)                  */
   int32_t ntnd;                /* hull nodes                                      */
   int32_t nbody;               /* bodies                                          */
-  int32_t isx, isy;            /* symmetry flags of the .pnl header (0 0 only)    */
+  int32_t isx, isy;            /* symmetry flags of the .pnl header: 0 0, or one
+                                  of them 1 for a half mesh (x >= 0 mirrored in
+                                  x = 0, or y >= 0 in y = 0; reference points on
+                                  the plane), unfolded into the full bodies    */
   const double *xyz;           /* (ntnd,3)  node coordinates                      */
   const int32_t *ncn;          /* (nelem)   vertices per panel, 3 or 4            */
   const int32_t *ncon;         /* (nelem,4) vertex node ids, 1-based              */
@@ -190,7 +193,8 @@ int hams_solve_batch(hams_ctx *ctx, int32_t nfreq, const hams_wave *waves, int32
  *   amat (n,n)        A of ASSB_LEFT_MULTI (or C = A^T A with lids)
  *   brmat (n,6nb)     radiation right-hand sides (or A^T B)
  *   bdmat (n,nbeta)   diffraction right-hand sides (or A^T B)
- * Any output pointer may be NULL. */
+ * Any output pointer may be NULL.  A context made from a half mesh
+ * (ISX or ISY = 1) holds the unfolded mesh and returns HAMS_ERR_UNSUPPORTED. */
 int hams_assemble(hams_ctx *ctx, const hams_wave *wave, int32_t nbeta, const double *beta_rad, double *amat,
                   double *brmat, double *bdmat);
 
