@@ -7,13 +7,19 @@
 // factorisation only has to be a good preconditioner, so it is organised for
 // the tensor cores instead of following LAPACK's pivot order:
 //
-//   for each diagonal block k (kNB = 64 rows):
-//     k_diag_lu      one CTA factors A_kk = P_k^T L_kk U_kk in shared memory
+//   for each panel of kPB = 4 diagonal blocks (256 columns):
+//     for each diagonal block k (kNB = 64 rows) of the panel:
+//       k_diag_lu    one CTA factors A_kk = P_k^T L_kk U_kk in shared memory
 //                    with partial pivoting inside the block, and forms
 //                    L_kk^-1 and U_kk^-1;
-//     k_apply_perm   applies P_k to the rest of block row k;
-//     GEMM           U_kj = L_kk^-1 A_kj, L_ik = A_ik U_kk^-1;
-//     GEMM           A_ij -= L_ik U_kj, the rank-64 trailing update.
+//       k_apply_perm applies P_k to the rest of block row k;
+//       GEMM         L_ik = A_ik U_kk^-1 below the block, U_kj = L_kk^-1 A_kj
+//                    and A_ij -= L_ik U_kj for the panel's columns only;
+//     GEMM           the panel's U rows for the columns right of it, by
+//                    block forward substitution with the L_kk^-1;
+//     GEMM           A_tt -= L_t,panel U_panel,t, one rank-256 trailing
+//                    update per panel (the trailing matrix is read and
+//                    written once per 256 columns instead of once per 64).
 //
 // The complex products run as real GEMMs on the real expansions of the
 // complex matrices (cuBLAS, tensor cores, FP32 accumulation; inputs rounded
@@ -24,11 +30,14 @@
 #include <cublas_v2.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "lu_mixed.h"
 
 namespace {
 
 constexpr int kNB = 64;
+constexpr int kPB = 4;   // diagonal blocks per panel: the trailing update runs once per kPB kNB columns
 constexpr int kLd = kNB + 1;  // padded shared-memory leading dimension
 
 // Real expansion of complex matrices.  A complex p x q matrix X becomes the
@@ -255,53 +264,109 @@ cublasStatus_t sgemm(cublasHandle_t h, cublasComputeType_t ct, int m, int n, int
 
 }  // namespace
 
-// U panel (2kNB x n floats), expanded L panel and its source (2 x 2n x 2kNB),
-// expanded inverses of the diagonal block (2 x 2kNB x 2kNB).
+// Workspace (floats): U rows W1 (2kNB x n), expanded L column of a block and
+// its source (2 x 2n x 2kNB), the expanded inverses of a panel's diagonal
+// blocks (2 x kPB x 2kNB x 2kNB), the expanded L rows of a block left of it
+// in its panel (2kNB x 2kNB (kPB - 1)) and the expanded L columns of a whole
+// panel (2n x 2kNB kPB).
 size_t mixed_lu_workspace_elems(int n) {
-  return (2 * (size_t)kNB * n + 2 * (2 * (size_t)n * 2 * kNB) + 2 * (size_t)(2 * kNB) * (2 * kNB)) / 2 + 1;
+  const size_t K2 = 2 * kNB;
+  return (K2 * n + 2 * (2 * (size_t)n * K2) + 2 * kPB * K2 * K2 + K2 * K2 * (kPB - 1) + 2 * (size_t)n * K2 * kPB) / 2 +
+         1;
 }
 
 int mixed_lu_factor(cudaStream_t st, cublasHandle_t blas, cublasComputeType_t ct, int n, float2* A, int* perm,
                     float2* work, int* dinfo, long long* launches, long long* lib_calls) {
   const int smem = (3 * kNB + 32) * kLd * (int)sizeof(float2);
   if (cudaFuncSetAttribute(k_diag_lu, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess) return 1;
-  const int nblk = (n + kNB - 1) / kNB, K2 = 2 * kNB;
-  float* W1 = (float*)work;                     // U panel, real 2nbk x w (ld 2kNB)
+  const int K2 = 2 * kNB, PW = kPB * kNB;
+  float* W1 = (float*)work;                     // U rows, real 2nbk x w (ld 2kNB)
   float* Ehat = W1 + (size_t)K2 * n;            // expanded A_ik, 2w x 2nbk (ld 2w)
   float* Lhat = Ehat + (size_t)2 * n * K2;      // expanded L_ik, 2w x 2nbk (ld 2w)
-  float* invL = Lhat + (size_t)2 * n * K2;      // 2nbk x 2nbk (ld 2kNB)
-  float* invU = invL + (size_t)K2 * K2;
+  float* invL = Lhat + (size_t)2 * n * K2;      // kPB x (2nbk x 2nbk, ld 2kNB)
+  float* invU = invL + (size_t)kPB * K2 * K2;
+  float* E2 = invU + (size_t)kPB * K2 * K2;     // expanded L rows left of a block, 2nbk x 2(k0 - p0) (ld 2nbk)
+  float* Ebig = E2 + (size_t)K2 * K2 * (kPB - 1);  // expanded L columns of a panel, 2wt x 2(p1 - p0) (ld 2wt)
   if (cudaMemsetAsync(dinfo, 0x7f, sizeof(int), st) != cudaSuccess) return 1;  // large positive: no zero pivot
-  if (cudaMemsetAsync(invL, 0, 2 * (size_t)K2 * K2 * sizeof(float), st) != cudaSuccess) return 1;
+  if (cudaMemsetAsync(invL, 0, 2 * (size_t)kPB * K2 * K2 * sizeof(float), st) != cudaSuccess) return 1;
   float* Ar = (float*)A;  // A viewed as floats: 2n x n, ld 2n
-  for (int b = 0; b < nblk; ++b) {
-    const int k0 = b * kNB, nbk = (n - k0 < kNB) ? n - k0 : kNB, k1 = k0 + nbk, w = n - k1, k2 = 2 * nbk;
-    k_diag_lu<<<1, 256, smem, st>>>(A, n, k0, nbk, perm, invL, invU, dinfo);
-    k_apply_perm<<<(n + 31) / 32, 256, 0, st>>>(A, n, n, k0, nbk, perm);
-    *launches += 2;
-    if (cudaGetLastError() != cudaSuccess) return 1;
-    if (w <= 0) break;
-    k_expand_panel<<<(unsigned)(((size_t)w * nbk + 255) / 256), 256, 0, st>>>(A, n, k1, k0, w, nbk, Ehat);
+  const size_t ldr = 2 * (size_t)n;
+  cublasStatus_t bs;
+  for (int p0 = 0, pb = 0; p0 < n; p0 += PW, ++pb) {
+    const int p1 = std::min(n, p0 + PW);
+    // the panel's column blocks, updates confined to the panel's columns
+    for (int s = 0, k0 = p0; k0 < p1; ++s, k0 += kNB) {
+      const int b = pb * kPB + s, nbk = std::min(kNB, n - k0), k1 = k0 + nbk, wr = n - k1, wp = p1 - k1,
+                k2 = 2 * nbk;
+      float* iL = invL + (size_t)s * K2 * K2;
+      float* iU = invU + (size_t)s * K2 * K2;
+      k_diag_lu<<<1, 256, smem, st>>>(A, n, k0, nbk, perm, iL, iU, dinfo);
+      k_apply_perm<<<(n + 31) / 32, 256, 0, st>>>(A, n, n, k0, nbk, perm);
+      *launches += 2;
+      if (cudaGetLastError() != cudaSuccess) return 1;
+      if (wr <= 0) break;
+      k_expand_panel<<<(unsigned)(((size_t)wr * nbk + 255) / 256), 256, 0, st>>>(A, n, k1, k0, wr, nbk, Ehat);
+      *launches += 1;
+      if (cudaGetLastError() != cudaSuccess) return 1;
+      // L_ik^ = A_ik^ U_kk^-1^
+      if ((bs = sgemm(blas, ct, 2 * wr, k2, k2, 1.0f, Ehat, 2 * wr, iU, K2, 0.0f, Lhat, 2 * wr)) != CUBLAS_STATUS_SUCCESS)
+        return 200 + 1000 * b + (int)bs;
+      *lib_calls += 1;
+      if (wp > 0) {
+        float* Akj = Ar + (size_t)k1 * ldr + 2 * k0;  // real 2nbk x wp, ld 2n
+        float* Aij = Ar + (size_t)k1 * ldr + 2 * k1;  // real 2wr x wp, ld 2n
+        // U_kj = L_kk^-1 A_kj and A_ij -= L_ik U_kj inside the panel
+        if ((bs = sgemm(blas, ct, k2, wp, k2, 1.0f, iL, K2, Akj, (int)ldr, 0.0f, W1, K2)) != CUBLAS_STATUS_SUCCESS)
+          return 100 + 1000 * b + (int)bs;
+        if ((bs = sgemm(blas, ct, 2 * wr, wp, k2, -1.0f, Lhat, 2 * wr, W1, K2, 1.0f, Aij, (int)ldr)) !=
+            CUBLAS_STATUS_SUCCESS)
+          return 300 + 1000 * b + (int)bs;
+        *lib_calls += 2;
+        if (cudaMemcpy2DAsync(Akj, ldr * 4, W1, (size_t)K2 * 4, (size_t)k2 * 4, wp, cudaMemcpyDeviceToDevice, st) !=
+            cudaSuccess)
+          return 1;
+      }
+      // L_ik = the even columns of L_ik^
+      if (cudaMemcpy2DAsync(A + (size_t)k0 * n + k1, (size_t)n * 8, Lhat, (size_t)2 * (2 * wr) * 4, (size_t)2 * wr * 4,
+                            nbk, cudaMemcpyDeviceToDevice, st) != cudaSuccess)
+        return 1;
+    }
+    const int wt = n - p1;
+    if (wt <= 0) break;
+    // U rows of the panel for the columns right of it: block forward
+    // substitution with the panel's unit lower diagonal blocks
+    float* Upt = Ar + (size_t)p1 * ldr + 2 * p0;  // real 2(p1 - p0) x wt, ld 2n
+    for (int s = 0, k0 = p0; k0 < p1; ++s, k0 += kNB) {
+      const int b = pb * kPB + s, nbk = std::min(kNB, p1 - k0), k2 = 2 * nbk;
+      float* Akt = Ar + (size_t)p1 * ldr + 2 * k0;  // real 2nbk x wt, ld 2n
+      if (s > 0) {
+        const int wl = k0 - p0;  // A_kt -= L_k,[p0,k0) U_[p0,k0),t
+        k_expand_panel<<<(unsigned)(((size_t)nbk * wl + 255) / 256), 256, 0, st>>>(A, n, k0, p0, nbk, wl, E2);
+        *launches += 1;
+        if (cudaGetLastError() != cudaSuccess) return 1;
+        if ((bs = sgemm(blas, ct, k2, wt, 2 * wl, -1.0f, E2, k2, Upt, (int)ldr, 1.0f, Akt, (int)ldr)) !=
+            CUBLAS_STATUS_SUCCESS)
+          return 400 + 1000 * b + (int)bs;
+        *lib_calls += 1;
+      }
+      if ((bs = sgemm(blas, ct, k2, wt, k2, 1.0f, invL + (size_t)s * K2 * K2, K2, Akt, (int)ldr, 0.0f, W1, K2)) !=
+          CUBLAS_STATUS_SUCCESS)
+        return 500 + 1000 * b + (int)bs;
+      *lib_calls += 1;
+      if (cudaMemcpy2DAsync(Akt, ldr * 4, W1, (size_t)K2 * 4, (size_t)k2 * 4, wt, cudaMemcpyDeviceToDevice, st) !=
+          cudaSuccess)
+        return 1;
+    }
+    // the trailing update of the whole panel at once: A_tt -= L_t,panel U_panel,t
+    const int pw = p1 - p0;
+    k_expand_panel<<<(unsigned)(((size_t)wt * pw + 255) / 256), 256, 0, st>>>(A, n, p1, p0, wt, pw, Ebig);
     *launches += 1;
     if (cudaGetLastError() != cudaSuccess) return 1;
-    float* Akj = Ar + (size_t)k1 * 2 * n + 2 * k0;  // real 2nbk x w, ld 2n
-    float* Aij = Ar + (size_t)k1 * 2 * n + 2 * k1;  // real 2w x w, ld 2n
-    // U_kj = L_kk^-1 A_kj;  L_ik^ = A_ik^ U_kk^-1^;  A_ij -= L_ik U_kj
-    cublasStatus_t bs;
-    if ((bs = sgemm(blas, ct, k2, w, k2, 1.0f, invL, K2, Akj, 2 * n, 0.0f, W1, K2)) != CUBLAS_STATUS_SUCCESS)
-      return 100 + 1000 * b + (int)bs;
-    if ((bs = sgemm(blas, ct, 2 * w, k2, k2, 1.0f, Ehat, 2 * w, invU, K2, 0.0f, Lhat, 2 * w)) != CUBLAS_STATUS_SUCCESS)
-      return 200 + 1000 * b + (int)bs;
-    if ((bs = sgemm(blas, ct, 2 * w, w, k2, -1.0f, Lhat, 2 * w, W1, K2, 1.0f, Aij, 2 * n)) != CUBLAS_STATUS_SUCCESS)
-      return 300 + 1000 * b + (int)bs;
-    *lib_calls += 3;
-    // U_kj back into A; L_ik = the even columns of L_ik^
-    if (cudaMemcpy2DAsync(Akj, (size_t)2 * n * 4, W1, (size_t)K2 * 4, (size_t)k2 * 4, w, cudaMemcpyDeviceToDevice, st) !=
-        cudaSuccess)
-      return 1;
-    if (cudaMemcpy2DAsync(A + (size_t)k0 * n + k1, (size_t)n * 8, Lhat, (size_t)2 * (2 * w) * 4, (size_t)2 * w * 4, nbk,
-                          cudaMemcpyDeviceToDevice, st) != cudaSuccess)
-      return 1;
+    float* Att = Ar + (size_t)p1 * ldr + 2 * p1;  // real 2wt x wt, ld 2n
+    if ((bs = sgemm(blas, ct, 2 * wt, wt, 2 * pw, -1.0f, Ebig, 2 * wt, Upt, (int)ldr, 1.0f, Att, (int)ldr)) !=
+        CUBLAS_STATUS_SUCCESS)
+      return 600 + 1000 * pb * kPB + (int)bs;
+    *lib_calls += 1;
   }
   return 0;
 }
