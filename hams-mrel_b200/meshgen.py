@@ -209,12 +209,13 @@ def case_c3(seed):
                 omegas=np.linspace(0.1, 3.0, 16), betas_deg=[0.0])
 
 
-def write_pnl(path, nodes, ncn, ncon, title="Hull Mesh"):
-    """.pnl file in the layout ReadBodyMesh reads (ReadPanelMesh.f90:46-99)."""
+def write_pnl(path, nodes, ncn, ncon, title="Hull Mesh", isx=0, isy=0):
+    """.pnl file in the layout ReadBodyMesh reads (ReadPanelMesh.f90:46-99); isx / isy = 1 marks a
+    half mesh (the part x >= 0 or y >= 0 of a body symmetric in that plane)."""
     with open(path, "w") as f:
         f.write(f"    --------------{title} File---------------\n \n")
         f.write("    # Number of Panels, Nodes, X-Symmetry and Y-Symmetry\n")
-        f.write(f"{ncn.size:12d}{nodes.shape[0]:12d}{0:12d}{0:12d}\n \n")
+        f.write(f"{ncn.size:12d}{nodes.shape[0]:12d}{isx:12d}{isy:12d}\n \n")
         f.write("    # Start Definition of Node Coordinates     ! node_number   x   y   z\n")
         for i, (x, y, z) in enumerate(nodes):
             f.write(f"{i + 1:5d}{x:18.6f}{y:18.6f}{z:18.6f}\n")
@@ -226,14 +227,16 @@ def write_pnl(path, nodes, ncn, ncon, title="Hull Mesh"):
 
 
 def write_deck(directory, case, nthread=8):
-    """ControlFile.in, HullMesh[_k].pnl and Hydrostatic[_k].in for `case` (input frequency type 3)."""
+    """ControlFile.in, HullMesh[_k].pnl and Hydrostatic[_k].in for `case` (input frequency type 3;
+    case["isx"] / case["isy"] = 1 for half meshes)."""
     os.makedirs(directory, exist_ok=True)
     nb = len(case["bodies"])
     multi = nb > 1
     lids = case.get("lids")
     for b, (nodes, ncn, ncon) in enumerate(case["bodies"]):
         # bodies are written in global coordinates with LCS = 0
-        write_pnl(os.path.join(directory, f"HullMesh_{b + 1}.pnl" if multi else "HullMesh.pnl"), nodes, ncn, ncon)
+        write_pnl(os.path.join(directory, f"HullMesh_{b + 1}.pnl" if multi else "HullMesh.pnl"), nodes, ncn, ncon,
+                  isx=case.get("isx", 0), isy=case.get("isy", 0))
         with open(os.path.join(directory, f"Hydrostatic_{b + 1}.in" if multi else "Hydrostatic.in"), "w") as f:
             f.write(" Center of Gravity:\n  0.0  0.0  0.0\n")
             for title in ("Body Mass Matrix:", "External Linear Damping Matrix:", "External Quadratic Damping Matrix:",
@@ -242,7 +245,7 @@ def write_deck(directory, case, nthread=8):
         if lids:
             lnodes, lncn, lncon = lids[b]
             write_pnl(os.path.join(directory, f"WaterPlaneMesh_{b + 1}.pnl" if multi else "WaterPlaneMesh.pnl"),
-                      lnodes, lncn, lncon, title="WaterPlane Mesh")
+                      lnodes, lncn, lncon, title="WaterPlane Mesh", isx=case.get("isx", 0), isy=case.get("isy", 0))
     om = case["omegas"]
     with open(os.path.join(directory, "ControlFile.in"), "w") as f:
         f.write("   --------------HAMS Control file---------------\n\n")

@@ -173,3 +173,29 @@ def test_driver_wamit_force_and_motion_files(tmp_path, deck):
         got, ref = np.array([got_by[h] for h in rh]), np.array(rv)
         err = np.linalg.norm(got - ref) / np.linalg.norm(ref)
         assert err < tol, f"{deck} {name}: relative Frobenius {err:.2e}"
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("axis", [0, 1])
+def test_driver_symmetric_half_mesh_deck(tmp_path, axis):
+    """A deck of half meshes (ISX = 1 or ISY = 1): the driver's files match the oracle's NSYS = 2
+    solve of the same deck to 1e-7."""
+    import meshgen
+    import test_symmetry
+
+    bodies, _, xr = test_symmetry.two_cylinders(axis)
+    case = dict(bodies=bodies, centres=[tuple(c) for c in xr], depth=40.0, omegas=np.array([0.6, 1.2]),
+                betas_deg=[0.0, 30.0], **({"isx": 1} if axis == 0 else {"isy": 1}))
+    inp = tmp_path / "input"
+    meshgen.write_deck(str(inp), case)
+    r = subprocess.run([RUN, str(inp), str(tmp_path / "gpu")], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    (tmp_path / "cpu").mkdir()
+    assert oracle_lib.load().orc_run_case(str(inp).encode(), str(tmp_path / "cpu").encode(), 8,
+                                          os.cpu_count() or 1) == 0
+    for kind in ("OAMASS", "ODAMPING", "OEXFOR"):
+        for m in range(1, 7):
+            head, got = _load(tmp_path / "gpu" / "Hams_format" / f"{kind}{m}.txt")
+            ohead, orc = _load(tmp_path / "cpu" / f"{kind}{m}.txt")
+            assert head == ohead
+            assert np.linalg.norm(got - orc) <= 1e-7 * np.linalg.norm(orc) + 1e-12, f"{kind}{m}"
