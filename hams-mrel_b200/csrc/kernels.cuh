@@ -36,15 +36,22 @@ __device__ __forceinline__ int near_flag(const DevGeom& g, int i, int j) {
 // A(I,J) (double layer, with 2 pi on the hull diagonal) and S(I,J) (single
 // layer) of one pair from its Green-function set, as BODINT_MULTI_LEFT and
 // RBC/DBC_MULTI_RIGHT combine them (BodyIntgrMulti.f90:48-173).
-__device__ __forceinline__ void store_pair(const DevGeom& g, size_t p, int i, int j, const grn4& G,
-                                           const double* __restrict__ rs, const double* __restrict__ rd,
-                                           double2* __restrict__ A, double2* __restrict__ S) {
-  double ds = g.ds[j], n1 = g.nrm[j], n2 = g.nrm[j + g.n], n3 = g.nrm[j + 2 * g.n];
-  double are = rd[p] + ds * (G.g[1].re * n1 + G.g[2].re * n2 + G.g[3].re * n3);
+// The same from the pair's source-panel area ds, normal n1..n3 and Rankine
+// terms rsp, rdp already in registers.
+__device__ __forceinline__ void store_pair_v(size_t p, int i, int j, const grn4& G, double ds, double n1, double n2,
+                                             double n3, double rsp, double rdp, double2* __restrict__ A,
+                                             double2* __restrict__ S) {
+  double are = rdp + ds * (G.g[1].re * n1 + G.g[2].re * n2 + G.g[3].re * n3);
   double aim = ds * (G.g[1].im * n1 + G.g[2].im * n2 + G.g[3].im * n3);
   if (i == j) are += 2.0 * 3.141592653589793;  // A(I,I) = 2 pi on hull rows (AssbMatxMulti.f90:75)
   A[p] = make_double2(are, aim);
-  S[p] = make_double2(rs[p] + G.g[0].re * ds, G.g[0].im * ds);
+  S[p] = make_double2(rsp + G.g[0].re * ds, G.g[0].im * ds);
+}
+
+__device__ __forceinline__ void store_pair(const DevGeom& g, size_t p, int i, int j, const grn4& G,
+                                           const double* __restrict__ rs, const double* __restrict__ rd,
+                                           double2* __restrict__ A, double2* __restrict__ S) {
+  store_pair_v(p, i, j, G, g.ds[j], g.nrm[j], g.nrm[j + g.n], g.nrm[j + 2 * g.n], rs[p], rd[p], A, S);
 }
 
 
