@@ -177,7 +177,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_green_sg(DevGeom g, WaveDev w, 
     double xp = 0, yp = 0, zp = -0.25 * h, xq = 0.1 * h, yq = 0, zq = -0.25 * h;
     // the pair's FP64 operands of the epilogue, loaded now so that their
     // latency passes under the network's layers
-    double pf_rs = 0.0, pf_rd = 0.0, pf_ds = 0.0, pf_n1 = 0.0, pf_n2 = 0.0, pf_n3 = 0.0, pf_pn = 0.0;
+    double pf_rs = 0.0, pf_rd = 0.0, pf_ds = 0.0, pf_n1 = 0.0, pf_n2 = 0.0, pf_n3 = 0.0, pf_pn = 0.0, pf_fld = 0.0;
+    double2 pf_src = make_double2(0.0, 0.0);
     if (live) {
       p = pairs[tp];
       i = (int)(p % (size_t)g.tn);
@@ -195,6 +196,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_green_sg(DevGeom g, WaveDev w, 
       pf_n2 = g.nrm[j + g.n];
       pf_n3 = g.nrm[j + 2 * g.n];
       pf_pn = g.pnsz[j];
+      pf_src = mt.src[g.n + j];  // the propagating mode's vertical factors (mode-table slot 1)
+      pf_fld = mt.fld[g.tn + i];
     }
     const double xpq = xq - xp, ypq = yq - yp;
     const double rr = sqrt(xpq * xpq + ypq * ypq);
@@ -280,8 +283,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_green_sg(DevGeom g, WaveDev w, 
       hams::cplx fg[3];
       double rk[3];
       {
-        const double2 sc = mt.src[g.n + j];
-        const double czp = mt.fld[g.tn + i], p0 = mt.pm[1] * sc.y * czp, dp0 = mt.pm[1] * sc.x * czp;
+        const double2 sc = pf_src;
+        const double czp = pf_fld, p0 = mt.pm[1] * sc.y * czp, dp0 = mt.pm[1] * sc.x * czp;
         double j0, j1, y0, y1;
         hams::jy01b(w.wk * rr, j0, j1, y0, y1);
         fg[0] = hams::cmk(-p0 * y0, p0 * j0);
