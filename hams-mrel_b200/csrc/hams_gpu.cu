@@ -146,6 +146,20 @@ __global__ void k_pair_keys(DevGeom g, double h, int sg_on, double far, const un
   idx[p] = (uint32_t)p;
 }
 
+// First index of each bin b = 0..nbins in the sorted keys (key >> 8 is the bin).
+__global__ void k_bin_offsets(const uint32_t* __restrict__ keys, long long np, int nbins, long long* off) {
+  const int b = threadIdx.x;
+  if (b > nbins) return;
+  const uint32_t v = (uint32_t)b << 8;
+  long long lo = 0, hi = np;
+  while (lo < hi) {
+    const long long mid = lo + (hi - lo) / 2;
+    if (keys[mid] < v) lo = mid + 1;
+    else hi = mid;
+  }
+  off[b] = lo;
+}
+
 // ---------------------------------------------------------------------------
 // per-frequency assembly: Green function fused with the pair algebra
 // ---------------------------------------------------------------------------
@@ -722,12 +736,14 @@ static int build_pairs(hams_ctx* c) {
   TRY(tbuf.alloc(tmp));
   CU(cub::DeviceRadixSort::SortPairs(tbuf.p, tmp, keys.p, keys2.p, idx.p, c->pairs.p, np, 0, 11, c->st));
   c->lib_calls += 1;
-  // bin boundaries: first index of each bin in the sorted keys
-  std::vector<uint32_t> hk(np);
-  CU(cudaMemcpyAsync(hk.data(), keys2.p, np * 4, cudaMemcpyDeviceToHost, c->st));
+  // bin boundaries: first index of each bin in the sorted keys, found on the
+  // device (a binary search per bin) so that only kBins + 1 numbers come back
+  DBuf<long long> offs;
+  TRY(offs.alloc(kBins + 1));
+  k_bin_offsets<<<1, 32, 0, c->st>>>(keys2.p, (long long)np, kBins, offs.p);
+  TRY(launch_check(c));
+  CU(cudaMemcpyAsync(c->bin_off, offs.p, (kBins + 1) * sizeof(long long), cudaMemcpyDeviceToHost, c->st));
   CU(cudaStreamSynchronize(c->st));
-  for (int b = 0; b <= kBins; ++b)
-    c->bin_off[b] = std::lower_bound(hk.begin(), hk.end(), (uint32_t)(b << 8), [](uint32_t a, uint32_t v) { return a < v; }) - hk.begin();
   return 0;
 }
 
