@@ -8,12 +8,17 @@ Green functions and assembly of the 5,400 x 5,400 complex system, the LU
 factorisation and solve, and the added-mass / damping / excitation
 reductions.  Synthetic parametric mesh (no external data).
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--form mixed|fp64]
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--form surrogate|mixed|fp64]
   python bench.py --impl reference ...   # the CPU implementation on the host cores
 
-Each rank solves its own K frequencies (weak scaling, no data-path
-collective); the timed region is the max over ranks of the device time
-between two events on the library's stream.  Rank 0 prints one JSON line.
+The default form is the surrogate form (network far pairs, the Green
+functions of identical body pairs computed once, complex64 panel LU on the
+tensor cores with FP64 refinement); the mixed and fp64 forms run on the same
+frequencies for the comparison and the error.  Each rank solves its own K
+frequencies (weak scaling, no data-path collective); the timed region is the
+max over ranks of the device time between two events on the library's
+stream.  `e2e` repeats the main form through the C ABI from host buffers,
+context set-up included.  Rank 0 prints one JSON line.
 """
 import argparse
 import json
