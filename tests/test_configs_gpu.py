@@ -6,8 +6,9 @@ infinite depth): the six smallest of the 128 seeded cases and the two
 smallest with two bodies (together: both depths, lids, two bodies) against
 the CPU oracle (added mass, damping, excitation within 1e-6 relative Frobenius, the
 plain form's bar), and the four largest (up to 5,757 panels) through the
-mixed form against the fp64 form (1e-6).  (The seed lists themselves are
-checked on the CPU.)
+mixed form against the fp64 form (1e-6); four cases in flight together, one
+host thread per case, give the same bits as one by one.  (The seed lists
+themselves are checked on the CPU.)
 
 The 6 x 6 array (`meshgen.case_c5()`: 36 cylinders, 20,160 panels, h 40 m)
 at full size, one frequency and three headings: GMRES (restart 50,
@@ -112,3 +113,34 @@ def test_c5_iterative_path_full_size():
     for x, y in zip(got, ref):
         assert np.all(np.isfinite(x)) and rel(x, y) < 1e-4
     gm.close()
+
+
+@pytest.mark.gpu
+def test_c3_cases_solved_concurrently():
+    """Heterogeneous cases in flight together: one context per case, each solved by its own host
+    thread (the C calls release the interpreter), gives the same bits as solving them one by one."""
+    import threading
+
+    seeds = SMALL[:4]
+    cases = [c3_case(s, with_oracle=False) for s in seeds]
+    runs = []
+    for c, _, ctx in cases:
+        waves = [hams_b200.wave_properties(om, c["depth"], G) for om in c["omegas"][::4]]
+        runs.append((ctx, waves, np.radians(c["betas_deg"])))
+    alone = [ctx.solve_batch(w, b) for ctx, w, b in runs]
+    together = [None] * len(runs)
+
+    def work(k):
+        ctx, w, b = runs[k]
+        together[k] = ctx.solve_batch(w, b)
+
+    th = [threading.Thread(target=work, args=(k,)) for k in range(len(runs))]
+    for t in th:
+        t.start()
+    for t in th:
+        t.join()
+    for a, b in zip(alone, together):
+        for x, y in zip(a, b):
+            assert np.array_equal(x, y)
+    for ctx, _, _ in runs:
+        ctx.close()
