@@ -1704,7 +1704,10 @@ extern "C" int hams_solve_batch(hams_ctx* c, int32_t nfreq, const hams_wave* wav
   std::vector<int> rc_of(nfreq, 0), lane_rc(L, 0);
   std::vector<std::string> lane_err(L), note_of(nfreq);
   c->fp_batch.assign(c->nfp > 0 ? nfreq : 0, std::vector<double>());
-  // lane t solves frequencies t, t + L, ... on its own stream and host thread
+  // each lane takes the next unsolved frequency when it is free (frequencies
+  // cost unevenly: out-of-range ones keep the series), on its own stream and
+  // host thread; every result lands at its frequency's index
+  std::atomic<int> next{0};
   auto run = [&](int t) {
     if (cudaSetDevice(c->dev) != cudaSuccess) {
       lane_rc[t] = HAMS_ERR_CUDA;
@@ -1712,7 +1715,7 @@ extern "C" int hams_solve_batch(hams_ctx* c, int32_t nfreq, const hams_wave* wav
       return;
     }
     std::vector<double> a((size_t)ndof * ndof), b((size_t)ndof * ndof), x(2 * (size_t)ndof * std::max(nbeta, 1));
-    for (int k = t; k < nfreq; k += L) {
+    for (int k = next.fetch_add(1); k < nfreq; k = next.fetch_add(1)) {
       int rc = solve_one(lane[t], &waves[k], nbeta, beta, a.data(), b.data(), x.data());
       if (rc < 0) {
         lane_rc[t] = rc;
