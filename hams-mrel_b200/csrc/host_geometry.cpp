@@ -11,6 +11,8 @@
 // each body's reference point (CalRotNormals :46).  It runs once per mesh.
 #include <algorithm>
 #include <cmath>
+#include <map>
+#include <tuple>
 #include <vector>
 
 #include "../../include/hams_gpu.h"
@@ -182,20 +184,29 @@ std::vector<int> body_block_reps(const hams_geom* g, double tol) {
   }
   const double eps = tol * std::max(1.0, hi - lo);
   // block (b1 field, b2 source) = block (c1, c2) when the templates agree and
-  // the offset of b2 from b1 equals that of c2 from c1
+  // the offset of b2 from b1 equals that of c2 from c1 (within eps); the
+  // representatives are filed by templates and offset cell (size eps), so a
+  // block looks at its own and the neighbouring cells only, and takes the
+  // first representative within eps, in block order
+  std::map<std::tuple<int, int, long long, long long>, std::vector<int>> cells;
   for (int b2 = 0; b2 < nb; ++b2)
     for (int b1 = 0; b1 < nb; ++b1) {
-      const size_t k = b1 + (size_t)nb * b2;
+      const int k = b1 + nb * b2;
       const double ox = s[b2].dx - s[b1].dx, oy = s[b2].dy - s[b1].dy;
-      for (size_t c = 0; c < k; ++c) {
-        if (rep[c] != (int)c) continue;
-        const int c1 = (int)(c % nb), c2 = (int)(c / nb);
-        if (s[c1].tmpl != s[b1].tmpl || s[c2].tmpl != s[b2].tmpl) continue;
-        if (std::fabs(s[c2].dx - s[c1].dx - ox) <= eps && std::fabs(s[c2].dy - s[c1].dy - oy) <= eps) {
-          rep[k] = (int)c;
-          break;
+      const long long qx = std::llround(ox / eps), qy = std::llround(oy / eps);
+      int best = k;
+      for (long long ex = -1; ex <= 1; ++ex)
+        for (long long ey = -1; ey <= 1; ++ey) {
+          auto it = cells.find(std::make_tuple(s[b1].tmpl, s[b2].tmpl, qx + ex, qy + ey));
+          if (it == cells.end()) continue;
+          for (int c : it->second) {
+            const int c1 = c % nb, c2 = c / nb;
+            if (c < best && std::fabs(s[c2].dx - s[c1].dx - ox) <= eps && std::fabs(s[c2].dy - s[c1].dy - oy) <= eps)
+              best = c;
+          }
         }
-      }
+      rep[k] = best;
+      if (best == k) cells[std::make_tuple(s[b1].tmpl, s[b2].tmpl, qx, qy)].push_back(k);
     }
   return rep;
 }

@@ -71,6 +71,17 @@ def test_grid_of_identical_bodies_shares_one_block_per_offset():
             assert r == first
 
 
+def test_large_grid_counts_offsets():
+    """144 small bodies on a 12 x 12 grid: one block per offset (23 x 23), found at once."""
+    pos = [(10.0 * ix, 10.0 * iy) for iy in range(12) for ix in range(12)]
+    rep, distinct = hams_b200.body_blocks(array_geom(pos, make=lambda x, y: meshgen.cylinder(2.0, 3.0, 8, 2, 1, x, y)))
+    assert distinct == 23 * 23
+    nb = len(pos)
+    for k in (1, 13, 143, nb * nb - 1, nb * 77 + 5):
+        r = rep.ravel(order="F")[k]
+        assert np.allclose(np.subtract(pos[r // nb], pos[r % nb]), np.subtract(pos[k // nb], pos[k % nb]))
+
+
 def test_uneven_row():
     rep, distinct = hams_b200.body_blocks(array_geom([(0.0, 0.0), (10.0, 0.0), (25.0, 0.0)]))
     assert distinct == 7  # one diagonal block, offsets +-10, +-15, +-25
