@@ -13,8 +13,9 @@ reductions.  Synthetic parametric mesh (no external data).
 
 The default form is the surrogate form (network far pairs, the Green
 functions of identical body pairs computed once, complex64 panel LU on the
-tensor cores with FP64 refinement); the mixed and fp64 forms run on the same
-frequencies for the comparison and the error.  Each rank solves its own K
+tensor cores with FP64 refinement); the surrogate form without body blocks,
+the mixed form and the fp64 form with and without body blocks run on the
+same frequencies for the like-for-like comparison and the error.  Each rank solves its own K
 frequencies (weak scaling, no data-path collective); the timed region is the
 max over ranks of the device time between two events on the library's
 stream.  `e2e` repeats the main form through the C ABI from host buffers,
@@ -34,19 +35,15 @@ import numpy as np
 REPO = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(REPO, "hams-mrel_b200"))
 
+import hams_b200  # noqa: E402
 import meshgen  # noqa: E402
 
 METRIC = "freq-solves/s @5.4k panels: surrogate+mixed vs plain FP64 GPU @≤1e-4 rel err"
 UNIT = "freq-solves/s"
 RHO, G = 1025.0, 9.81
 LANES = 8  # frequencies in flight in hams_solve_batch (the library's default)
-SG_FAR = 3.0  # surrogate pairs: centre distance beyond 3 source-panel sizes
-# Frequencies the surrogate serves, by K = k0 h tanh(k0 h): on this array the
-# damping below 0.26 rad/s (K < 0.3) and the excitation above 2.05 rad/s
-# (K > 21.5, up to the first irregular frequency of the cylinders, 2.43 rad/s)
-# are small differences of large terms that amplify the network's error past
-# 1e-4; those frequencies keep the series.
-SG_K_RANGE = (0.3, 21.5)
+SG_FAR = hams_b200.SURROGATE_FAR  # surrogate pairs: centre distance beyond 3 source-panel sizes
+SG_K_RANGE = hams_b200.SURROGATE_K_RANGE
 
 
 def _peaks():
@@ -64,17 +61,15 @@ WORKLOAD = "3x3 cylinder array R=4 T=8 spacing 20 m, 5400 quad panels, depth 50 
 
 # FP64 operations per EIGENE panel pair of the series Green kernel, from the
 # executed-instruction counters of one ncu capture of that kernel on the
-# 3,240-panel profiling case: dadd + dmul + 2 dfma
-# (smsp__sass_thread_inst_executed_op_d*), and its DRAM bytes per pair
+# 3,240-panel profiling case (`--profile-case --form fp64`): dadd + dmul +
+# 2 dfma (smsp__sass_thread_inst_executed_op_d*), and its DRAM bytes per pair
 # (dram__bytes_read.sum + dram__bytes_write.sum over the launch's 4,093,706
-# pairs), scaled to a full launch by its pair count
-# (profiles/k_green_series_eigene_c2_array.md).
+# pairs), scaled to a full launch by its pair count.
 EIGENE_FP64_FLOPS_PER_PAIR = 44_410
 EIGENE_DRAM_BYTES_PER_PAIR = 2_381
 # DRAM bytes per pair of the surrogate kernel: ncu's dram__bytes_read.sum +
 # dram__bytes_write.sum on the 3,240-panel profiling case (642.0 MB for
-# 10,233,540 pairs), scaled to a full launch by its pair count
-# (profiles/k_green_sg_c2_array.md)
+# 10,233,540 pairs), scaled to a full launch by its pair count.
 SG_DRAM_BYTES_PER_PAIR = 62.73
 
 
@@ -163,84 +158,95 @@ class ClockSampler:
 
 
 # ------------------------------------------------------- CPU (oracle) timing
-def cpu_sample_time(case, xyz, ncn, ncon, cnt, xr, omega, target_s=8.0, threads=None):
-    """Seconds per frequency of the CPU implementation, from a bounded sample.
-
-    Assembly: the oracle's OpenMP row assembly (every `stride`-th hull row,
-    all host threads), scaled by n / rows.  LU and solve: LAPACK zgetrf /
-    zgetrs (the reference calls the same routines through MKL) on the
-    n x n system, or on a leading m x m block scaled by (n/m)^3 and (n/m)^2
-    when the full factorisation would take longer than a few seconds.
-    Force reductions (O(n * modes)) are left out; they are < 0.1 % of a step.
-    """
+def oracle_for_timing():
+    """The oracle, built for this host's cores (-O3 -march=native) in a
+    temporary directory, for the timed CPU legs; the portable build if that
+    fails.  Returns (module, build description)."""
+    if not os.environ.get("HAMS_ORACLE_SO"):
+        out = os.path.join(tempfile.mkdtemp(prefix="hams_oracle_"), "libhams_oracle_native.so")
+        r = subprocess.run(["make", "-s", "-C", os.path.join(REPO, "oracle"), "native", f"NATIVE_OUT={out}"],
+                           stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+        if r.returncode == 0 and os.path.exists(out):
+            os.environ["HAMS_ORACLE_SO"] = out
     sys.path.insert(0, os.path.join(REPO, "oracle"))
     import oracle_lib
+
+    native = bool(os.environ.get("HAMS_ORACLE_SO"))
+    return oracle_lib, ("gcc -O3 -march=native -fopenmp" if native else "gcc -O3 -fopenmp (portable build)")
+
+
+def cpu_frequency(oc, omega, betas, threads):
+    """One frequency solved on the host cores, every part of it run in full:
+    the oracle's OpenMP assembly of all rows of the system (the reference's
+    CALGREEN_MULTI, BODINT_MULTI_LEFT, ASSB_LEFT_MULTI, ASSB_RBC_MULTI and
+    ASSB_DBC_MULTI), LAPACK zgetrf / zgetrs on that assembled system (the
+    routines RADIATION_SOLVER_MULTI and DIFFRACTION_SOLVER_MULTI call through
+    MKL; OpenBLAS here) and the oracle's force reductions (RFORCE_MULTI,
+    EFORCE_MULTI).  Returns seconds and the split."""
     import scipy.linalg.lapack as lapack
 
-    threads = threads or len(os.sched_getaffinity(0))
-    oc = oracle_lib.Case(xyz, ncn, ncon, cnt, xr, case["depth"], rho=RHO, g=G)
     oc.opts.nthread = threads
-    n = oc.n
-    betas = np.radians(case["betas_deg"])
+    t0 = time.perf_counter()
     w = oc.wave(omega)
-    # calibrate the stride on a handful of rows, then time the sample
-    stride = max(1, n // max(threads, 8))
-    t = time.perf_counter()
-    oc.assemble_rows(w, betas, stride, 0)
-    t_probe = time.perf_counter() - t
-    rows_probe = (n + stride - 1) // stride
-    per_row = t_probe / rows_probe
-    want = max(rows_probe, min(n, int(0.6 * target_s / max(per_row, 1e-9))))
-    stride = max(1, n // want)
-    t = time.perf_counter()
-    a, _, _ = oc.assemble_rows(w, betas, stride, 1 % stride if stride > 1 else 0)
-    t_rows = time.perf_counter() - t
-    nr = a.shape[0]
-    t_asm = t_rows * n / nr
-    # LU + solve on a diagonally dominant complex matrix of the same size
-    rng = np.random.default_rng(0)
-    m = min(n, 1350)
-    while True:
-        mat = (rng.standard_normal((m, m)) + 1j * rng.standard_normal((m, m))).astype(np.complex128)
-        mat[np.diag_indices(m)] += 4.0 * np.sqrt(m)
-        rhs = np.asfortranarray(rng.standard_normal((m, 58)) + 0j)
-        mat = np.asfortranarray(mat)
-        t = time.perf_counter()
-        lu, piv, info = lapack.zgetrf(mat, overwrite_a=True)
-        lapack.zgetrs(lu, piv, rhs, overwrite_b=True)
-        t_lu = time.perf_counter() - t
-        if m == n or t_lu * (n / m) ** 3 > 0.4 * target_s:
-            break
-        m = n if (n / m) ** 3 * t_lu < 0.25 * target_s else min(n, 2 * m)
-    t_lin = t_lu * (n / m) ** 3
-    sample = f"oracle assembly of {nr}/{n} rows (stride {stride}) x {n / nr:.1f}; LAPACK zgetrf+zgetrs " \
-             f"(58 RHS) {m}x{m}" + (f" x (n/m)^3 = {(n / m) ** 3:.1f}" if m < n else "") + f"; omega={omega:.3f}"
-    return t_asm + t_lin, threads, sample, dict(assembly_s=t_asm, lu_s=t_lin)
+    a, b, d = oc.assemble(w, betas)
+    t1 = time.perf_counter()
+    n, nsys = oc.n, oc.geom.nsys
+    xr = np.zeros_like(b)
+    xd = np.zeros_like(d)
+    for ip in range(nsys):
+        lu, piv, info = lapack.zgetrf(a[:, :, ip], overwrite_a=True)
+        xr[:, :, ip] = lapack.zgetrs(lu, piv, b[:, :, ip])[0]
+        xd[:, ip, :] = lapack.zgetrs(lu, piv, d[:, ip, :])[0]
+    t2 = time.perf_counter()
+    oc.forces(w, betas, xr, xd)
+    t3 = time.perf_counter()
+    return t3 - t0, dict(assembly_s=t1 - t0, lu_s=t2 - t1, forces_s=t3 - t2)
+
+
+def cpu_case(case, xyz, ncn, ncon, cnt, xr):
+    orc, build = oracle_for_timing()
+    oc = orc.Case(xyz, ncn, ncon, cnt, xr, case["depth"], rho=RHO, g=G)
+    return oc, build
 
 
 def reference_arm(args):
-    """The CPU implementation of the path on the host cores (rank 0 only)."""
+    """The CPU implementation of the path on the host cores (rank 0 only):
+    whole frequencies, nothing scaled.  A step is one frequency of the
+    sweep; as many of the K steps run as fit --cpu-seconds (at least two),
+    and the line's `steps` is the number that ran."""
     ws, rank, _ = dist_env()
     if rank != 0:
         return
     case, xyz, ncn, ncon, cnt, xr = build_case()
+    oc, build = cpu_case(case, xyz, ncn, ncon, cnt, xr)
+    threads = len(os.sched_getaffinity(0))
+    betas = np.radians(case["betas_deg"])
     omegas = case["omegas"]
-    per = []
-    cores, sample = None, None
-    for s in range(args.warmup + args.steps):
-        om = omegas[s % len(omegas)]
-        sec, cores, sample, _ = cpu_sample_time(case, xyz, ncn, ncon, cnt, xr, om,
-                                                target_s=args.cpu_seconds or 3.0)
-        if s >= args.warmup:
-            per.append(sec)
+    budget = args.cpu_seconds or 120.0
+    per, parts, om_run = [], [], []
+    t_start = time.perf_counter()
+    for s in range(args.steps):
+        # the K steps spread over the sweep, as on the GPU
+        om = float(omegas[(s * len(omegas)) // max(args.steps, 1)])
+        sec, part = cpu_frequency(oc, om, betas, threads)
+        per.append(sec)
+        parts.append(part)
+        om_run.append(round(om, 4))
+        elapsed = time.perf_counter() - t_start
+        if len(per) >= 2 and elapsed + sec > budget:
+            break
     total = sum(per)
     value = len(per) / total
+    mean = {k: round(float(np.mean([p[k] for p in parts])), 3) for k in parts[0]}
+    sample = (f"{len(per)} whole frequencies ({', '.join(map(str, om_run))} rad/s) of the {len(omegas)}-frequency "
+              f"sweep, each fully assembled ({oc.n} x {oc.n}), factored and reduced; oracle {build}, "
+              f"LAPACK zgetrf/zgetrs (OpenBLAS); no warm-up (no compilation or caches to warm on the host)")
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / len(per),
+            "steps": len(per), "steps_requested": args.steps, "warmup": 0, "ms_per_step": 1e3 * total / len(per),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": WORKLOAD, "form": "cpu"},
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
-                             "sample": "per step: " + sample},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample,
+                             **mean},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -328,12 +334,18 @@ def e2e_form(hb, dev, case, xyz, ncn, ncon, cnt, xr, prec, omegas, betas, steps,
 # forms: precision, surrogate on, dtype, refinement target, identical body
 # blocks computed once.  The surrogate form's accuracy is set by the network
 # (~1e-5 in the outputs), so its refinement stops at a relative residual of
-# 1e-7; it also computes the Green functions of each of the 25 distinct
-# (field, source) body blocks of the array once (hams_opts.body_blocks).  The
-# plain forms compute every pair, as the reference does.
+# 1e-7; the mixed form refines to 1e-12.  Body blocks (the Green functions of
+# each of the 25 distinct (field, source) body blocks of the array computed
+# once, hams_opts.body_blocks) are an exact geometric reuse that any form can
+# use, so the surrogate and fp64 forms run both with and without them and the
+# speed-ups are reported like for like.
 FORMS = {"surrogate": ("mixed", True, "f64 near + f16/f32 MLP far, c64 LU + f64 refinement", 1e-7, 1),
+         "surrogate_noblocks": ("mixed", True, "f64 near + f16/f32 MLP far, c64 LU + f64 refinement", 1e-7, 0),
          "mixed": ("mixed", False, "f64, c64 LU + f64 refinement", 1e-12, 0),
-         "fp64": ("fp64", False, "f64", 0.0, 0)}
+         "fp64": ("fp64", False, "f64", 0.0, 0),
+         "fp64_blocks": ("fp64", False, "f64", 0.0, 1)}
+# the plain drop-in each form is compared with, like for like (body blocks on or off)
+PLAIN_OF = {"surrogate": "fp64_blocks", "surrogate_noblocks": "fp64", "mixed": "fp64", "fp64_blocks": "fp64"}
 
 
 def gpu_arm(args):
@@ -398,15 +410,16 @@ def gpu_arm(args):
     forms = {}
     for name, r in runs.items():
         v = ws * args.steps / (max_over_ranks(r["ms"]) * 1e-3)
-        err = None
+        pr, on, _, tol, blocks = FORMS[name]
+        forms[name] = {"value": v, "precision": pr, "surrogate": on, "body_blocks": bool(blocks),
+                       "refine_tol": tol if pr == "mixed" else None, "rel_err_vs_fp64": None}
         if "fp64" in runs and name != "fp64":
-            e = [max(rel(a[0], b[0]), rel(a[1], b[1]), rel(a[2], b[2])) for a, b in
-                 zip(r["results"], runs["fp64"]["results"])]
-            err = max_over_ranks(max(e))
-            med = float(np.median(e))
-        forms[name] = {"value": v, "rel_err_vs_fp64": err}
-        if err is not None:
-            forms[name]["rel_err_median"] = med
+            # worst of the relative Frobenius errors of added mass, damping and excitation against the
+            # plain fp64 form (every pair computed), per frequency
+            e = [[rel(a[k], b[k]) for k in range(3)] for a, b in zip(r["results"], runs["fp64"]["results"])]
+            worst = [max(x) for x in e]
+            forms[name].update(rel_err_vs_fp64=max_over_ranks(max(worst)), rel_err_median=float(np.median(worst)),
+                               rel_err_amas_bdmp_exfc=[max_over_ranks(max(x[k] for x in e)) for k in range(3)])
 
     value = ws * args.steps / (ms * 1e-3)
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
@@ -431,7 +444,14 @@ def gpu_arm(args):
                     "parts_rank0": {k: round(v, 4) for k, v in e2e_parts.items()}},
             "forms": forms}
     if "fp64" in forms and args.form != "fp64":
-        line["speedup_vs_fp64"] = value / forms["fp64"]["value"]
+        sp = {}
+        for name, plain in (("surrogate", "fp64_blocks"), ("surrogate_noblocks", "fp64")):
+            if name in forms and plain in forms:
+                sp[f"{name}_vs_{plain}"] = forms[name]["value"] / forms[plain]["value"]
+        sp["headline_form_vs_plain_fp64"] = value / forms["fp64"]["value"]
+        sp["note"] = ("like for like: body blocks on against on, off against off; the blocks-off ratio is the "
+                      "speed-up of the network and the tensor-core solve alone")
+        line["speedup_vs_fp64"] = sp
         line["rel_err_vs_fp64"] = forms[args.form]["rel_err_vs_fp64"]
     tm = main["timings"]
     if sg_main is not None:
@@ -464,9 +484,15 @@ def gpu_arm(args):
             roof.update(achieved=ach, frac=ach / peak, flops_per_pair=EIGENE_FP64_FLOPS_PER_PAIR)
         line["roofline"] = roof
     if rank == 0 and ws == 1 and not args.no_cpu:
-        sec, cores, sample, parts = cpu_sample_time(case, xyz, ncn, ncon, cnt, xr, float(allom[len(allom) // 2]),
-                                                    target_s=args.cpu_seconds or 8.0)
-        line["cpu_baseline"] = {"value": 1.0 / sec, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample,
+        # one whole frequency of the same workload on the host cores (about 15 s), nothing scaled
+        oc, build = cpu_case(case, xyz, ncn, ncon, cnt, xr)
+        cores = len(os.sched_getaffinity(0))
+        om = float(allom[len(allom) // 2])
+        sec, parts = cpu_frequency(oc, om, betas, cores)
+        line["cpu_baseline"] = {"value": 1.0 / sec, "unit": UNIT, "cores": cores, "kind": "port",
+                                "sample": f"one whole frequency (omega = {om:.3f} rad/s, {oc.n} x {oc.n} system "
+                                          f"fully assembled, factored and reduced); oracle {build}, LAPACK "
+                                          f"zgetrf/zgetrs (OpenBLAS)",
                                 **{k: round(v, 3) for k, v in parts.items()}}
     if rank == 0:
         print(json.dumps(line), flush=True)
@@ -484,7 +510,7 @@ def main():
     ap.add_argument("--form", choices=list(FORMS), default="surrogate")
     ap.add_argument("--only-form", action="store_true", help="time only --form (no fp64 / other forms beside it)")
     ap.add_argument("--cpu-seconds", type=float, default=None,
-                    help="CPU work per baseline sample (default 8 s; 3 s per step of --impl reference)")
+                    help="time budget of --impl reference (default 120 s; at least two whole frequencies run)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--profile-case", action="store_true",
                     help="the coarser 3,240-panel array, for profiler captures (not a bench line)")

@@ -359,6 +359,10 @@ std::string fmt_e(int w, int dg, double v) {
     std::snprintf(out, sizeof(out), "%*s", w, z.c_str());
     return out;
   }
+  if (std::isnan(v) || std::isinf(v)) {  // the Fortran runtime's spelling, right-aligned
+    std::snprintf(out, sizeof(out), "%*s", w, std::isnan(v) ? "NaN" : (v < 0.0 ? "-Infinity" : "Infinity"));
+    return out;
+  }
   char m[64];
   std::snprintf(m, sizeof(m), "%.*e", dg - 1, std::fabs(v));
   int e = std::atoi(std::strchr(m, 'e') + 1) + 1;
@@ -376,6 +380,10 @@ std::string fmt_e(int w, int dg, double v) {
 // Fortran ESw.d (one digit before the point, two-digit exponent).
 std::string fmt_es(int w, int dg, double v) {
   char out[64];
+  if (std::isnan(v) || std::isinf(v)) {
+    std::snprintf(out, sizeof(out), "%*s", w, std::isnan(v) ? "NaN" : (v < 0.0 ? "-Infinity" : "Infinity"));
+    return out;
+  }
   std::snprintf(out, sizeof(out), "%*.*E", w, dg, v);
   return out;
 }

@@ -1822,14 +1822,17 @@ extern "C" int hams_eval_green(hams_ctx* c, const hams_wave* w, int32_t npts, co
 // ---------------------------------------------------------------------------
 // hams_eval_green_static: hams_eval_green without device allocation.  Its
 // staging lives in one fixed reservation per device: the results (4 complex
-// per point), the points (6 doubles), the flags and the overflow word.
+// per point), the points (6 doubles), the flags, the overflow word and the
+// frequency's wave numbers (so that the call touches none of the context's
+// per-frequency buffers, which a solve on another stream may be using).
 // ---------------------------------------------------------------------------
 constexpr size_t kStaticPts = HAMS_EVAL_STATIC_MAX_POINTS;
 constexpr size_t kStaticOutOff = 0;                                   // double2 (4 * kStaticPts)
 constexpr size_t kStaticPtsOff = kStaticOutOff + 4 * kStaticPts * 16;  // double (6 * kStaticPts)
 constexpr size_t kStaticFlagOff = kStaticPtsOff + 6 * kStaticPts * 8;  // int (kStaticPts)
 constexpr size_t kStaticOvfOff = kStaticFlagOff + kStaticPts * 4;      // int
-constexpr size_t kStaticBytes = (kStaticOvfOff + 4 + 255) / 256 * 256;
+constexpr size_t kStaticWvnOff = (kStaticOvfOff + 4 + 7) / 8 * 8;      // double (HAMS_NK)
+constexpr size_t kStaticBytes = (kStaticWvnOff + HAMS_NK * 8 + 255) / 256 * 256;
 static __device__ __align__(256) unsigned char g_eval_static[kStaticBytes];
 
 constexpr int kStaticMaxDevices = 64;
@@ -1865,12 +1868,13 @@ extern "C" int hams_eval_green_static(hams_ctx* c, const hams_wave* w, int32_t n
   double* dp = (double*)(base + kStaticPtsOff);
   int* df = (int*)(base + kStaticFlagOff);
   int* dovf = (int*)(base + kStaticOvfOff);
+  double* dwvn = (double*)(base + kStaticWvnOff);
   CU(cudaMemcpyAsync(dp, pts, 6 * (size_t)npts * 8, cudaMemcpyHostToDevice, c->st));
   CU(cudaMemcpyAsync(df, flag, (size_t)npts * 4, cudaMemcpyHostToDevice, c->st));
   WaveDev wd = wave_dev(c, w);
-  if (c->opts.depth >= 0.0 && !wd.limit) CU(cudaMemcpyAsync(c->wvn.p, w->wvn, HAMS_NK * 8, cudaMemcpyHostToDevice, c->st));
+  if (c->opts.depth >= 0.0 && !wd.limit) CU(cudaMemcpyAsync(dwvn, w->wvn, HAMS_NK * 8, cudaMemcpyHostToDevice, c->st));
   CU(cudaMemsetAsync(dovf, 0, sizeof(int), c->st));  // the overflow word must start at zero
-  launch_eval_green((npts + 127) / 128, c->st, npts, dp, df, wd, c->wvn.p, dout, dovf);
+  launch_eval_green((npts + 127) / 128, c->st, npts, dp, df, wd, dwvn, dout, dovf);
   TRY(launch_check(c));
   CU(cudaMemcpyAsync(grn, dout, 4 * (size_t)npts * 16, cudaMemcpyDeviceToHost, c->st));
   int ovf = 0;

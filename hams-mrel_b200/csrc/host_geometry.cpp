@@ -193,7 +193,9 @@ std::vector<int> body_block_reps(const hams_geom* g, double tol) {
     for (int b1 = 0; b1 < nb; ++b1) {
       const int k = b1 + nb * b2;
       const double ox = s[b2].dx - s[b1].dx, oy = s[b2].dy - s[b1].dy;
-      const long long qx = std::llround(ox / eps), qy = std::llround(oy / eps);
+      // floor keeps two offsets within eps of each other at most one cell apart
+      // (rounding to nearest would put +-eps/2 two cells apart)
+      const long long qx = (long long)std::floor(ox / eps), qy = (long long)std::floor(oy / eps);
       int best = k;
       for (long long ex = -1; ex <= 1; ++ex)
         for (long long ey = -1; ey <= 1; ++ey) {

@@ -218,7 +218,11 @@ int hams_eval_green(hams_ctx *ctx, const hams_wave *wave, int32_t npts, const do
  * device share the reservation: each call waits for its own stream before it
  * returns, so calls one after another are safe, but calls that overlap in
  * time on one device (from several host threads) race and must be
- * serialised by the caller.  Same arguments and results as hams_eval_green. */
+ * serialised by the caller.  The call reads the context's geometry only (the
+ * wave numbers are staged in the reservation too), but it enqueues on the
+ * context's stream and counts its launch there: pass a context that is not
+ * solving during the call (solves may run on other contexts of the device).
+ * Same arguments and results as hams_eval_green. */
 #define HAMS_EVAL_STATIC_MAX_POINTS 4096
 int hams_eval_green_static(hams_ctx *ctx, const hams_wave *wave, int32_t npts, const double *pts,
                            const int32_t *flag, double *grn);

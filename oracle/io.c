@@ -434,6 +434,10 @@ static void fmt_e(char *out, int w, int dg, double v)
         snprintf(out, 64, "%*s", w, z);
         return;
     }
+    if (isnan(v) || isinf(v)) { /* the Fortran runtime's spelling, right-aligned */
+        snprintf(out, 64, "%*s", w, isnan(v) ? "NaN" : (v < 0.0 ? "-Infinity" : "Infinity"));
+        return;
+    }
     snprintf(m, sizeof(m), "%.*e", dg - 1, fabs(v));
     e = atoi(strchr(m, 'e') + 1) + 1;
     k = 0;

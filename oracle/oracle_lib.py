@@ -54,12 +54,15 @@ _LIB = None
 
 
 def load():
+    """The oracle library: ``oracle/libhams_oracle.so``, or the build named by
+    HAMS_ORACLE_SO (the host-tuned build the timed CPU baseline uses)."""
     global _LIB
     if _LIB is not None:
         return _LIB
-    if not os.path.exists(ORACLE_SO):
+    path = os.environ.get("HAMS_ORACLE_SO") or ORACLE_SO
+    if path == ORACLE_SO and not os.path.exists(ORACLE_SO):
         build()
-    lib = ctypes.CDLL(ORACLE_SO)
+    lib = ctypes.CDLL(path)
     lib.orc_wave_props.argtypes = [c_int, c_dbl, c_dbl, c_dbl, c_int, ctypes.POINTER(OrcWave)]
     lib.orc_dispersion_c.argtypes = [P_dbl, c_int, c_dbl, c_dbl]
     lib.orc_fingreen3d_c.argtypes = [c_dbl] * 7 + [P_dbl, c_int, c_dbl, P_dbl, c_int]

@@ -199,3 +199,26 @@ def test_driver_symmetric_half_mesh_deck(tmp_path, axis):
             ohead, orc = _load(tmp_path / "cpu" / f"{kind}{m}.txt")
             assert head == ohead
             assert np.linalg.norm(got - orc) <= 1e-7 * np.linalg.norm(orc) + 1e-12, f"{kind}{m}"
+
+
+@pytest.mark.gpu
+def test_driver_zero_and_infinite_frequency_limits(tmp_path):
+    """examples/example1_multi_bodies (5 x 727 panels, h = 0.9 m, 0_inf_frequency_limits = 1) cut to
+    its first regular frequency: the zero- and infinite-frequency records of OAMASS/ODAMPING/OEXFOR
+    as the reference prints them (added mass within 1e-6, damping zero at both limits, excitation
+    zero at the zero limit and NaN at the infinite one, where the reference's incident-wave terms
+    divide infinities, PatclVelct.f90:90-110), and the regular frequency within the oracle's
+    tolerances of the same deck."""
+    from test_oracle_golden import compare_limit_files, cut_deck
+
+    deck = cut_deck(os.path.join(GOLDEN, "example1", "input"), str(tmp_path / "in"), 1)
+    r = subprocess.run([RUN, deck, str(tmp_path / "gpu")], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    got = str(tmp_path / "gpu" / "Hams_format")
+    exp = os.path.join(GOLDEN, "example1", "expected")
+    compare_limit_files(got, exp, 1e-4, 1e-2, 1e-4)
+    for m in range(1, 7):  # the two limit records (25 body pairs each) of added mass
+        head, g = _load(os.path.join(got, f"OAMASS{m}.txt"))
+        rhead, ref = _load(os.path.join(exp, f"OAMASS{m}.txt"))
+        assert head[:50] == rhead[:50]
+        assert np.linalg.norm(g[:50] - ref[:50]) / np.linalg.norm(ref[:50]) < 1e-6

@@ -103,3 +103,74 @@ def test_deck_loader_lid_and_single_body(oracle):
     assert list(d["body_nelem"]) == [234]
     assert np.allclose(d["ixyz_p"][:, 2], 0.0)
     assert d["nbeta"] == 36 and d["nper"] == 10
+
+
+def cut_deck(src, dst, nfreq):
+    """Copy the deck in src to dst with its frequency list cut to the first
+    nfreq frequencies (the zero- and infinite-frequency limits, when the deck
+    asks for them, come on top)."""
+    import re
+    import shutil
+
+    os.makedirs(dst, exist_ok=True)
+    for f in os.listdir(src):
+        shutil.copyfile(os.path.join(src, f), os.path.join(dst, f))
+    ctl = os.path.join(dst, "ControlFile.in")
+    text = open(ctl).read()
+    text, k = re.subn(r"(Number_of_frequencies\s+)(-?)\d+", lambda m: f"{m.group(1)}{m.group(2)}{nfreq}", text, 1)
+    assert k == 1
+    open(ctl, "w").write(text)
+    return dst
+
+
+def compare_limit_files(got_dir, exp_dir, tol_a, tol_b, tol_x):
+    """Per frequency record of the OAMASS/ODAMPING/OEXFOR files: the heads
+    print identically, NaN where the reference printed NaN, exact zeros where
+    it printed zeros (damping and excitation at the zero-frequency limit,
+    damping at the infinite-frequency limit), and the relative Frobenius
+    error of every other record within the tolerance.  Returns the worst
+    error per kind."""
+    worst = {}
+    for kind, tol in (("OAMASS", tol_a), ("ODAMPING", tol_b), ("OEXFOR", tol_x)):
+        worst[kind] = 0.0
+        for m in range(1, 7):
+            ref = _load(os.path.join(exp_dir, f"{kind}{m}.txt"))
+            got = _load(os.path.join(got_dir, f"{kind}{m}.txt"))[:len(ref)]
+            assert [r[:2] for r in got] == [r[:2] for r in ref]
+            r = np.array([[float(x) for x in row[2:]] for row in ref])
+            g = np.array([[float(x) for x in row[2:]] for row in got])
+            assert np.array_equal(np.isnan(r), np.isnan(g)), f"{kind}{m}: NaN entries differ"
+            heads = [tuple(row[:2]) for row in ref]
+            for key in dict.fromkeys(heads):
+                idx = [i for i, h in enumerate(heads) if h == key]
+                rr, gg = r[idx], g[idx]
+                if np.isnan(rr).any():
+                    continue
+                nr = np.linalg.norm(rr)
+                if nr == 0.0:
+                    assert np.all(gg == 0.0), f"{kind}{m} at {key}: nonzero where the reference prints zero"
+                    continue
+                e = np.linalg.norm(gg - rr) / nr
+                worst[kind] = max(worst[kind], e)
+                assert e < tol, f"{kind}{m} at {key}: relative Frobenius {e:.3e} >= {tol}"
+    return worst
+
+
+def test_oracle_zero_and_infinite_frequency_limits(tmp_path, oracle):
+    """examples/example1_multi_bodies (5 bodies x 727 panels, h = 0.9 m, 0_inf_frequency_limits = 1):
+    the zero- and infinite-frequency added mass prints as the reference's (observed: identically),
+    damping is zero at both limits and excitation zero at the zero limit and NaN at the infinite one,
+    as the reference prints them (its incident-wave terms divide infinities there,
+    PatclVelct.f90:90-110); the first regular frequency (0.2 rad/s) within the tolerances of the
+    other decks (observed A 3.9e-5, B 3.8e-3 for the small roll damping, X 1.2e-5)."""
+    deck = cut_deck(os.path.join(GOLDEN, "example1", "input"), str(tmp_path / "in"), 1)
+    out = tmp_path / "out"
+    out.mkdir()
+    rc = oracle.orc_run_case(deck.encode(), str(out).encode(), 8, os.cpu_count() or 1)
+    assert rc == 0
+    worst = compare_limit_files(str(out), os.path.join(GOLDEN, "example1", "expected"), 1e-4, 1e-2, 1e-4)
+    print("example1", worst)
+    # the limit records print identically
+    for kind in ("OAMASS", "ODAMPING"):
+        ref = _load(os.path.join(GOLDEN, "example1", "expected", f"{kind}1.txt"))[:50]
+        assert _load(out / f"{kind}1.txt")[:50] == ref

@@ -98,3 +98,25 @@ def test_static_rejects_more_points_than_reserved():
     assert rc == 0, msg
     assert rel(got, ctx.eval_green(w, pts, flag)) <= TOL
     ctx.close()
+
+
+def test_static_allocates_no_device_memory():
+    """The property the entry point exists for: after a first call on the device (which looks the
+    reservation up), further calls leave the device's free memory exactly as it was."""
+    import torch
+
+    ctx = context(30.0)
+    w = hams_b200.wave_properties(0.9, 30.0, 9.81)
+    pts, flag = points(MAX_POINTS, 30.0, seed=7)
+    rc, first, msg = eval_static(ctx, w, pts, flag)
+    assert rc == 0, msg
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info(0)
+    for k in range(5):
+        rc, got, msg = eval_static(ctx, w, pts, flag)
+        assert rc == 0, msg
+        assert np.array_equal(got, first)
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info(0)
+    assert free1 == free0, f"free device memory changed by {free0 - free1} bytes"
+    ctx.close()
