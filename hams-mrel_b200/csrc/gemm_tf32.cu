@@ -1,0 +1,265 @@
+// gemm_tf32.cu -- C = alpha A B + beta C on the fifth-generation tensor cores.
+//
+// One CTA computes a 128 x 128 tile of C.  Warp 0 streams the K panels of A
+// and B into a three-stage shared-memory ring with the tensor memory
+// accelerator (cp.async.bulk.tensor, 128-byte swizzle, no multicast: every
+// operand is this GPU's own memory); warp 1 owns the tile's 128 tensor-memory
+// columns and issues tcgen05.mma kind::tf32 (M = 128, N = 128, K = 8) from
+// one thread, four per 32-wide K panel, releasing each stage with
+// tcgen05.commit; warps 2-5 read the FP32 accumulator back with tcgen05.ld
+// (thread = row of the tile) and write alpha acc + beta C.  With 97 KB of
+// shared memory and 128 tensor-memory columns, two CTAs share an SM, so one
+// CTA's epilogue runs under the other's main loop.
+//
+// Out-of-range rows and columns of A and B (ragged M, N, K) are zero-filled
+// by the copies; the epilogue writes only the rows and columns inside C.
+//
+// Every wait on a pipeline barrier is bounded.  A wait that gives up sets
+// bit 0 of the error word and a shared abort flag; the other roles stop at
+// their next wait, the copies already issued are waited for (bounded), the
+// issued MMAs are waited for, and the CTA frees its tensor memory before it
+// returns.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <mutex>
+
+#include "gemm_tf32.h"
+
+namespace {
+
+constexpr int kBM = 128, kBN = 128, kBK = 32;  // tile rows, columns, K panel (32 floats = one 128-byte row)
+constexpr int kStages = 3;
+constexpr int kThreads = 192;
+constexpr int kABytes = kBM * kBK * 4;  // 16 KB per stage
+constexpr int kBBytes = kBN * kBK * 4;  // 16 KB per stage
+constexpr int kOffB = kStages * kABytes;
+constexpr int kOffBar = kOffB + kStages * kBBytes;  // full[kStages], empty[kStages], acc
+constexpr int kOffMisc = kOffBar + 8 * (2 * kStages + 1);
+constexpr int kSmemBytes = kOffMisc + 16 + 1024;  // + alignment slack of the dynamic window
+constexpr long long kSpin = 1ll << 22;
+
+// instruction descriptor, kind::tf32: D f32 (bit 4), A and B tf32 (format 2
+// at bits 7 and 10), both K-major, N >> 3 at bit 17, M >> 4 at bit 24
+constexpr uint32_t kIdesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(kBN >> 3) << 17) |
+                            ((uint32_t)(kBM >> 4) << 24);
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// shared-memory descriptor of a K-major operand tile written by the copy
+// engine with 128-byte swizzle: rows of 128 bytes, 8-row groups 1024 bytes
+// apart (stride byte offset), version 1, layout SWIZZLE_128B
+__device__ __forceinline__ uint64_t sdesc_sw128(uint32_t saddr) {
+  return (uint64_t)((saddr >> 4) & 0x3FFFu) | (1ull << 16) | ((uint64_t)(1024 >> 4) << 32) | (1ull << 46) |
+         (2ull << 61);
+}
+
+__device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
+  uint32_t done;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}\n"
+      : "=r"(done)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return done != 0;
+}
+
+// bounded wait; false if it gave up or another role aborted the tile
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int* abort_flag) {
+  for (long long it = 0; it < kSpin; ++it) {
+    if (mbar_try(bar, parity)) return true;
+    if ((it & 1023) == 1023 && *abort_flag) return false;
+  }
+  return false;
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&v)[16]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+      "%15}, [%16];"
+      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+        "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+      : "r"(taddr));
+}
+
+__global__ void __launch_bounds__(kThreads, 2)
+    k_gemm_tf32(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, float* __restrict__ C,
+                int ldc, int M, int N, int K, float alpha, float beta, int c_rowmajor, int* err) {
+  extern __shared__ unsigned char smem_raw[];
+  unsigned char* smem = smem_raw + ((1024 - (smem_u32(smem_raw) & 1023)) & 1023);  // 1024-aligned window
+  const uint32_t sbase = smem_u32(smem);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + kOffBar);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(smem + kOffMisc);
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(smem + kOffMisc + 4);
+  const uint32_t bar_full = smem_u32(&bars[0]), bar_empty = smem_u32(&bars[kStages]),
+                 bar_acc = smem_u32(&bars[2 * kStages]);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int m0 = blockIdx.x * kBM, n0 = blockIdx.y * kBN;
+  const int nk = (K + kBK - 1) / kBK;
+
+  if (tid == 0) {
+    *abort_flag = 0;
+    for (int s = 0; s < 2 * kStages + 1; ++s)
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&bars[s])));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tmA)) : "memory");
+    asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tmB)) : "memory");
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)), "r"(kBN));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tbase = *reinterpret_cast<volatile uint32_t*>(tslot);
+
+  if (warp == 0) {
+    if (lane == 0) {  // producer
+      int issued = 0;
+      for (int kb = 0; kb < nk; ++kb) {
+        const int s = kb % kStages;
+        if (kb >= kStages && !mbar_wait(bar_empty + 8 * s, (uint32_t)((kb / kStages - 1) & 1), abort_flag)) {
+          atomicOr(err, 1);
+          *abort_flag = 1;
+          break;
+        }
+        const uint32_t fb = bar_full + 8 * s;
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(fb), "r"(kABytes + kBBytes)
+                     : "memory");
+        asm volatile(
+            "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::
+                "r"(sbase + s * kABytes),
+            "l"(reinterpret_cast<uint64_t>(&tmA)), "r"(kb * kBK), "r"(m0), "r"(fb)
+            : "memory");
+        asm volatile(
+            "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::
+                "r"(sbase + kOffB + s * kBBytes),
+            "l"(reinterpret_cast<uint64_t>(&tmB)), "r"(kb * kBK), "r"(n0), "r"(fb)
+            : "memory");
+        issued = kb + 1;
+      }
+      // the copies in flight land before the CTA leaves (bounded)
+      for (int kb = issued > kStages ? issued - kStages : 0; kb < issued; ++kb) {
+        const int s = kb % kStages;
+        for (long long it = 0; it < kSpin && !mbar_try(bar_full + 8 * s, (uint32_t)((kb / kStages) & 1)); ++it) {
+        }
+      }
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {  // MMA issue
+      for (int kb = 0; kb < nk; ++kb) {
+        const int s = kb % kStages;
+        if (!mbar_wait(bar_full + 8 * s, (uint32_t)((kb / kStages) & 1), abort_flag)) {
+          atomicOr(err, 1);
+          *abort_flag = 1;
+          break;
+        }
+        tc_fence_after();
+        const uint64_t da = sdesc_sw128(sbase + s * kABytes), db = sdesc_sw128(sbase + kOffB + s * kBBytes);
+#pragma unroll
+        for (int kk = 0; kk < kBK / 8; ++kk) {  // K = 8 tf32 = 32 bytes along the swizzled row
+          const uint32_t acc = (kb | kk) != 0;
+          asm volatile(
+              "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+              "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tbase),
+              "l"(da + (uint64_t)(2 * kk)), "l"(db + (uint64_t)(2 * kk)), "r"(kIdesc), "r"(acc));
+        }
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                         bar_empty + 8 * s)
+                     : "memory");
+      }
+      // completion of every MMA issued (also on abort, so that tensor memory is idle before it is freed)
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar_acc)
+                   : "memory");
+      for (long long it = 0; it < kSpin && !mbar_try(bar_acc, 0); ++it) {
+      }
+    }
+  } else {  // epilogue: warps 2-5, warp w reads tensor-memory lanes 32 (w % 4) ...
+    const int q = warp & 3, row = m0 + 32 * q + lane;
+    bool ok = mbar_wait(bar_acc, 0, abort_flag);
+    if (!ok) {
+      atomicOr(err, 1);
+      *abort_flag = 1;
+    }
+    ok = __all_sync(0xffffffffu, ok && !*abort_flag);  // the tensor-memory loads below are warp-wide
+    tc_fence_after();
+    if (ok) {
+      const uint32_t trow = tbase + ((uint32_t)(32 * q) << 16);
+#pragma unroll 1
+      for (int c0 = 0; c0 < kBN; c0 += 16) {
+        uint32_t v[16];
+        tmem_ld16(trow + (uint32_t)c0, v);
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        if (row < M) {
+#pragma unroll
+          for (int j = 0; j < 16; ++j) {
+            const int col = n0 + c0 + j;
+            if (col < N) {
+              float* dst = c_rowmajor ? C + (size_t)row * ldc + col : C + (size_t)col * ldc + row;
+              const float a = __uint_as_float(v[j]);
+              *dst = beta == 0.0f ? alpha * a : fmaf(alpha, a, beta * *dst);
+            }
+          }
+        }
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 1) {
+    __syncwarp();
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tbase), "r"(kBN));
+  }
+}
+
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  });
+  return fn;
+}
+
+// 2-D map of a K-major operand: inner extent k floats, `rows` rows ld floats
+// apart, box of 32 floats x box_rows rows, 128-byte swizzle, zero fill
+bool make_map(CUtensorMap* tm, const float* base, int k, int rows, int ld, int box_rows) {
+  auto fn = encode_fn();
+  if (!fn) return false;
+  cuuint64_t dims[2] = {(cuuint64_t)k, (cuuint64_t)rows};
+  cuuint64_t strides[1] = {(cuuint64_t)ld * 4};
+  cuuint32_t box[2] = {(cuuint32_t)kBK, (cuuint32_t)box_rows};
+  cuuint32_t estr[2] = {1, 1};
+  return fn(tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(base), dims, strides, box, estr,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+}  // namespace
+
+int gemm_tf32(cudaStream_t st, int m, int n, int k, float alpha, const float* A, int lda, const float* B, int ldb,
+              float beta, float* C, int ldc, bool c_rowmajor, int* err) {
+  if (m <= 0 || n <= 0) return 0;
+  if (k <= 0 || (reinterpret_cast<uintptr_t>(A) & 15) || (reinterpret_cast<uintptr_t>(B) & 15) || (lda & 3) ||
+      (ldb & 3) || lda < k || ldb < k)
+    return 1;
+  if (cudaFuncSetAttribute(k_gemm_tf32, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes) != cudaSuccess)
+    return 1;
+  CUtensorMap ta, tb;
+  if (!make_map(&ta, A, k, m, lda, kBM) || !make_map(&tb, B, k, n, ldb, kBN)) return 1;
+  dim3 grid((unsigned)((m + kBM - 1) / kBM), (unsigned)((n + kBN - 1) / kBN));
+  k_gemm_tf32<<<grid, kThreads, kSmemBytes, st>>>(ta, tb, C, ldc, m, n, k, alpha, beta, c_rowmajor ? 1 : 0, err);
+  return cudaGetLastError() == cudaSuccess ? 0 : 1;
+}

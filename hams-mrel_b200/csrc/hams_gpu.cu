@@ -85,6 +85,7 @@ static int fail(int code, const char* fmt, ...) {
 
 #include "kernels.cuh"
 #include "lu_mixed.h"
+#include "gemm_tf32.h"
 #include "green_sg.h"
 #include "hmatrix.h"
 #include "surrogate.h"
@@ -466,6 +467,12 @@ __global__ void k_forces(DevGeom g, WaveDev w, IncWave q, const double* __restri
 __global__ void k_z2c(const double2* __restrict__ a, float2* __restrict__ b, size_t n) {
   size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   for (; t < n; t += (size_t)gridDim.x * blockDim.x) b[t] = make_float2((float)a[t].x, (float)a[t].y);
+}
+// b (ld ldb) <- the n x n complex128 matrix a (ld n) rounded to complex64
+__global__ void k_z2c_ld(const double2* __restrict__ a, float2* __restrict__ b, int n, int ldb) {
+  const size_t tot = (size_t)n * n;
+  for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < tot; t += (size_t)gridDim.x * blockDim.x)
+    b[(t / n) * ldb + t % n] = make_float2((float)a[t].x, (float)a[t].y);
 }
 __global__ void k_c2z_add(const float2* __restrict__ a, double2* __restrict__ b, size_t n) {
   size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -875,7 +882,7 @@ static int ctx_frequency_buffers(hams_ctx* c) {
   TRY(c->wvn.alloc(HAMS_NK));
   TRY(c->ovf.alloc(1));
   TRY(c->ipiv.alloc(n));
-  TRY(c->info.alloc(1));
+  TRY(c->info.alloc(2));  // the solver's info word and the tensor-core kernels' error word
   return 0;
 }
 
@@ -1183,39 +1190,42 @@ static int assemble_dev(hams_ctx* c, const hams_wave* w, int nbeta) {
 // refine_tol of that column's scale.  Returns HAMS_ERR_NUMERIC when the
 // factorisation breaks down or the refinement stalls.
 static int mixed_solve(hams_ctx* c, double2* M, const double2* rhs, int ldr, int nrhs, int kind, int* info_host) {
-  const int n = c->n;
+  const int n = c->n, lda = mixed_lu_ld(n);
   const cuDoubleComplex one = make_cuDoubleComplex(1.0, 0.0), mone = make_cuDoubleComplex(-1.0, 0.0);
-  size_t nn = (size_t)n * n, nx = (size_t)n * nrhs;
-  TRY(c->Af.alloc(nn));
+  const size_t nx = (size_t)n * nrhs;
+  TRY(c->Af.alloc((size_t)lda * n));
   TRY(c->Xf.alloc(nx));
   TRY(c->R.alloc(nx));
   TRY(c->colratio.alloc(nrhs));
   CU(cudaMemcpy2DAsync(c->X.p, (size_t)n * 16, rhs, (size_t)ldr * 16, (size_t)n * 16, nrhs, cudaMemcpyDeviceToDevice, c->st));
-  k_z2c<<<1184, 256, 0, c->st>>>(M, c->Af.p, nn);
+  k_z2c_ld<<<1184, 256, 0, c->st>>>(M, c->Af.p, n, lda);
   TRY(launch_check(c));
   const bool block = kind != HAMS_LU_LIBRARY;
   c->lu_used = kind;
   if (block) {
-    TRY(c->luw.alloc(mixed_lu_workspace_elems(n) + nx));
+    TRY(c->luw.alloc(mixed_lu_workspace_elems(n, nrhs)));
     TRY(c->perm.alloc(n));
     long long la = 0, lb = 0;
-    cublasComputeType_t ct = kind == HAMS_LU_BLOCK_TF32 ? CUBLAS_COMPUTE_32F_FAST_TF32 : CUBLAS_COMPUTE_32F_EMULATED_16BFX9;
-    int rc = mixed_lu_factor(c->st, c->blas, ct, n, c->Af.p, c->perm.p, c->luw.p, c->info.p, &la, &lb);
+    // TF32: the library's tcgen05 GEMM; the FP32 emulation on BF16 tensor cores is cuBLAS's
+    const bool own = kind == HAMS_LU_BLOCK_TF32;
+    int rc = mixed_lu_factor(c->st, c->blas, own, CUBLAS_COMPUTE_32F_EMULATED_16BFX9, n, lda, c->Af.p, c->perm.p,
+                             c->luw.p, c->info.p, &la, &lb);
     c->launches += la;
     c->lib_calls += lb;
     if (rc == 1) return fail(HAMS_ERR_NUMERIC, "block LU: CUDA failed");
     if (rc) return fail(HAMS_ERR_NUMERIC, "block LU: cuBLAS status %d in GEMM %d of block %d", rc % 100, rc % 1000 / 100,
                         rc / 1000);
-    int zp = 0;
-    CU(cudaMemcpyAsync(&zp, c->info.p, sizeof(int), cudaMemcpyDeviceToHost, c->st));
+    int word[2] = {0, 0};
+    CU(cudaMemcpyAsync(word, c->info.p, 2 * sizeof(int), cudaMemcpyDeviceToHost, c->st));
     CU(cudaStreamSynchronize(c->st));
-    if (zp <= n) return fail(HAMS_ERR_NUMERIC, "block LU: zero pivot in column %d", zp);
+    if (word[1]) return fail(HAMS_ERR_CUDA, "block LU: a tensor-core GEMM gave up waiting on its pipeline (%d)", word[1]);
+    if (word[0] <= n) return fail(HAMS_ERR_NUMERIC, "block LU: zero pivot in column %d", word[0]);
     *info_host = 0;
   } else {
     int lw = 0;
-    CUS(cusolverDnCgetrf_bufferSize(c->solver, n, n, (cuComplex*)c->Af.p, n, &lw));
+    CUS(cusolverDnCgetrf_bufferSize(c->solver, n, n, (cuComplex*)c->Af.p, lda, &lw));
     TRY(c->work32.alloc((size_t)lw * sizeof(cuComplex)));
-    CUS(cusolverDnCgetrf(c->solver, n, n, (cuComplex*)c->Af.p, n, (cuComplex*)c->work32.p, c->ipiv.p, c->info.p));
+    CUS(cusolverDnCgetrf(c->solver, n, n, (cuComplex*)c->Af.p, lda, (cuComplex*)c->work32.p, c->ipiv.p, c->info.p));
     c->lib_calls += 1;
     CU(cudaMemcpyAsync(info_host, c->info.p, sizeof(int), cudaMemcpyDeviceToHost, c->st));
   }
@@ -1223,15 +1233,13 @@ static int mixed_solve(hams_ctx* c, double2* M, const double2* rhs, int ldr, int
   // Xf <- LU^-1 Xf
   auto lu_solve = [&]() -> int {
     if (block) {
-      long long la = 0, lb = 0;
-      int rc = mixed_lu_solve(c->st, c->blas, n, nrhs, c->Af.p, c->perm.p, c->Xf.p,
-                              c->luw.p + mixed_lu_workspace_elems(n), &la, &lb);
+      long long la = 0;
+      int rc = mixed_lu_solve(c->st, n, lda, nrhs, c->Af.p, c->perm.p, c->Xf.p, c->luw.p, c->info.p + 1, &la);
       c->launches += la;
-      c->lib_calls += lb;
       if (rc) return fail(HAMS_ERR_CUDA, "block LU solve failed");
       return 0;
     }
-    CUS(cusolverDnCgetrs(c->solver, CUBLAS_OP_N, n, nrhs, (cuComplex*)c->Af.p, n, c->ipiv.p, (cuComplex*)c->Xf.p, n,
+    CUS(cusolverDnCgetrs(c->solver, CUBLAS_OP_N, n, nrhs, (cuComplex*)c->Af.p, lda, c->ipiv.p, (cuComplex*)c->Xf.p, n,
                          c->info.p));
     c->lib_calls += 1;
     return 0;
@@ -1257,7 +1265,10 @@ static int mixed_solve(hams_ctx* c, double2* M, const double2* rhs, int ldr, int
     TRY(launch_check(c));
     // the relative residual is checked against the rhs column scale
     CU(cudaMemcpyAsync(ratio.data(), c->colratio.p, nrhs * 8, cudaMemcpyDeviceToHost, c->st));
+    int werr = 0;
+    if (block) CU(cudaMemcpyAsync(&werr, c->info.p + 1, sizeof(int), cudaMemcpyDeviceToHost, c->st));
     CU(cudaStreamSynchronize(c->st));
+    if (werr) return fail(HAMS_ERR_CUDA, "block LU solve: a wait on another block gave up (%d)", werr);
     double worst = 0.0;
     for (double r : ratio) worst = std::max(worst, r);
     c->refine_sweeps = it;
@@ -2097,5 +2108,36 @@ extern "C" int hams_measure_fp64_peak(int32_t device, double* tflops) {
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   *tflops = 2.0 * 8.0 * iters * (double)threads * blocks / (ms * 1e-3) / 1e12;
+  return 0;
+}
+
+// ---------------------------------------------------------------------------
+// Diagnostic: the block LU's tensor-core GEMM on host arrays
+// ---------------------------------------------------------------------------
+extern "C" int hams_diag_gemm_tf32(int32_t device, int32_t m, int32_t n, int32_t k, float alpha, const float* a,
+                                   int32_t lda, const float* b, int32_t ldb, float beta, float* c, int32_t ldc,
+                                   int32_t c_rowmajor) {
+  g_err.clear();
+  if (m < 1 || n < 1 || k < 1 || !a || !b || !c || lda < k || ldb < k || (lda & 3) || (ldb & 3) ||
+      ldc < (c_rowmajor ? n : m))
+    return fail(HAMS_ERR_ARG, "bad GEMM arguments");
+  if (cudaSetDevice(device) != cudaSuccess) return fail(HAMS_ERR_CUDA, "cudaSetDevice(%d) failed", device);
+  const size_t na = (size_t)m * lda, nb = (size_t)n * ldb, nc = c_rowmajor ? (size_t)m * ldc : (size_t)n * ldc;
+  DBuf<float> da, db, dc;
+  DBuf<int> derr;
+  TRY(da.alloc(na));
+  TRY(db.alloc(nb));
+  TRY(dc.alloc(nc));
+  TRY(derr.alloc(1));
+  CU(cudaMemcpy(da.p, a, na * 4, cudaMemcpyHostToDevice));
+  CU(cudaMemcpy(db.p, b, nb * 4, cudaMemcpyHostToDevice));
+  CU(cudaMemcpy(dc.p, c, nc * 4, cudaMemcpyHostToDevice));
+  CU(cudaMemset(derr.p, 0, sizeof(int)));
+  if (gemm_tf32(0, m, n, k, alpha, da.p, lda, db.p, ldb, beta, dc.p, ldc, c_rowmajor != 0, derr.p))
+    return fail(HAMS_ERR_CUDA, "gemm_tf32 launch failed: %s", cudaGetErrorString(cudaGetLastError()));
+  int err = 0;
+  CU(cudaMemcpy(&err, derr.p, sizeof(int), cudaMemcpyDeviceToHost));
+  CU(cudaMemcpy(c, dc.p, nc * 4, cudaMemcpyDeviceToHost));
+  if (err) return fail(HAMS_ERR_CUDA, "gemm_tf32: a pipeline wait gave up (%d)", err);
   return 0;
 }

@@ -22,16 +22,30 @@
 //                    written once per 256 columns instead of once per 64).
 //
 // The complex products run as real GEMMs on the real expansions of the
-// complex matrices (cuBLAS, tensor cores, FP32 accumulation; inputs rounded
-// to TF32, or FP32 emulated on BF16 tensor cores).  Pivoting is local to
-// each diagonal block (P is block diagonal); the FP64 refinement checks the
-// result, and the caller falls back to a partially pivoted LU if the
-// refinement does not converge.
+// complex matrices, on the library's tcgen05 kernel (gemm_tf32.cu: TF32
+// operands, FP32 accumulation in tensor memory), or on cuBLAS when the
+// caller asks for its FP32 emulation on BF16 tensor cores.  Every left
+// operand is laid out K-major (expanded panels written row-major by
+// k_expand_rm, L_kk^-1 row-major) and every right operand is a column-major
+// slice of the matrix itself, so no operand is transposed in memory.
+// Pivoting is local to each diagonal block (P is block diagonal); the FP64
+// refinement checks the result, and the caller falls back to a partially
+// pivoted LU if the refinement does not converge.
+//
+// The solve (ZGETRS's part) runs as two launches of a block triangular-solve
+// kernel, one per triangle, on the diagonal-block inverses the factorisation
+// keeps: the CTA of block row b and a chunk of 16 right-hand sides subtracts
+// T_bj X_j as each earlier block's X_j is published (a flag per block and
+// chunk), then forms X_b = T_bb^-1 (B_b - sum).  CTAs take their block rows
+// from an atomic ticket in dependency order, so every block a CTA waits for
+// belongs to a CTA that is already running; each wait is bounded and a wait
+// that gives up sets an error bit.
 #include <cublas_v2.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
 
+#include "gemm_tf32.h"
 #include "lu_mixed.h"
 
 namespace {
@@ -51,6 +65,13 @@ __device__ __forceinline__ void put_expanded(float* E, int lde, int i, int k, fl
   E[(size_t)(2 * k) * lde + 2 * i + 1] = x.y;
   E[(size_t)(2 * k + 1) * lde + 2 * i] = -x.y;
   E[(size_t)(2 * k + 1) * lde + 2 * i + 1] = x.x;
+}
+
+// The same expansion stored row-major (E[row * lde + col]): the K-major
+// layout of a left operand of the tensor-core GEMM.
+__device__ __forceinline__ void put_expanded_rm(float* E, int lde, int i, int k, float2 x) {
+  *reinterpret_cast<float2*>(E + (size_t)(2 * i) * lde + 2 * k) = make_float2(x.x, -x.y);
+  *reinterpret_cast<float2*>(E + (size_t)(2 * i + 1) * lde + 2 * k) = make_float2(x.y, x.x);
 }
 
 __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
@@ -125,11 +146,14 @@ __device__ void tri_inverse(const float2* T, float2* X, float2* W, bool lower) {
 // One CTA of 256 threads: LU with partial pivoting of the nbk x nbk
 // diagonal block at (k0, k0), written back in place (unit L below, U on and
 // above the diagonal); the block's row permutation as global source rows in
-// perm; the expansions of L^-1 and U^-1 (2nbk x 2nbk, ld 2 kNB) in invL,
-// invU.  info gets 1 + the first global column whose pivot is zero.  A
-// partial last block is padded with the identity to kNB.
+// perm; the expansions of L^-1 (row-major) and U^-1 (column-major), 2nbk x
+// 2nbk with ld 2 kNB, in invL, invU -- the K-major layouts of a left and a
+// right GEMM operand; and the complex kNB x kNB inverses (column-major, the
+// identity-padded block for a partial last block) in invLc, invUc for the
+// triangular solves.  info gets 1 + the first global column whose pivot is
+// zero.  A partial last block is padded with the identity to kNB.
 __global__ void __launch_bounds__(256) k_diag_lu(float2* A, int lda, int k0, int nbk, int* perm, float* invL,
-                                                 float* invU, int* info) {
+                                                 float* invU, float2* invLc, float2* invUc, int* info) {
   extern __shared__ float2 sm[];
   float2* T = sm;                  // [col * kLd + row]
   float2* X = sm + kNB * kLd;      // L^-1
@@ -218,18 +242,46 @@ __global__ void __launch_bounds__(256) k_diag_lu(float2* A, int lda, int k0, int
   for (int e = tid; e < nbk * nbk; e += 256) {
     int r = e % nbk, c = e / nbk;
     A[(size_t)(k0 + c) * lda + k0 + r] = T[c * kLd + r];
-    put_expanded(invL, 2 * kNB, r, c, X[c * kLd + r]);
+    put_expanded_rm(invL, 2 * kNB, r, c, X[c * kLd + r]);
     put_expanded(invU, 2 * kNB, r, c, Y[c * kLd + r]);
+  }
+  for (int e = tid; e < kNB * kNB; e += 256) {
+    int r = e % kNB, c = e / kNB;
+    invLc[e] = X[c * kLd + r];
+    invUc[e] = Y[c * kLd + r];
   }
   for (int i = tid; i < nbk; i += 256) perm[k0 + i] = k0 + prm[i];
 }
 
-// E (2w x 2nbk, ld 2w) <- expansion of the w x nbk column panel at (k1, k0).
-__global__ void k_expand_panel(const float2* __restrict__ A, int lda, int k1, int k0, int w, int nbk, float* E) {
-  size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= (size_t)w * nbk) return;
-  int i = (int)(e % w), k = (int)(e / w);
-  put_expanded(E, 2 * w, i, k, A[(size_t)(k0 + k) * lda + k1 + i]);
+
+// E (2w x 2kc, row-major, ld lde) <- the real expansion of the complex w x kc
+// block of A at (r0, c0): a 32 x 32 tile through shared memory, so that the
+// column-major reads of A and the row-major writes of E are both coalesced.
+__global__ void __launch_bounds__(256) k_expand_rm(const float2* __restrict__ A, int lda, int r0, int c0, int w,
+                                                   int kc, float* __restrict__ E, int lde) {
+  __shared__ float2 tile[32][33];
+  const int i0 = blockIdx.x * 32, k0 = blockIdx.y * 32, tx = threadIdx.x % 32, ty = threadIdx.x / 32;
+  for (int c = ty; c < 32; c += 8)
+    if (i0 + tx < w && k0 + c < kc) tile[c][tx] = A[(size_t)(c0 + k0 + c) * lda + r0 + i0 + tx];
+  __syncthreads();
+  for (int r = ty; r < 32; r += 8)
+    if (i0 + r < w && k0 + tx < kc) put_expanded_rm(E, lde, i0 + r, k0 + tx, tile[tx][r]);
+}
+
+// The complex L_ik (wr x nbk) into A at (k1, k0) from the row-major
+// expansion Lhat (2wr x 2nbk, ld ldl): entry (i, c) is (Lhat[2i][2c],
+// Lhat[2i+1][2c]).
+__global__ void __launch_bounds__(256) k_extract_l(const float* __restrict__ Lhat, int ldl, int wr, int nbk,
+                                                   float2* __restrict__ A, int lda, int k1, int k0) {
+  __shared__ float2 tile[32][33];
+  const int i0 = blockIdx.x * 32, c0 = blockIdx.y * 32, tx = threadIdx.x % 32, ty = threadIdx.x / 32;
+  for (int r = ty; r < 32; r += 8)
+    if (i0 + r < wr && c0 + tx < nbk)
+      tile[r][tx] = make_float2(Lhat[(size_t)(2 * (i0 + r)) * ldl + 2 * (c0 + tx)],
+                                Lhat[(size_t)(2 * (i0 + r) + 1) * ldl + 2 * (c0 + tx)]);
+  __syncthreads();
+  for (int c = ty; c < 32; c += 8)
+    if (i0 + tx < wr && c0 + c < nbk) A[(size_t)(k0 + c0 + c) * lda + k1 + i0 + tx] = tile[tx][c];
 }
 
 // Rows k0..k0+nbk-1 of every column outside the diagonal block take the
@@ -246,52 +298,202 @@ __global__ void k_apply_perm(float2* A, int lda, int n, int k0, int nbk, const i
     if (live) A[(size_t)c * lda + k0 + i] = tile[i][tx];
 }
 
-// X (n x nrhs, ld n) <- rows gathered by perm.
-__global__ void k_gather_rows(const float2* __restrict__ src, float2* __restrict__ dst, int n, int nrhs,
-                              const int* __restrict__ perm) {
-  size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= (size_t)n * nrhs) return;
-  int r = (int)(e % n);
-  size_t c = e / n;
-  dst[e] = src[c * n + perm[r]];
+// ---------------------------------------------------------------------------
+// Block triangular solves
+// ---------------------------------------------------------------------------
+constexpr int kNC = 16;  // right-hand sides per CTA
+constexpr int kTrsmSmem = (kNB * (kNB + 1) + 2 * kNB * kNC) * (int)sizeof(float2);
+constexpr long long kFlagSpin = 1ll << 24;
+
+__device__ __forceinline__ float2 csub_mul(float2 s, float2 a, float2 b) {
+  return make_float2(s.x - (a.x * b.x - a.y * b.y), s.y - (a.x * b.y + a.y * b.x));
 }
 
-cublasStatus_t sgemm(cublasHandle_t h, cublasComputeType_t ct, int m, int n, int k, float alpha, const float* A,
-                     int lda, const float* B, int ldb, float beta, float* C, int ldc) {
-  return cublasGemmEx(h, CUBLAS_OP_N, CUBLAS_OP_N, m, n, k, &alpha, A, CUDA_R_32F, lda, B, CUDA_R_32F, ldb, &beta, C,
-                      CUDA_R_32F, ldc, ct, CUBLAS_GEMM_DEFAULT);
+// One launch solves one triangle for all right-hand sides.  lower: unit L,
+// blocks in increasing order, the right-hand sides gathered through perm
+// from B; upper: U, blocks in decreasing order, B unpermuted.  X receives
+// the solution (n x nrhs, ld n).  flags (nblk x nch) and ticket start at 0.
+__global__ void __launch_bounds__(256) k_trsm_block(const float2* __restrict__ A, int lda, int n, int nrhs, int nblk,
+                                                    int nch, bool lower, const float2* __restrict__ invc,
+                                                    const int* __restrict__ perm, const float2* __restrict__ B,
+                                                    float2* X, int* flags, unsigned int* ticket, int* err) {
+  extern __shared__ float2 sm[];
+  float2* sT = sm;                    // a 64 x 64 block, column-major, ld kNB + 1
+  float2* sX = sm + kNB * (kNB + 1);  // the published X_j of the chunk (64 x kNC)
+  float2* sAcc = sX + kNB * kNC;      // B_b - sum, the operand of the inverse
+  __shared__ int s_id, s_abort;
+  const int tid = threadIdx.x;
+  if (tid == 0) {
+    s_id = (int)atomicAdd(ticket, 1u);
+    s_abort = 0;
+  }
+  __syncthreads();
+  const int order = s_id / nch, ch = s_id % nch;
+  const int b = lower ? order : nblk - 1 - order;
+  const int q0 = ch * kNC, r = tid % kNB, qq = (tid / kNB) * 4;  // this thread: row r, chunk columns qq..qq+3
+  const int row = b * kNB + r;
+  // the block's right-hand sides
+  for (int e = tid; e < kNB * kNC; e += 256) {
+    const int rr = e % kNB, q = e / kNB, gr = b * kNB + rr;
+    float2 v = make_float2(0.0f, 0.0f);
+    if (gr < n && q0 + q < nrhs) v = B[(size_t)(q0 + q) * n + (lower ? perm[gr] : gr)];
+    sAcc[q * kNB + rr] = v;
+  }
+  __syncthreads();
+  float2 acc[4];
+  for (int u = 0; u < 4; ++u) acc[u] = make_float2(0.0f, 0.0f);
+  for (int step = 0; step < order; ++step) {
+    const int j = lower ? step : nblk - 1 - step;
+    // the off-diagonal block T = A[b rows, j columns], read while the flag is awaited
+    for (int e = tid; e < kNB * kNB; e += 256) {
+      const int rr = e % kNB, cc = e / kNB, gr = b * kNB + rr, gc = j * kNB + cc;
+      sT[cc * (kNB + 1) + rr] = (gr < n && gc < n) ? A[(size_t)gc * lda + gr] : make_float2(0.0f, 0.0f);
+    }
+    if (tid == 0) {
+      const volatile int* f = flags + j * nch + ch;
+      long long it = 0;
+      while (*f == 0) {
+        if (++it > kFlagSpin) {
+          atomicOr(err, 2);
+          s_abort = 1;
+          break;
+        }
+        __nanosleep(64);
+      }
+      __threadfence();
+    }
+    __syncthreads();
+    if (s_abort) break;
+    for (int e = tid; e < kNB * kNC; e += 256) {
+      const int rr = e % kNB, q = e / kNB, gr = j * kNB + rr;
+      sX[q * kNB + rr] =
+          (gr < n && q0 + q < nrhs) ? __ldcg(X + (size_t)(q0 + q) * n + gr) : make_float2(0.0f, 0.0f);
+    }
+    __syncthreads();
+#pragma unroll 4
+    for (int k = 0; k < kNB; ++k) {
+      const float2 t = sT[k * (kNB + 1) + r];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) acc[u] = csub_mul(acc[u], t, sX[(qq + u) * kNB + k]);
+    }
+    __syncthreads();
+  }
+  // X_b = T_bb^-1 (B_b - sum)
+  for (int u = 0; u < 4; ++u) {
+    float2& s = sAcc[(qq + u) * kNB + r];
+    s = make_float2(s.x + acc[u].x, s.y + acc[u].y);
+  }
+  const float2* inv = invc + (size_t)b * kNB * kNB;
+  for (int e = tid; e < kNB * kNB; e += 256) sT[(e / kNB) * (kNB + 1) + e % kNB] = inv[e];
+  __syncthreads();
+  float2 out[4];
+  for (int u = 0; u < 4; ++u) out[u] = make_float2(0.0f, 0.0f);
+#pragma unroll 4
+  for (int k = 0; k < kNB; ++k) {
+    const float2 t = sT[k * (kNB + 1) + r];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) out[u] = csub_mul(out[u], t, sAcc[(qq + u) * kNB + k]);
+  }
+  if (row < n)
+    for (int u = 0; u < 4; ++u)
+      if (q0 + qq + u < nrhs) X[(size_t)(q0 + qq + u) * n + row] = make_float2(-out[u].x, -out[u].y);
+  __threadfence();
+  __syncthreads();
+  if (tid == 0) atomicExch(flags + b * nch + ch, 1);  // published (also after an abandoned wait, so no CTA hangs)
 }
+
+// ---------------------------------------------------------------------------
+// GEMM dispatch: C = alpha A B + beta C, A K-major (row-major m x k), B
+// K-major (column-major k x n), C column-major or row-major.
+// ---------------------------------------------------------------------------
+struct Gemm {
+  bool own;
+  cublasHandle_t blas;
+  cublasComputeType_t ct;
+  cudaStream_t st;
+  int* err;
+  long long* launches;
+  long long* lib_calls;
+};
+
+// 0, 1 on a launch error, or 10 + cuBLAS status
+int gemm(const Gemm& g, int m, int n, int k, float alpha, const float* A, int lda, const float* B, int ldb, float beta,
+         float* C, int ldc, bool c_rowmajor) {
+  if (m <= 0 || n <= 0 || k <= 0) return 0;
+  if (g.own) {
+    *g.launches += 1;
+    return gemm_tf32(g.st, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, c_rowmajor, g.err);
+  }
+  *g.lib_calls += 1;
+  cublasStatus_t s;
+  if (!c_rowmajor)  // A row-major m x k is the column-major k x m matrix: op T
+    s = cublasGemmEx(g.blas, CUBLAS_OP_T, CUBLAS_OP_N, m, n, k, &alpha, A, CUDA_R_32F, lda, B, CUDA_R_32F, ldb, &beta,
+                     C, CUDA_R_32F, ldc, g.ct, CUBLAS_GEMM_DEFAULT);
+  else  // C^T = B^T A^T, column-major n x m
+    s = cublasGemmEx(g.blas, CUBLAS_OP_T, CUBLAS_OP_N, n, m, k, &alpha, B, CUDA_R_32F, ldb, A, CUDA_R_32F, lda, &beta,
+                     C, CUDA_R_32F, ldc, g.ct, CUBLAS_GEMM_DEFAULT);
+  return s == CUBLAS_STATUS_SUCCESS ? 0 : 10 + (int)s;
+}
+
+// Workspace offsets (floats): W1 (2kNB x n, column-major), Ehat and Lhat
+// (2n x 2kNB, row-major), the expanded inverses of a panel's diagonal blocks
+// (kPB each, L^-1 row-major, U^-1 column-major), E2 (2kNB x 2kNB (kPB - 1),
+// row-major), Ebig (2n x 2kNB kPB, row-major), then the complex inverses of
+// every diagonal block (kNB x kNB each, L then U), the forward solution of
+// the solve (n x nrhs) and the solve's flags and ticket.
+struct Layout {
+  size_t W1, Ehat, Lhat, invL, invU, E2, Ebig, invLc, invUc, T, flags, total;
+  Layout(int n, int nrhs) {
+    const size_t K2 = 2 * kNB, nblk = (size_t)(n + kNB - 1) / kNB, nch = (size_t)(nrhs + kNC - 1) / kNC;
+    W1 = 0;
+    Ehat = W1 + K2 * n;
+    Lhat = Ehat + 2 * (size_t)n * K2;
+    invL = Lhat + 2 * (size_t)n * K2;
+    invU = invL + kPB * K2 * K2;
+    E2 = invU + kPB * K2 * K2;
+    Ebig = E2 + K2 * K2 * (kPB - 1);
+    invLc = Ebig + 2 * (size_t)n * K2 * kPB;  // complex from here on; offsets stay in floats
+    invUc = invLc + 2 * nblk * kNB * kNB;
+    T = invUc + 2 * nblk * kNB * kNB;
+    flags = T + 2 * (size_t)n * std::max(nrhs, 1);
+    total = flags + ((nblk * nch + 4) + 3) / 4 * 4;  // ints, one float each
+  }
+};
 
 }  // namespace
 
-// Workspace (floats): U rows W1 (2kNB x n), expanded L column of a block and
-// its source (2 x 2n x 2kNB), the expanded inverses of a panel's diagonal
-// blocks (2 x kPB x 2kNB x 2kNB), the expanded L rows of a block left of it
-// in its panel (2kNB x 2kNB (kPB - 1)) and the expanded L columns of a whole
-// panel (2n x 2kNB kPB).
-size_t mixed_lu_workspace_elems(int n) {
-  const size_t K2 = 2 * kNB;
-  return (K2 * n + 2 * (2 * (size_t)n * K2) + 2 * kPB * K2 * K2 + K2 * K2 * (kPB - 1) + 2 * (size_t)n * K2 * kPB) / 2 +
-         1;
-}
+size_t mixed_lu_workspace_elems(int n, int nrhs) { return Layout(n, nrhs).total / 2 + 1; }
 
-int mixed_lu_factor(cudaStream_t st, cublasHandle_t blas, cublasComputeType_t ct, int n, float2* A, int* perm,
-                    float2* work, int* dinfo, long long* launches, long long* lib_calls) {
+int mixed_lu_factor(cudaStream_t st, cublasHandle_t blas, bool own_gemm, cublasComputeType_t ct, int n, int lda,
+                    float2* A, int* perm, float2* work, int* dinfo, long long* launches, long long* lib_calls) {
   const int smem = (3 * kNB + 32) * kLd * (int)sizeof(float2);
   if (cudaFuncSetAttribute(k_diag_lu, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess) return 1;
+  if (lda < n || (lda & 1)) return 1;
   const int K2 = 2 * kNB, PW = kPB * kNB;
-  float* W1 = (float*)work;                     // U rows, real 2nbk x w (ld 2kNB)
-  float* Ehat = W1 + (size_t)K2 * n;            // expanded A_ik, 2w x 2nbk (ld 2w)
-  float* Lhat = Ehat + (size_t)2 * n * K2;      // expanded L_ik, 2w x 2nbk (ld 2w)
-  float* invL = Lhat + (size_t)2 * n * K2;      // kPB x (2nbk x 2nbk, ld 2kNB)
-  float* invU = invL + (size_t)kPB * K2 * K2;
-  float* E2 = invU + (size_t)kPB * K2 * K2;     // expanded L rows left of a block, 2nbk x 2(k0 - p0) (ld 2nbk)
-  float* Ebig = E2 + (size_t)K2 * K2 * (kPB - 1);  // expanded L columns of a panel, 2wt x 2(p1 - p0) (ld 2wt)
+  const Layout L(n, 0);
+  float* ws = (float*)work;
+  float* W1 = ws + L.W1;      // U rows, real 2nbk x w (column-major, ld 2kNB)
+  float* Ehat = ws + L.Ehat;  // expanded A_ik, 2wr x 2nbk (row-major, ld 2kNB)
+  float* Lhat = ws + L.Lhat;  // expanded L_ik, 2wr x 2nbk (row-major, ld 2kNB)
+  float* invL = ws + L.invL;  // kPB x (2kNB x 2kNB), row-major
+  float* invU = ws + L.invU;  // kPB x (2kNB x 2kNB), column-major
+  float* E2 = ws + L.E2;      // expanded L rows left of a block in its panel, 2nbk x 2(k0 - p0) (row-major)
+  float* Ebig = ws + L.Ebig;  // expanded L columns of a panel, 2wt x 2(p1 - p0) (row-major)
+  float2* invLc = (float2*)(ws + L.invLc);
+  float2* invUc = (float2*)(ws + L.invUc);
   if (cudaMemsetAsync(dinfo, 0x7f, sizeof(int), st) != cudaSuccess) return 1;  // large positive: no zero pivot
-  if (cudaMemsetAsync(invL, 0, 2 * (size_t)kPB * K2 * K2 * sizeof(float), st) != cudaSuccess) return 1;
-  float* Ar = (float*)A;  // A viewed as floats: 2n x n, ld 2n
-  const size_t ldr = 2 * (size_t)n;
-  cublasStatus_t bs;
+  if (cudaMemsetAsync(dinfo + 1, 0, sizeof(int), st) != cudaSuccess) return 1;
+  Gemm g{own_gemm, blas, ct, st, dinfo + 1, launches, lib_calls};
+  float* Ar = (float*)A;  // A viewed as floats: 2 lda x n, column-major
+  const int ldr = 2 * lda;
+  auto expand = [&](int r0, int c0, int w, int kc, float* E, int lde) {
+    dim3 grid((unsigned)((w + 31) / 32), (unsigned)((kc + 31) / 32));
+    k_expand_rm<<<grid, 256, 0, st>>>(A, lda, r0, c0, w, kc, E, lde);
+    *launches += 1;
+    return cudaGetLastError() == cudaSuccess;
+  };
+  auto code = [](int rc, int g, int b) { return rc == 1 ? 1 : 100 * g + 1000 * b + rc - 10; };
+  int rc;
   for (int p0 = 0, pb = 0; p0 < n; p0 += PW, ++pb) {
     const int p1 = std::min(n, p0 + PW);
     // the panel's column blocks, updates confined to the panel's columns
@@ -300,91 +502,84 @@ int mixed_lu_factor(cudaStream_t st, cublasHandle_t blas, cublasComputeType_t ct
                 k2 = 2 * nbk;
       float* iL = invL + (size_t)s * K2 * K2;
       float* iU = invU + (size_t)s * K2 * K2;
-      k_diag_lu<<<1, 256, smem, st>>>(A, n, k0, nbk, perm, iL, iU, dinfo);
-      k_apply_perm<<<(n + 31) / 32, 256, 0, st>>>(A, n, n, k0, nbk, perm);
+      k_diag_lu<<<1, 256, smem, st>>>(A, lda, k0, nbk, perm, iL, iU, invLc + (size_t)b * kNB * kNB,
+                                      invUc + (size_t)b * kNB * kNB, dinfo);
+      k_apply_perm<<<(n + 31) / 32, 256, 0, st>>>(A, lda, n, k0, nbk, perm);
       *launches += 2;
       if (cudaGetLastError() != cudaSuccess) return 1;
       if (wr <= 0) break;
-      k_expand_panel<<<(unsigned)(((size_t)wr * nbk + 255) / 256), 256, 0, st>>>(A, n, k1, k0, wr, nbk, Ehat);
-      *launches += 1;
-      if (cudaGetLastError() != cudaSuccess) return 1;
-      // L_ik^ = A_ik^ U_kk^-1^
-      if ((bs = sgemm(blas, ct, 2 * wr, k2, k2, 1.0f, Ehat, 2 * wr, iU, K2, 0.0f, Lhat, 2 * wr)) != CUBLAS_STATUS_SUCCESS)
-        return 200 + 1000 * b + (int)bs;
-      *lib_calls += 1;
+      if (!expand(k1, k0, wr, nbk, Ehat, K2)) return 1;
+      // L_ik^ = A_ik^ U_kk^-1^ (row-major: the left operand of the update below)
+      if ((rc = gemm(g, 2 * wr, k2, k2, 1.0f, Ehat, K2, iU, K2, 0.0f, Lhat, K2, true))) return code(rc, 2, b);
       if (wp > 0) {
-        float* Akj = Ar + (size_t)k1 * ldr + 2 * k0;  // real 2nbk x wp, ld 2n
-        float* Aij = Ar + (size_t)k1 * ldr + 2 * k1;  // real 2wr x wp, ld 2n
+        float* Akj = Ar + (size_t)k1 * ldr + 2 * k0;  // real 2nbk x wp, ld 2 lda
+        float* Aij = Ar + (size_t)k1 * ldr + 2 * k1;  // real 2wr x wp, ld 2 lda
         // U_kj = L_kk^-1 A_kj and A_ij -= L_ik U_kj inside the panel
-        if ((bs = sgemm(blas, ct, k2, wp, k2, 1.0f, iL, K2, Akj, (int)ldr, 0.0f, W1, K2)) != CUBLAS_STATUS_SUCCESS)
-          return 100 + 1000 * b + (int)bs;
-        if ((bs = sgemm(blas, ct, 2 * wr, wp, k2, -1.0f, Lhat, 2 * wr, W1, K2, 1.0f, Aij, (int)ldr)) !=
-            CUBLAS_STATUS_SUCCESS)
-          return 300 + 1000 * b + (int)bs;
-        *lib_calls += 2;
-        if (cudaMemcpy2DAsync(Akj, ldr * 4, W1, (size_t)K2 * 4, (size_t)k2 * 4, wp, cudaMemcpyDeviceToDevice, st) !=
-            cudaSuccess)
+        if ((rc = gemm(g, k2, wp, k2, 1.0f, iL, K2, Akj, ldr, 0.0f, W1, K2, false))) return code(rc, 1, b);
+        if ((rc = gemm(g, 2 * wr, wp, k2, -1.0f, Lhat, K2, W1, K2, 1.0f, Aij, ldr, false))) return code(rc, 3, b);
+        if (cudaMemcpy2DAsync(Akj, (size_t)ldr * 4, W1, (size_t)K2 * 4, (size_t)k2 * 4, wp, cudaMemcpyDeviceToDevice,
+                              st) != cudaSuccess)
           return 1;
       }
-      // L_ik = the even columns of L_ik^
-      if (cudaMemcpy2DAsync(A + (size_t)k0 * n + k1, (size_t)n * 8, Lhat, (size_t)2 * (2 * wr) * 4, (size_t)2 * wr * 4,
-                            nbk, cudaMemcpyDeviceToDevice, st) != cudaSuccess)
-        return 1;
+      {  // L_ik into A
+        dim3 grid((unsigned)((wr + 31) / 32), (unsigned)((nbk + 31) / 32));
+        k_extract_l<<<grid, 256, 0, st>>>(Lhat, K2, wr, nbk, A, lda, k1, k0);
+        *launches += 1;
+        if (cudaGetLastError() != cudaSuccess) return 1;
+      }
     }
     const int wt = n - p1;
     if (wt <= 0) break;
     // U rows of the panel for the columns right of it: block forward
     // substitution with the panel's unit lower diagonal blocks
-    float* Upt = Ar + (size_t)p1 * ldr + 2 * p0;  // real 2(p1 - p0) x wt, ld 2n
+    float* Upt = Ar + (size_t)p1 * ldr + 2 * p0;  // real 2(p1 - p0) x wt, ld 2 lda
     for (int s = 0, k0 = p0; k0 < p1; ++s, k0 += kNB) {
       const int b = pb * kPB + s, nbk = std::min(kNB, p1 - k0), k2 = 2 * nbk;
-      float* Akt = Ar + (size_t)p1 * ldr + 2 * k0;  // real 2nbk x wt, ld 2n
+      float* Akt = Ar + (size_t)p1 * ldr + 2 * k0;  // real 2nbk x wt, ld 2 lda
       if (s > 0) {
         const int wl = k0 - p0;  // A_kt -= L_k,[p0,k0) U_[p0,k0),t
-        k_expand_panel<<<(unsigned)(((size_t)nbk * wl + 255) / 256), 256, 0, st>>>(A, n, k0, p0, nbk, wl, E2);
-        *launches += 1;
-        if (cudaGetLastError() != cudaSuccess) return 1;
-        if ((bs = sgemm(blas, ct, k2, wt, 2 * wl, -1.0f, E2, k2, Upt, (int)ldr, 1.0f, Akt, (int)ldr)) !=
-            CUBLAS_STATUS_SUCCESS)
-          return 400 + 1000 * b + (int)bs;
-        *lib_calls += 1;
+        if (!expand(k0, p0, nbk, wl, E2, 2 * wl)) return 1;
+        if ((rc = gemm(g, k2, wt, 2 * wl, -1.0f, E2, 2 * wl, Upt, ldr, 1.0f, Akt, ldr, false))) return code(rc, 4, b);
       }
-      if ((bs = sgemm(blas, ct, k2, wt, k2, 1.0f, invL + (size_t)s * K2 * K2, K2, Akt, (int)ldr, 0.0f, W1, K2)) !=
-          CUBLAS_STATUS_SUCCESS)
-        return 500 + 1000 * b + (int)bs;
-      *lib_calls += 1;
-      if (cudaMemcpy2DAsync(Akt, ldr * 4, W1, (size_t)K2 * 4, (size_t)k2 * 4, wt, cudaMemcpyDeviceToDevice, st) !=
-          cudaSuccess)
+      if ((rc = gemm(g, k2, wt, k2, 1.0f, invL + (size_t)s * K2 * K2, K2, Akt, ldr, 0.0f, W1, K2, false)))
+        return code(rc, 5, b);
+      if (cudaMemcpy2DAsync(Akt, (size_t)ldr * 4, W1, (size_t)K2 * 4, (size_t)k2 * 4, wt, cudaMemcpyDeviceToDevice,
+                            st) != cudaSuccess)
         return 1;
     }
     // the trailing update of the whole panel at once: A_tt -= L_t,panel U_panel,t
     const int pw = p1 - p0;
-    k_expand_panel<<<(unsigned)(((size_t)wt * pw + 255) / 256), 256, 0, st>>>(A, n, p1, p0, wt, pw, Ebig);
-    *launches += 1;
-    if (cudaGetLastError() != cudaSuccess) return 1;
-    float* Att = Ar + (size_t)p1 * ldr + 2 * p1;  // real 2wt x wt, ld 2n
-    if ((bs = sgemm(blas, ct, 2 * wt, wt, 2 * pw, -1.0f, Ebig, 2 * wt, Upt, (int)ldr, 1.0f, Att, (int)ldr)) !=
-        CUBLAS_STATUS_SUCCESS)
-      return 600 + 1000 * pb * kPB + (int)bs;
-    *lib_calls += 1;
+    if (!expand(p1, p0, wt, pw, Ebig, 2 * pw)) return 1;
+    float* Att = Ar + (size_t)p1 * ldr + 2 * p1;  // real 2wt x wt, ld 2 lda
+    if ((rc = gemm(g, 2 * wt, wt, 2 * pw, -1.0f, Ebig, 2 * pw, Upt, ldr, 1.0f, Att, ldr, false)))
+      return code(rc, 6, pb * kPB);
   }
   return 0;
 }
 
-int mixed_lu_solve(cudaStream_t st, cublasHandle_t blas, int n, int nrhs, const float2* A, const int* perm, float2* X,
-                   float2* tmp, long long* launches, long long* lib_calls) {
-  size_t tot = (size_t)n * nrhs;
-  k_gather_rows<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(X, tmp, n, nrhs, perm);
-  *launches += 1;
+int mixed_lu_solve(cudaStream_t st, int n, int lda, int nrhs, const float2* A, const int* perm, float2* X,
+                   float2* work, int* dflag, long long* launches) {
+  if (nrhs <= 0) return 0;
+  if (cudaFuncSetAttribute(k_trsm_block, cudaFuncAttributeMaxDynamicSharedMemorySize, kTrsmSmem) != cudaSuccess)
+    return 1;
+  const Layout L(n, nrhs);
+  float* ws = (float*)work;
+  const int nblk = (n + kNB - 1) / kNB, nch = (nrhs + kNC - 1) / kNC;
+  const float2* invLc = (const float2*)(ws + L.invLc);
+  const float2* invUc = (const float2*)(ws + L.invUc);
+  float2* T = (float2*)(ws + L.T);
+  int* flags = (int*)(ws + L.flags);
+  unsigned int* ticket = (unsigned int*)(flags + nblk * nch);
+  const unsigned grid = (unsigned)(nblk * nch);
+  // forward: T = L^-1 P X; backward: X = U^-1 T
+  if (cudaMemsetAsync(flags, 0, (size_t)(nblk * nch + 1) * sizeof(int), st) != cudaSuccess) return 1;
+  k_trsm_block<<<grid, 256, kTrsmSmem, st>>>(A, lda, n, nrhs, nblk, nch, true, invLc, perm, X, T, flags, ticket,
+                                             dflag);
   if (cudaGetLastError() != cudaSuccess) return 1;
-  const cuComplex one = make_cuComplex(1.0f, 0.0f);
-  if (cublasCtrsm(blas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N, CUBLAS_DIAG_UNIT, n, nrhs, &one,
-                  (const cuComplex*)A, n, (cuComplex*)tmp, n) != CUBLAS_STATUS_SUCCESS)
-    return 2;
-  if (cublasCtrsm(blas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT, n, nrhs, &one,
-                  (const cuComplex*)A, n, (cuComplex*)tmp, n) != CUBLAS_STATUS_SUCCESS)
-    return 2;
-  *lib_calls += 2;
-  if (cudaMemcpyAsync(X, tmp, tot * sizeof(float2), cudaMemcpyDeviceToDevice, st) != cudaSuccess) return 1;
+  if (cudaMemsetAsync(flags, 0, (size_t)(nblk * nch + 1) * sizeof(int), st) != cudaSuccess) return 1;
+  k_trsm_block<<<grid, 256, kTrsmSmem, st>>>(A, lda, n, nrhs, nblk, nch, false, invUc, perm, T, X, flags, ticket,
+                                             dflag);
+  if (cudaGetLastError() != cudaSuccess) return 1;
+  *launches += 2;
   return 0;
 }

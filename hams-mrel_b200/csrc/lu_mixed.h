@@ -3,19 +3,30 @@
 #include <cublas_v2.h>
 #include <cuda_runtime.h>
 
-// Elements (float2) of the workspace mixed_lu_factor needs for order n.
-size_t mixed_lu_workspace_elems(int n);
+// Elements (float2) of the workspace mixed_lu_factor / mixed_lu_solve need
+// for order n and nrhs right-hand sides.
+size_t mixed_lu_workspace_elems(int n, int nrhs);
 
-// In-place factorisation P A = L U of the n x n complex64 matrix A (ld n),
-// P block diagonal (pivoting inside each 64-row diagonal block); perm (n)
-// receives the permutation as source rows, dinfo 1 + the first column with
-// a zero pivot (or a large value if none).  GEMMs run on cuBLAS with compute
-// type ct.  Returns 0, 1 on a CUDA error, or 100 g + 1000 b + status for a
-// cuBLAS error of GEMM g (1-3) at block b.
-int mixed_lu_factor(cudaStream_t st, cublasHandle_t blas, cublasComputeType_t ct, int n, float2* A, int* perm,
-                    float2* work, int* dinfo, long long* launches, long long* lib_calls);
+// Leading dimension (complex elements) of the matrix the block LU works on:
+// n rounded up to even, so that every column of the float view starts on a
+// 16-byte boundary (the tensor-memory-accelerator copies need it).
+inline int mixed_lu_ld(int n) { return n + (n & 1); }
 
-// X (n x nrhs, ld n) <- (P^T L U)^-1 X using the factors of mixed_lu_factor;
-// tmp holds n x nrhs elements.
-int mixed_lu_solve(cudaStream_t st, cublasHandle_t blas, int n, int nrhs, const float2* A, const int* perm, float2* X,
-                   float2* tmp, long long* launches, long long* lib_calls);
+// In-place factorisation P A = L U of the n x n complex64 matrix A (leading
+// dimension lda = mixed_lu_ld(n)), P block diagonal (pivoting inside each
+// 64-row diagonal block); perm (n) receives the permutation as source rows,
+// dinfo[0] 1 + the first column with a zero pivot (or a large value if
+// none), dinfo[1] the tensor-core kernels' error word (nonzero if a pipeline
+// wait gave up).  With own_gemm the products run on the library's tcgen05
+// kernel (TF32 operands, FP32 accumulation); otherwise on cuBLAS with
+// compute type ct.  Returns 0, 1 on a CUDA or launch error, or 100 g + 1000 b
+// + status for a cuBLAS error of GEMM g at block b.
+int mixed_lu_factor(cudaStream_t st, cublasHandle_t blas, bool own_gemm, cublasComputeType_t ct, int n, int lda,
+                    float2* A, int* perm, float2* work, int* dinfo, long long* launches, long long* lib_calls);
+
+// X (n x nrhs, ld n) <- (P^T L U)^-1 X with the factors of mixed_lu_factor,
+// by the library's block triangular-solve kernels (one launch per triangle).
+// dflag: the error word (bit 1 set if a wait on another block gave up).
+// Returns 0 or 1 on a launch error.
+int mixed_lu_solve(cudaStream_t st, int n, int lda, int nrhs, const float2* A, const int* perm, float2* X,
+                   float2* work, int* dflag, long long* launches);

@@ -104,6 +104,8 @@ def load_library(path=LIB_PATH):
     lib.hams_surrogate_train.argtypes = [c_int, ctypes.POINTER(SgTrain), P_flt, P_dbl]
     lib.hams_surrogate_eval.argtypes = [c_int, P_flt, c_int, P_dbl, P_dbl]
     lib.hams_surrogate_grad.argtypes = [c_int, P_flt, c_int, P_flt, P_flt, P_dbl, P_flt]
+    lib.hams_diag_gemm_tf32.argtypes = [c_int, c_int, c_int, c_int, ctypes.c_float, P_flt, c_int, P_flt, c_int,
+                                        ctypes.c_float, P_flt, c_int, c_int]
     _LIB = lib
     return lib
 
@@ -319,6 +321,22 @@ def measure_fp64_peak(device=0):
     t = ctypes.c_double()
     _check(load_library().hams_measure_fp64_peak(device, ctypes.byref(t)))
     return t.value
+
+
+def diag_gemm_tf32(a, b, c=None, alpha=1.0, beta=0.0, c_rowmajor=False, device=0):
+    """The block LU's tensor-core GEMM: alpha a @ b + beta c for float32 a (m x k), b (k x n), c (m x n)."""
+    m, k = a.shape
+    n = b.shape[1]
+    ld = (k + 3) // 4 * 4
+    A = np.zeros((m, ld), dtype=np.float32)
+    A[:, :k] = a
+    B = np.zeros((n, ld), dtype=np.float32)  # column-major k x n
+    B[:, :k] = b.T
+    C = np.zeros((m, n), dtype=np.float32) if c is None else np.asarray(c, dtype=np.float32)
+    Cbuf = np.ascontiguousarray(C) if c_rowmajor else np.ascontiguousarray(C.T)
+    _check(load_library().hams_diag_gemm_tf32(device, m, n, k, alpha, _f(A), ld, _f(B), ld, beta, _f(Cbuf),
+                                               n if c_rowmajor else m, int(c_rowmajor)))
+    return Cbuf if c_rowmajor else Cbuf.T
 
 
 # ---------------------------------------------------------------------------

@@ -334,6 +334,14 @@ int hams_mark_elapsed(hams_ctx *ctx, int32_t a, int32_t b, double *ms);
  * denominator of the Green-function kernels' roofline. */
 int hams_measure_fp64_peak(int32_t device, double *tflops);
 
+/* Diagnostic (no counterpart in the reference): the mixed form's
+ * tensor-core GEMM (tcgen05.mma kind::tf32, FP32 accumulation) on host
+ * arrays, for tests: C = alpha A B + beta C with A m x k row-major (lda, a
+ * multiple of 4), B k x n column-major (ldb, a multiple of 4), C m x n
+ * column-major, or row-major with c_rowmajor (ldc). */
+int hams_diag_gemm_tf32(int32_t device, int32_t m, int32_t n, int32_t k, float alpha, const float *a, int32_t lda,
+                        const float *b, int32_t ldb, float beta, float *c, int32_t ldc, int32_t c_rowmajor);
+
 /* Message of the last failing call on this thread ("" if none). */
 const char *hams_last_error(void);
 
