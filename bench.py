@@ -225,9 +225,18 @@ def reference_arm(args):
     budget = args.cpu_seconds or 120.0
     per, parts, om_run = [], [], []
     t_start = time.perf_counter()
+    # the sweep in an order whose every prefix is spread over the whole range (the
+    # GPU arm's K steps are spread over it too): 0, 1/2, 1/4, 3/4, 1/8, ... of the sweep
+    order, seen = [], set()
+    for d in range(12):
+        for q in range(2 ** max(d - 1, 0)):
+            k = ((2 * q + 1) * len(omegas)) // 2 ** d if d else 0
+            if k not in seen and k < len(omegas):
+                seen.add(k)
+                order.append(k)
+    order += [k for k in range(len(omegas)) if k not in seen]
     for s in range(args.steps):
-        # the K steps spread over the sweep, as on the GPU
-        om = float(omegas[(s * len(omegas)) // max(args.steps, 1)])
+        om = float(omegas[order[s % len(order)]])
         sec, part = cpu_frequency(oc, om, betas, threads)
         per.append(sec)
         parts.append(part)

@@ -255,8 +255,19 @@ int gemm_tf32(cudaStream_t st, int m, int n, int k, float alpha, const float* A,
   if (k <= 0 || (reinterpret_cast<uintptr_t>(A) & 15) || (reinterpret_cast<uintptr_t>(B) & 15) || (lda & 3) ||
       (ldb & 3) || lda < k || ldb < k)
     return 1;
-  if (cudaFuncSetAttribute(k_gemm_tf32, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes) != cudaSuccess)
-    return 1;
+  // the shared-memory opt-in, once per device
+  static std::mutex mu;
+  static bool attr_set[64] = {};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 1;
+  {
+    std::lock_guard<std::mutex> lock(mu);
+    if (!attr_set[dev]) {
+      if (cudaFuncSetAttribute(k_gemm_tf32, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes) != cudaSuccess)
+        return 1;
+      attr_set[dev] = true;
+    }
+  }
   CUtensorMap ta, tb;
   if (!make_map(&ta, A, k, m, lda, kBM) || !make_map(&tb, B, k, n, ldb, kBN)) return 1;
   dim3 grid((unsigned)((m + kBM - 1) / kBM), (unsigned)((n + kBN - 1) / kBN));

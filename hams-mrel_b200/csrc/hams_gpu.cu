@@ -168,6 +168,71 @@ __global__ void k_bin_offsets(const uint32_t* __restrict__ keys, long long np, i
 // in green_series.cu.
 // EIGEN runs at 8 blocks per SM like the series kernels; LINTON's adaptive
 // quadrature keeps its registers.
+// ---------------------------------------------------------------------------
+// the series' judgement of the surrogate
+// ---------------------------------------------------------------------------
+// dst[k] = src[k * stride], k < count
+__global__ void k_stride_pick(const uint32_t* __restrict__ src, long long count, long long stride,
+                              uint32_t* __restrict__ dst) {
+  const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < count) dst[k] = src[k * stride];
+}
+
+// the A and S entries of the listed pairs: out[k] = A[p_k], out[ns + k] = S[p_k]
+__global__ void k_gather_pairs(const uint32_t* __restrict__ list, int ns, const double2* __restrict__ A,
+                               const double2* __restrict__ S, double2* __restrict__ out) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= ns) return;
+  out[k] = A[list[k]];
+  out[ns + k] = S[list[k]];
+}
+
+// out = {sum |A1 - A2|^2, sum (Re A2)^2, sum |S1 - S2|^2, sum (Re S2)^2} over the samples (one CTA)
+__global__ void __launch_bounds__(1024) k_sample_err(const double2* __restrict__ g1, const double2* __restrict__ g2,
+                                                     int ns, double* __restrict__ out) {
+  __shared__ double red[4][32];
+  double v[4] = {0.0, 0.0, 0.0, 0.0};
+  for (int k = threadIdx.x; k < ns; k += blockDim.x) {
+    const double2 a1 = g1[k], a2 = g2[k], s1 = g1[ns + k], s2 = g2[ns + k];
+    v[0] += (a1.x - a2.x) * (a1.x - a2.x) + (a1.y - a2.y) * (a1.y - a2.y);
+    v[1] += a2.x * a2.x;
+    v[2] += (s1.x - s2.x) * (s1.x - s2.x) + (s1.y - s2.y) * (s1.y - s2.y);
+    v[3] += s2.x * s2.x;
+  }
+  for (int q = 0; q < 4; ++q) {
+    for (int o = 16; o; o >>= 1) v[q] += __shfl_xor_sync(0xffffffffu, v[q], o);
+    if ((threadIdx.x & 31) == 0) red[q][threadIdx.x >> 5] = v[q];
+  }
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    for (int q = 0; q < 4; ++q) {
+      double x = threadIdx.x < (blockDim.x >> 5) ? red[q][threadIdx.x] : 0.0;
+      for (int o = 16; o; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+      if (threadIdx.x == 0) out[q] = x;
+    }
+  }
+}
+
+// The sensitivity probe: in place, every pair the surrogate evaluates (the
+// criterion of k_pair_keys' bins 4 and 5, copied body blocks included)
+// becomes eps times the real part of its A and S entries, every other pair 0.
+__global__ void k_probe_far(DevGeom g, double h, double far, double eps, double2* __restrict__ A,
+                            double2* __restrict__ S) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y;
+  if (i >= g.tn) return;
+  const size_t p = (size_t)i + (size_t)j * g.tn;
+  const double dx = g.xq[j] - g.fxyz[i], dy = g.xq[j + g.n] - g.fxyz[i + g.tn];
+  const double rr = sqrt(dx * dx + dy * dy);
+  const int b = hams::fin_branch(rr, h);
+  bool on = false;
+  if (b == hams::kEigenE || b == hams::kEigen) {
+    const double zq = g.xq[j + 2 * g.n], zp = g.fxyz[i + 2 * g.tn], dz = zq - zp;
+    on = sqrt(dx * dx + dy * dy + dz * dz) > far * g.pnsz[j] && sg::in_domain(rr / h, (zq + h) / h, (zp + h) / h, sg::kKmin);
+  }
+  A[p] = make_double2(on ? eps * A[p].x : 0.0, 0.0);
+  S[p] = make_double2(on ? eps * S[p].x : 0.0, 0.0);
+}
+
 template <int BR>
 __global__ void __launch_bounds__(128, BR == hams::kEigen ? 8 : 1) k_green_fin(DevGeom g, WaveDev w, const double* __restrict__ wvn,
                                                    hams::ModeTab mt, const uint32_t* __restrict__ pairs,
@@ -656,7 +721,8 @@ struct hams_ctx {
   cudaEvent_t ev[6] = {};
   cudaEvent_t evb[6] = {};
   cudaEvent_t evf = nullptr;
-  static constexpr int kTimings = 20;
+  cudaEvent_t evc = nullptr;  // start of the last solve_one
+  static constexpr int kTimings = 28;
   double last_ms[kTimings] = {};
   std::atomic<long long> launches{0};   // kernels of this library
   std::atomic<long long> lib_calls{0};  // cuBLAS / cuSOLVER / CUB calls
@@ -676,6 +742,14 @@ struct hams_ctx {
   SgDev sgd{};
   int sms = 148;
   int sg_used = 0;  // the last solve evaluated its far pairs with the surrogate
+  // the series' judgement of the surrogate (hams_ctx_set_surrogate_tolerance):
+  // sampled far pairs evaluated both ways, the outputs' sensitivity probe
+  double sg_tol = 0.0;
+  DBuf<uint32_t> sg_samp;  // sampled surrogate pairs: sg_ns4 of bin 4, then sg_ns5 of bin 5
+  int sg_ns4 = 0, sg_ns5 = 0;
+  DBuf<double2> sg_g1, sg_g2;  // the sampled A and S entries from the network, then from the series
+  DBuf<double> sg_red, outbuf2;
+  double sg_judge[8] = {};  // e_A, e_S, kappa_A, kappa_B, kappa_X, estimate, re-solved with the series, samples
   std::string note;  // what the last solve changed on its own (fallbacks), or empty
   bool unfolded = false;  // built from a half mesh (ISX or ISY = 1), see unfold_symmetry
 };
@@ -717,6 +791,7 @@ extern "C" void hams_ctx_destroy(hams_ctx* c) {
   for (auto& e : c->marks)
     if (e) cudaEventDestroy(e);
   if (c->evf) cudaEventDestroy(c->evf);
+  if (c->evc) cudaEventDestroy(c->evc);
   if (c->solver) cusolverDnDestroy(c->solver);
   if (c->blas) cublasDestroy(c->blas);
   if (c->st) cudaStreamDestroy(c->st);
@@ -900,6 +975,7 @@ static int ctx_handles(hams_ctx* c) {
   for (auto& e : c->evb) CU(cudaEventCreate(&e));
   for (auto& e : c->marks) CU(cudaEventCreate(&e));
   CU(cudaEventCreate(&c->evf));
+  CU(cudaEventCreate(&c->evc));
   return 0;
 }
 
@@ -936,6 +1012,10 @@ static int make_lane(hams_ctx* c, hams_ctx** out) {
     l->sg_kmin = c->sg_kmin;
     l->sg_kmax = c->sg_kmax;
     l->sgd = c->sgd;
+    l->sg_tol = c->sg_tol;
+    l->sg_samp.view(c->sg_samp);
+    l->sg_ns4 = c->sg_ns4;
+    l->sg_ns5 = c->sg_ns5;
     l->sms = c->sms;
     l->chunks_h = c->chunks_h;
     rc = ctx_frequency_buffers(l);
@@ -1100,8 +1180,10 @@ static WaveDev wave_dev(const hams_ctx* c, const hams_wave* w) {
   return d;
 }
 
-// Assemble A (tn x n) and the right-hand sides B (tn x (6nb+nbeta)) on the device.
-static int assemble_dev(hams_ctx* c, const hams_wave* w, int nbeta) {
+// Assemble A (tn x n) and the right-hand sides B (tn x (6nb+nbeta)) on the
+// device; force_series keeps the series for the far pairs of a surrogate
+// context (the re-solve of a frequency the series judged).
+static int assemble_dev(hams_ctx* c, const hams_wave* w, int nbeta, bool force_series = false) {
   const int n = c->n, tn = c->tn, nb = c->nb, nrhs = 6 * nb + nbeta;
   WaveDev wd = wave_dev(c, w);
   if (c->opts.depth >= 0.0 && !wd.limit) CU(cudaMemcpyAsync(c->wvn.p, w->wvn, HAMS_NK * 8, cudaMemcpyHostToDevice, c->st));
@@ -1137,12 +1219,34 @@ static int assemble_dev(hams_ctx* c, const hams_wave* w, int nbeta) {
     const long long cs = c->bin_off[6] - c->bin_off[4];
     const double hh = c->opts.depth, K = wd.wk * hh * tanh(wd.wk * hh);
     if (cs > 0) {
-      if (!wd.limit && K >= c->sg_kmin && K <= c->sg_kmax) {
+      if (!force_series && !wd.limit && K >= c->sg_kmin && K <= c->sg_kmax) {
         if (launch_green_sg(c->st, c->sms, c->g, wd, c->sgd, c->mt, K, c->pairs.p + c->bin_off[4], cs, c->rs.p,
                             c->rd.p, c->A.p, c->S.p, c->ovf.p))
           return fail(HAMS_ERR_CUDA, "surrogate kernel launch failed");
         c->launches += 1;
         c->sg_used = 1;
+        const int ns = c->sg_ns4 + c->sg_ns5;
+        if (c->sg_tol > 0.0 && ns > 0) {
+          // the sampled far pairs: the network's entries, then the series' over them (the entries of A
+          // and S at the samples end up from the series)
+          TRY(c->sg_g1.alloc(2 * (size_t)ns));
+          TRY(c->sg_g2.alloc(2 * (size_t)ns));
+          TRY(c->sg_red.alloc(4));
+          const unsigned gb = (unsigned)((ns + 255) / 256);
+          k_gather_pairs<<<gb, 256, 0, c->st>>>(c->sg_samp.p, ns, c->A.p, c->S.p, c->sg_g1.p);
+          TRY(launch_check(c));
+          if (c->sg_ns4 > 0)
+            launch_green_series(hams::kEigenE, (unsigned)((c->sg_ns4 + 127) / 128), c->st, c->g, wd, c->wvn.p, c->mt,
+                                c->sg_samp.p, c->sg_ns4, c->rs.p, c->rd.p, c->A.p, c->S.p, c->ovf.p);
+          if (c->sg_ns5 > 0)
+            k_green_fin<3><<<(unsigned)((c->sg_ns5 + 127) / 128), 128, 0, c->st>>>(
+                c->g, wd, c->wvn.p, c->mt, c->sg_samp.p + c->sg_ns4, c->sg_ns5, c->rs.p, c->rd.p, c->A.p, c->S.p,
+                c->ovf.p);
+          TRY(launch_check(c, (c->sg_ns4 > 0) + (c->sg_ns5 > 0)));
+          k_gather_pairs<<<gb, 256, 0, c->st>>>(c->sg_samp.p, ns, c->A.p, c->S.p, c->sg_g2.p);
+          k_sample_err<<<1, 1024, 0, c->st>>>(c->sg_g1.p, c->sg_g2.p, ns, c->sg_red.p);
+          TRY(launch_check(c, 2));
+        }
       } else {
         long long ce = c->bin_off[5] - c->bin_off[4], cg = c->bin_off[6] - c->bin_off[5];
         if (ce > 0)
@@ -1636,17 +1740,125 @@ static int field_dev(hams_ctx* c, const hams_wave* w, int nbeta) {
   return 0;
 }
 
+// Xf (n x nrhs) <- (L U)^-1 Xf with the factors the last mixed solve left in Af.
+static int mixed_apply(hams_ctx* c, int nrhs) {
+  const int n = c->n, lda = mixed_lu_ld(n);
+  if (c->lu_used == HAMS_LU_LIBRARY) {
+    CUS(cusolverDnCgetrs(c->solver, CUBLAS_OP_N, n, nrhs, (cuComplex*)c->Af.p, lda, c->ipiv.p, (cuComplex*)c->Xf.p, n,
+                         c->info.p));
+    c->lib_calls += 1;
+    return 0;
+  }
+  long long la = 0;
+  const int rc = mixed_lu_solve(c->st, n, lda, nrhs, c->Af.p, c->perm.p, c->Xf.p, c->luw.p, c->info.p + 1, &la);
+  c->launches += la;
+  if (rc) return fail(HAMS_ERR_CUDA, "block LU solve failed");
+  return 0;
+}
+
+// Safety factor of the judgement: the largest ratio of a frequency's true
+// error (against the plain series) to its estimate e kappa, observed on the
+// 5,400-panel 3 x 3 array of cylinders (h = 50 m) over 0.2-2.5 rad/s, rounded up.
+constexpr double kJudgeSafety = 1.0;
+
+// The series' judgement of a frequency solved with the surrogate: an estimate
+// of the surrogate's relative error in added mass, damping and excitation.
+//   e      the network's relative error on the far-pair entries of A and S,
+//          from the pairs sampled during the assembly (k_sample_err);
+//   kappa  the outputs' sensitivity to the far-pair entries: every entry the
+//          network produced is perturbed by eps of its real part (the part
+//          the network changes), and the first-order change of the solution,
+//          dX = (L U)^-1 (dB - dA X), is carried through the force
+//          reductions; kappa = |output change| / (eps |output|) per output.
+// The estimate is kJudgeSafety e max(kappa).  A and S are overwritten (the
+// frequency does not read them again).  Requires the mixed solve's factors.
+static int surrogate_judge(hams_ctx* c, const hams_wave* w, int nbeta) {
+  const int n = c->n, tn = c->tn, nb = c->nb, ndof = 6 * nb, nrhs = ndof + nbeta;
+  const double eps = 1e-3;
+  const cuDoubleComplex one = make_cuDoubleComplex(1.0, 0.0), mone = make_cuDoubleComplex(-1.0, 0.0);
+  WaveDev wd = wave_dev(c, w);
+  k_probe_far<<<dim3((tn + 127) / 128, n), 128, 0, c->st>>>(c->g, c->opts.depth, c->sg_far, eps, c->A.p, c->S.p);
+  TRY(launch_check(c));
+  // dB: the right-hand sides of the probe's S (this frequency's diffraction weights are still in wd)
+  const int nch = (int)c->chunks_h.size();
+  k_rhs_partial<<<dim3((tn + 127) / 128, nch), 128, 0, c->st>>>(c->g, c->S.p, c->chunks.p, c->wd.p, nbeta, c->part.p);
+  k_rhs_final<<<(tn + 127) / 128, 128, 0, c->st>>>(tn, nb, nch, c->chunk_body.p, c->part.p, nbeta, c->B.p);
+  TRY(launch_check(c, 2));
+  // r = dB - dA X, then dX = (L U)^-1 r
+  CUB_(cublasZgemm(c->blas, CUBLAS_OP_N, CUBLAS_OP_N, n, nrhs, n, &mone, (cuDoubleComplex*)c->A.p, tn,
+                   (cuDoubleComplex*)c->X.p, n, &one, (cuDoubleComplex*)c->B.p, tn));
+  c->lib_calls += 1;
+  const size_t nx = (size_t)n * nrhs;
+  k_z2c<<<592, 256, 0, c->st>>>(c->B.p, c->Xf.p, nx);  // tn == n: B is n x nrhs, contiguous
+  TRY(launch_check(c));
+  TRY(mixed_apply(c, nrhs));
+  TRY(c->R.alloc(nx));
+  CU(cudaMemcpyAsync(c->R.p, c->X.p, nx * 16, cudaMemcpyDeviceToDevice, c->st));
+  k_c2z_add<<<592, 256, 0, c->st>>>(c->Xf.p, c->R.p, nx);
+  TRY(launch_check(c));
+  const size_t tot = 2 * (size_t)ndof * ndof + 2 * (size_t)ndof * std::max(nbeta, 1);
+  TRY(c->outbuf2.alloc(tot));
+  IncWave q = inc_params(wd, c->opts.amp, c->opts.g, c->opts.xw[0], c->opts.xw[1]);
+  double* a2 = c->outbuf2.p;
+  k_forces<<<dim3(nb, 6, nrhs), 256, 0, c->st>>>(c->g, wd, q, c->beta.p, nbeta, c->opts.isol, c->opts.rho, c->R.p,
+                                                 c->n, a2, a2 + (size_t)ndof * ndof,
+                                                 (double2*)(a2 + 2 * (size_t)ndof * ndof));
+  TRY(launch_check(c));
+  std::vector<double> o1(tot), o2(tot);
+  double red[4] = {0.0, 0.0, 0.0, 0.0};
+  CU(cudaMemcpyAsync(o1.data(), c->outbuf.p, tot * 8, cudaMemcpyDeviceToHost, c->st));
+  CU(cudaMemcpyAsync(o2.data(), c->outbuf2.p, tot * 8, cudaMemcpyDeviceToHost, c->st));
+  CU(cudaMemcpyAsync(red, c->sg_red.p, 4 * 8, cudaMemcpyDeviceToHost, c->st));
+  CU(cudaStreamSynchronize(c->st));
+  auto kappa = [&](size_t off, size_t cnt) {
+    double d = 0.0, r = 0.0;
+    for (size_t e = off; e < off + cnt; ++e) {
+      d += (o2[e] - o1[e]) * (o2[e] - o1[e]);
+      r += o1[e] * o1[e];
+    }
+    return r > 0.0 ? std::sqrt(d / r) / eps : 0.0;
+  };
+  const size_t na = (size_t)ndof * ndof;
+  double* j = c->sg_judge;
+  j[0] = red[1] > 0.0 ? std::sqrt(red[0] / red[1]) : 0.0;
+  j[1] = red[3] > 0.0 ? std::sqrt(red[2] / red[3]) : 0.0;
+  j[2] = kappa(0, na);
+  j[3] = kappa(na, na);
+  j[4] = nbeta > 0 ? kappa(2 * na, 2 * (size_t)ndof * nbeta) : 0.0;
+  j[5] = kJudgeSafety * std::max(j[0], j[1]) * std::max(j[2], std::max(j[3], j[4]));
+  j[7] = (double)(c->sg_ns4 + c->sg_ns5);
+  return 0;
+}
+
 static int solve_one(hams_ctx* c, const hams_wave* w, int nbeta, const double* beta, double* amas, double* bdmp,
                      double* exfc) {
   const int ndof = 6 * c->nb;
   if (nbeta < 0) return fail(HAMS_ERR_ARG, "nbeta < 0");
   TRY(c->beta.alloc(std::max(nbeta, 1)));
   if (nbeta > 0) CU(cudaMemcpyAsync(c->beta.p, beta, (size_t)nbeta * 8, cudaMemcpyHostToDevice, c->st));
+  CU(cudaEventRecord(c->evc, c->st));
+  for (double& v : c->sg_judge) v = 0.0;
   TRY(assemble_dev(c, w, nbeta));
   int info = 0;
   TRY(solve_dev(c, ndof + nbeta, &info));
   CU(cudaEventRecord(c->ev[3], c->st));
   TRY(forces_dev(c, w, nbeta));
+  if (c->sg_used && c->sg_tol > 0.0 && c->sg_ns4 + c->sg_ns5 > 0 && c->opts.precision == HAMS_PREC_MIXED &&
+      c->opts.solver != HAMS_SOLVER_GMRES && c->nl == 0) {
+    TRY(surrogate_judge(c, w, nbeta));
+    if (c->sg_judge[5] > c->sg_tol) {  // the series takes this frequency
+      const std::string keep = c->note;
+      TRY(assemble_dev(c, w, nbeta, true));
+      TRY(solve_dev(c, ndof + nbeta, &info));
+      CU(cudaEventRecord(c->ev[3], c->st));
+      TRY(forces_dev(c, w, nbeta));
+      c->sg_judge[6] = 1.0;
+      char buf[160];
+      std::snprintf(buf, sizeof buf, "surrogate estimate %.2e > %.2e: re-solved with the series", c->sg_judge[5],
+                    c->sg_tol);
+      c->note = keep.empty() ? std::string(buf) : keep + "; " + buf;
+    }
+  }
   if (c->nfp > 0) TRY(field_dev(c, w, nbeta));
   CU(cudaEventRecord(c->ev[4], c->st));
   double* o = c->outbuf.p;
@@ -1663,7 +1875,7 @@ static int solve_one(hams_ctx* c, const hams_wave* w, int nbeta, const double* b
   cudaEventElapsedTime(&ms, c->ev[1], c->ev[2]); c->last_ms[1] = ms;
   cudaEventElapsedTime(&ms, c->ev[2], c->ev[3]); c->last_ms[2] = ms;
   cudaEventElapsedTime(&ms, c->ev[3], c->ev[4]); c->last_ms[3] = ms;
-  cudaEventElapsedTime(&ms, c->ev[0], c->ev[5]); c->last_ms[4] = ms;
+  cudaEventElapsedTime(&ms, c->evc, c->ev[5]); c->last_ms[4] = ms;
   for (int b = 0; b < 4; ++b) {
     c->last_ms[5 + b] = 0.0;
     c->last_ms[11 + b] = (double)(c->bin_off[b + 1] - c->bin_off[b]);
@@ -1678,6 +1890,7 @@ static int solve_one(hams_ctx* c, const hams_wave* w, int nbeta, const double* b
   c->last_ms[17] = c->sg_used ? (double)(c->bin_off[6] - c->bin_off[4]) : 0.0;
   c->last_ms[18] = c->opts.precision == HAMS_PREC_MIXED ? c->ir_rate : 0.0;
   c->last_ms[19] = (double)c->blk_pairs;
+  for (int k = 0; k < 8; ++k) c->last_ms[20 + k] = c->sg_judge[k];
   if (ovf & 2) return fail(HAMS_ERR_CUDA, "surrogate kernel: a tensor-core completion wait gave up");
   if (ovf) return fail(HAMS_ERR_NUMERIC, "adaptive quadrature stack overflow in the LINTON branch");
   if (info > 0) return info;  // singular pivot, LAPACK style
@@ -1913,6 +2126,39 @@ extern "C" int hams_ctx_set_surrogate_range(hams_ctx* c, double kmin, double kma
   return 0;
 }
 
+extern "C" int hams_ctx_set_surrogate_tolerance(hams_ctx* c, double tol) {
+  g_err.clear();
+  if (!c || c->is_lane) return fail(HAMS_ERR_ARG, "null context");
+  if (!(tol >= 0.0)) return fail(HAMS_ERR_ARG, "tolerance must be >= 0");
+  if (cudaSetDevice(c->dev) != cudaSuccess) return fail(HAMS_ERR_CUDA, "cudaSetDevice failed");
+  for (hams_ctx* l : c->lanes) CU(cudaStreamSynchronize(l->st));
+  CU(cudaStreamSynchronize(c->st));
+  c->sg_tol = tol;
+  for (hams_ctx* l : c->lanes) l->sg_tol = tol;
+  return 0;
+}
+
+// The pairs the judgement samples: every stride-th pair of the surrogate's
+// bins (sorted by series length, so the sample spans every length), about
+// kJudgeSamples in all.
+constexpr long long kJudgeSamples = 16384;
+static int build_judge_samples(hams_ctx* c) {
+  c->sg_ns4 = c->sg_ns5 = 0;
+  const long long c4 = c->bin_off[5] - c->bin_off[4], c5 = c->bin_off[6] - c->bin_off[5];
+  if (!c->sg_on || c4 + c5 <= 0) return 0;
+  const long long stride = std::max(1LL, (c4 + c5) / kJudgeSamples);
+  const long long n4 = (c4 + stride - 1) / stride, n5 = (c5 + stride - 1) / stride;
+  TRY(c->sg_samp.alloc((size_t)std::max(n4 + n5, 1LL)));
+  if (n4 > 0) k_stride_pick<<<(unsigned)((n4 + 255) / 256), 256, 0, c->st>>>(c->pairs.p + c->bin_off[4], n4, stride, c->sg_samp.p);
+  if (n5 > 0)
+    k_stride_pick<<<(unsigned)((n5 + 255) / 256), 256, 0, c->st>>>(c->pairs.p + c->bin_off[5], n5, stride,
+                                                                 c->sg_samp.p + n4);
+  TRY(launch_check(c, (n4 > 0) + (n5 > 0)));
+  c->sg_ns4 = (int)n4;
+  c->sg_ns5 = (int)n5;
+  return 0;
+}
+
 extern "C" int hams_ctx_set_surrogate(hams_ctx* c, const float* params, int32_t nparams, double far_factor) {
   g_err.clear();
   if (!c || c->is_lane) return fail(HAMS_ERR_ARG, "null context");
@@ -1946,6 +2192,7 @@ extern "C" int hams_ctx_set_surrogate(hams_ctx* c, const float* params, int32_t 
     c->sg_on = 0;
   }
   TRY(build_pairs(c));
+  TRY(build_judge_samples(c));
   int nmode = c->mt.nmode;
   if (c->bin_off[3] > c->bin_off[2] || c->bin_off[5] > c->bin_off[4]) nmode = std::max(nmode, hams::kEigenEMax + 1);
   c->mt.nmode = nmode;
@@ -1957,6 +2204,9 @@ extern "C" int hams_ctx_set_surrogate(hams_ctx* c, const float* params, int32_t 
     l->sg_kmin = c->sg_kmin;
     l->sg_kmax = c->sg_kmax;
     l->sgd = c->sgd;
+    l->sg_samp.view(c->sg_samp);
+    l->sg_ns4 = c->sg_ns4;
+    l->sg_ns5 = c->sg_ns5;
     l->mt.nmode = nmode;
   }
   return 0;

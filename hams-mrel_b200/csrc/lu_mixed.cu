@@ -313,6 +313,9 @@ __device__ __forceinline__ float2 csub_mul(float2 s, float2 a, float2 b) {
 // blocks in increasing order, the right-hand sides gathered through perm
 // from B; upper: U, blocks in decreasing order, B unpermuted.  X receives
 // the solution (n x nrhs, ld n).  flags (nblk x nch) and ticket start at 0.
+// The grid is small and persistent: each CTA takes tickets (block row and
+// chunk, in dependency order) until none is left, so CTAs that wait for an
+// earlier block hold few SMs.
 __global__ void __launch_bounds__(256) k_trsm_block(const float2* __restrict__ A, int lda, int n, int nrhs, int nblk,
                                                     int nch, bool lower, const float2* __restrict__ invc,
                                                     const int* __restrict__ perm, const float2* __restrict__ B,
@@ -323,83 +326,87 @@ __global__ void __launch_bounds__(256) k_trsm_block(const float2* __restrict__ A
   float2* sAcc = sX + kNB * kNC;      // B_b - sum, the operand of the inverse
   __shared__ int s_id, s_abort;
   const int tid = threadIdx.x;
-  if (tid == 0) {
-    s_id = (int)atomicAdd(ticket, 1u);
-    s_abort = 0;
-  }
-  __syncthreads();
-  const int order = s_id / nch, ch = s_id % nch;
-  const int b = lower ? order : nblk - 1 - order;
-  const int q0 = ch * kNC, r = tid % kNB, qq = (tid / kNB) * 4;  // this thread: row r, chunk columns qq..qq+3
-  const int row = b * kNB + r;
-  // the block's right-hand sides
-  for (int e = tid; e < kNB * kNC; e += 256) {
-    const int rr = e % kNB, q = e / kNB, gr = b * kNB + rr;
-    float2 v = make_float2(0.0f, 0.0f);
-    if (gr < n && q0 + q < nrhs) v = B[(size_t)(q0 + q) * n + (lower ? perm[gr] : gr)];
-    sAcc[q * kNB + rr] = v;
-  }
-  __syncthreads();
-  float2 acc[4];
-  for (int u = 0; u < 4; ++u) acc[u] = make_float2(0.0f, 0.0f);
-  for (int step = 0; step < order; ++step) {
-    const int j = lower ? step : nblk - 1 - step;
-    // the off-diagonal block T = A[b rows, j columns], read while the flag is awaited
-    for (int e = tid; e < kNB * kNB; e += 256) {
-      const int rr = e % kNB, cc = e / kNB, gr = b * kNB + rr, gc = j * kNB + cc;
-      sT[cc * (kNB + 1) + rr] = (gr < n && gc < n) ? A[(size_t)gc * lda + gr] : make_float2(0.0f, 0.0f);
-    }
+  for (;;) {
+    __syncthreads();  // the previous ticket's shared data is no longer read
     if (tid == 0) {
-      const volatile int* f = flags + j * nch + ch;
-      long long it = 0;
-      while (*f == 0) {
-        if (++it > kFlagSpin) {
-          atomicOr(err, 2);
-          s_abort = 1;
-          break;
-        }
-        __nanosleep(64);
-      }
-      __threadfence();
+      s_id = (int)atomicAdd(ticket, 1u);
+      s_abort = 0;
     }
     __syncthreads();
-    if (s_abort) break;
+    if (s_id >= nblk * nch) return;
+    const int order = s_id / nch, ch = s_id % nch;
+    const int b = lower ? order : nblk - 1 - order;
+    const int q0 = ch * kNC, r = tid % kNB, qq = (tid / kNB) * 4;  // this thread: row r, chunk columns qq..qq+3
+    const int row = b * kNB + r;
+    // the block's right-hand sides
     for (int e = tid; e < kNB * kNC; e += 256) {
-      const int rr = e % kNB, q = e / kNB, gr = j * kNB + rr;
-      sX[q * kNB + rr] =
-          (gr < n && q0 + q < nrhs) ? __ldcg(X + (size_t)(q0 + q) * n + gr) : make_float2(0.0f, 0.0f);
+      const int rr = e % kNB, q = e / kNB, gr = b * kNB + rr;
+      float2 v = make_float2(0.0f, 0.0f);
+      if (gr < n && q0 + q < nrhs) v = B[(size_t)(q0 + q) * n + (lower ? perm[gr] : gr)];
+      sAcc[q * kNB + rr] = v;
     }
     __syncthreads();
-#pragma unroll 4
+    float2 acc[4];
+    for (int u = 0; u < 4; ++u) acc[u] = make_float2(0.0f, 0.0f);
+    for (int step = 0; step < order; ++step) {
+      const int j = lower ? step : nblk - 1 - step;
+      // the off-diagonal block T = A[b rows, j columns], read while the flag is awaited
+      for (int e = tid; e < kNB * kNB; e += 256) {
+        const int rr = e % kNB, cc = e / kNB, gr = b * kNB + rr, gc = j * kNB + cc;
+        sT[cc * (kNB + 1) + rr] = (gr < n && gc < n) ? A[(size_t)gc * lda + gr] : make_float2(0.0f, 0.0f);
+      }
+      if (tid == 0) {
+        const volatile int* f = flags + j * nch + ch;
+        long long it = 0;
+        while (*f == 0) {
+          if (++it > kFlagSpin) {
+            atomicOr(err, 2);
+            s_abort = 1;
+            break;
+          }
+          __nanosleep(64);
+        }
+        __threadfence();
+      }
+      __syncthreads();
+      if (s_abort) break;
+      for (int e = tid; e < kNB * kNC; e += 256) {
+        const int rr = e % kNB, q = e / kNB, gr = j * kNB + rr;
+        sX[q * kNB + rr] =
+            (gr < n && q0 + q < nrhs) ? __ldcg(X + (size_t)(q0 + q) * n + gr) : make_float2(0.0f, 0.0f);
+      }
+      __syncthreads();
+  #pragma unroll 4
+      for (int k = 0; k < kNB; ++k) {
+        const float2 t = sT[k * (kNB + 1) + r];
+  #pragma unroll
+        for (int u = 0; u < 4; ++u) acc[u] = csub_mul(acc[u], t, sX[(qq + u) * kNB + k]);
+      }
+      __syncthreads();
+    }
+    // X_b = T_bb^-1 (B_b - sum)
+    for (int u = 0; u < 4; ++u) {
+      float2& s = sAcc[(qq + u) * kNB + r];
+      s = make_float2(s.x + acc[u].x, s.y + acc[u].y);
+    }
+    const float2* inv = invc + (size_t)b * kNB * kNB;
+    for (int e = tid; e < kNB * kNB; e += 256) sT[(e / kNB) * (kNB + 1) + e % kNB] = inv[e];
+    __syncthreads();
+    float2 out[4];
+    for (int u = 0; u < 4; ++u) out[u] = make_float2(0.0f, 0.0f);
+  #pragma unroll 4
     for (int k = 0; k < kNB; ++k) {
       const float2 t = sT[k * (kNB + 1) + r];
-#pragma unroll
-      for (int u = 0; u < 4; ++u) acc[u] = csub_mul(acc[u], t, sX[(qq + u) * kNB + k]);
+  #pragma unroll
+      for (int u = 0; u < 4; ++u) out[u] = csub_mul(out[u], t, sAcc[(qq + u) * kNB + k]);
     }
+    if (row < n)
+      for (int u = 0; u < 4; ++u)
+        if (q0 + qq + u < nrhs) X[(size_t)(q0 + qq + u) * n + row] = make_float2(-out[u].x, -out[u].y);
+    __threadfence();
     __syncthreads();
+    if (tid == 0) atomicExch(flags + b * nch + ch, 1);  // published (also after an abandoned wait, so no CTA hangs)
   }
-  // X_b = T_bb^-1 (B_b - sum)
-  for (int u = 0; u < 4; ++u) {
-    float2& s = sAcc[(qq + u) * kNB + r];
-    s = make_float2(s.x + acc[u].x, s.y + acc[u].y);
-  }
-  const float2* inv = invc + (size_t)b * kNB * kNB;
-  for (int e = tid; e < kNB * kNB; e += 256) sT[(e / kNB) * (kNB + 1) + e % kNB] = inv[e];
-  __syncthreads();
-  float2 out[4];
-  for (int u = 0; u < 4; ++u) out[u] = make_float2(0.0f, 0.0f);
-#pragma unroll 4
-  for (int k = 0; k < kNB; ++k) {
-    const float2 t = sT[k * (kNB + 1) + r];
-#pragma unroll
-    for (int u = 0; u < 4; ++u) out[u] = csub_mul(out[u], t, sAcc[(qq + u) * kNB + k]);
-  }
-  if (row < n)
-    for (int u = 0; u < 4; ++u)
-      if (q0 + qq + u < nrhs) X[(size_t)(q0 + qq + u) * n + row] = make_float2(-out[u].x, -out[u].y);
-  __threadfence();
-  __syncthreads();
-  if (tid == 0) atomicExch(flags + b * nch + ch, 1);  // published (also after an abandoned wait, so no CTA hangs)
 }
 
 // ---------------------------------------------------------------------------
@@ -570,7 +577,9 @@ int mixed_lu_solve(cudaStream_t st, int n, int lda, int nrhs, const float2* A, c
   float2* T = (float2*)(ws + L.T);
   int* flags = (int*)(ws + L.flags);
   unsigned int* ticket = (unsigned int*)(flags + nblk * nch);
-  const unsigned grid = (unsigned)(nblk * nch);
+  // a few CTAs per chunk column: enough to overlap the block rows' sums, few
+  // enough that waiting CTAs leave the GPU to the other frequencies in flight
+  const unsigned grid = (unsigned)std::min(nblk * nch, 8 * nch);
   // forward: T = L^-1 P X; backward: X = U^-1 T
   if (cudaMemsetAsync(flags, 0, (size_t)(nblk * nch + 1) * sizeof(int), st) != cudaSuccess) return 1;
   k_trsm_block<<<grid, 256, kTrsmSmem, st>>>(A, lda, n, nrhs, nblk, nch, true, invLc, perm, X, T, flags, ticket,

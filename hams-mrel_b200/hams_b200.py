@@ -98,6 +98,7 @@ def load_library(path=LIB_PATH):
     lib.hams_surrogate_param_count.restype = c_int
     lib.hams_ctx_set_surrogate.argtypes = [ctypes.c_void_p, P_flt, c_int, c_dbl]
     lib.hams_ctx_set_surrogate_range.argtypes = [ctypes.c_void_p, c_dbl, c_dbl]
+    lib.hams_ctx_set_surrogate_tolerance.argtypes = [ctypes.c_void_p, c_dbl]
     lib.hams_ctx_set_field_points.argtypes = [ctypes.c_void_p, c_int, P_dbl]
     lib.hams_field_potentials.argtypes = [ctypes.c_void_p, c_int, P_dbl]
     lib.hams_surrogate_samples.argtypes = [c_int, c_int, ctypes.c_uint64, c_int, P_dbl]
@@ -258,14 +259,16 @@ class Context:
 
     def timings(self):
         """Stage times of the last solve (ms), per-branch Green kernel times and pair counts."""
-        ms = np.zeros(20)
-        load_library().hams_last_timings(self._h, _d(ms), 20)
+        ms = np.zeros(28)
+        load_library().hams_last_timings(self._h, _d(ms), 28)
         return dict(green=ms[0], rhs=ms[1], solve=ms[2], forces=ms[3], total=ms[4], green_linton=ms[5],
                     green_pidcock=ms[6], green_eigene=ms[7], green_eigen=ms[8], factor=ms[9], refine_sweeps=int(ms[10]),
                     iterations=int(ms[10]),
                     pairs_linton=int(ms[11]), pairs_pidcock=int(ms[12]), pairs_eigene=int(ms[13]),
                     pairs_eigen=int(ms[14]), lu_used=int(ms[15]), green_surrogate=ms[16],
-                    pairs_surrogate=int(ms[17]), ir_rate=ms[18], pairs_copied=int(ms[19]))
+                    pairs_surrogate=int(ms[17]), ir_rate=ms[18], pairs_copied=int(ms[19]),
+                    judge_err_a=ms[20], judge_err_s=ms[21], judge_kappa=(ms[22], ms[23], ms[24]),
+                    judge_estimate=ms[25], judge_resolved=bool(ms[26]), judge_samples=int(ms[27]))
 
     def set_surrogate(self, params, far_factor=3.0, k_range=None):
         """Far pairs from the trained network (params float32), or the series again (params None);
@@ -278,6 +281,11 @@ class Context:
         _check(lib.hams_ctx_set_surrogate(self._h, _f(self._sg), self._sg.size, float(far_factor)))
         kmin, kmax = k_range if k_range is not None else (0.04, 40.0)
         _check(lib.hams_ctx_set_surrogate_range(self._h, float(kmin), float(kmax)))
+
+    def set_surrogate_tolerance(self, tol):
+        """The series judges each frequency the network serves; above tol the frequency is re-solved
+        with the series (0 switches the judgement off)."""
+        _check(load_library().hams_ctx_set_surrogate_tolerance(self._h, float(tol)))
 
     def set_field_points(self, xfp):
         """Field points (nfp, 3) whose potentials every later solve evaluates (None: off)."""
@@ -332,7 +340,7 @@ def diag_gemm_tf32(a, b, c=None, alpha=1.0, beta=0.0, c_rowmajor=False, device=0
     A[:, :k] = a
     B = np.zeros((n, ld), dtype=np.float32)  # column-major k x n
     B[:, :k] = b.T
-    C = np.zeros((m, n), dtype=np.float32) if c is None else np.asarray(c, dtype=np.float32)
+    C = np.zeros((m, n), dtype=np.float32) if c is None else np.array(c, dtype=np.float32)  # a copy
     Cbuf = np.ascontiguousarray(C) if c_rowmajor else np.ascontiguousarray(C.T)
     _check(load_library().hams_diag_gemm_tf32(device, m, n, k, alpha, _f(A), ld, _f(B), ld, beta, _f(Cbuf),
                                                n if c_rowmajor else m, int(c_rowmajor)))

@@ -279,6 +279,24 @@ int hams_ctx_set_surrogate(hams_ctx *ctx, const float *params, int32_t nparams, 
  * on the series. */
 int hams_ctx_set_surrogate_range(hams_ctx *ctx, double kmin, double kmax);
 
+/* The series judges the surrogate, frequency by frequency (no counterpart in
+ * the reference, which has no surrogate).  With tol > 0, every frequency the
+ * network serves (mixed precision, LU solver, no lids) is checked after its
+ * solve: the series re-evaluates a sample of about 16,000 far pairs, giving
+ * the network's relative error e on the far-pair entries of A and S, and a
+ * sensitivity probe (those entries perturbed in proportion, the first-order
+ * change carried through the factorisation already made and the force
+ * reductions) gives each output's amplification kappa.  When the estimate
+ * e kappa (times a safety factor calibrated on the 5,400-panel array)
+ * exceeds tol, the frequency is assembled again with the series and
+ * re-solved; hams_last_note says so and hams_last_timings reports the
+ * estimate.  The probe amplifies what the system amplifies: the long-wave
+ * damping (a small imaginary part of large potentials) and the bands around
+ * irregular frequencies, where the hand-picked K range of
+ * hams_ctx_set_surrogate_range would otherwise be needed.  tol = 0 (the
+ * default) switches the judgement off. */
+int hams_ctx_set_surrogate_tolerance(hams_ctx *ctx, double tol);
+
 /* Timing of the last solve in milliseconds: [0] Green/assembly kernels,
  * [1] right-hand sides, [2] factorisation + solves, [3] reductions,
  * [4] whole call, [5..8] Green kernels of the LINTON, PIDCOCK, EIGENE and
@@ -288,8 +306,14 @@ int hams_ctx_set_surrogate_range(hams_ctx *ctx, double kmin, double kmax);
  * (or the series standing in for it), [17] pairs the surrogate evaluated,
  * [18] the mixed form's largest residual reduction factor over one refinement
  * sweep (about the condition number times the factorisation's error),
- * [19] pairs copied from identical body blocks (hams_opts.body_blocks).
- * n is the capacity of ms (20 fills all). Returns the number written. */
+ * [19] pairs copied from identical body blocks (hams_opts.body_blocks),
+ * and, for a frequency the surrogate solved with a tolerance set
+ * (hams_ctx_set_surrogate_tolerance): [20] the network's sampled relative
+ * error on the far-pair entries of A, [21] of S, [22..24] the added mass',
+ * damping's and excitation's sensitivity to those entries, [25] the error
+ * estimate, [26] 1 if the frequency was re-solved with the series, [27] the
+ * pairs sampled.  n is the capacity of ms (28 fills all). Returns the number
+ * written. */
 int hams_last_timings(hams_ctx *ctx, double *ms, int32_t n);
 
 /* Field points (ControlFile Number_of_field_points, InputFiles.f90:193-203):
