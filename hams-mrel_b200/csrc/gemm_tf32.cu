@@ -23,28 +23,35 @@
 #include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
+#include <map>
 #include <mutex>
 
 #include "gemm_tf32.h"
 
 namespace {
 
-constexpr int kBM = 128, kBN = 128, kBK = 32;  // tile rows, columns, K panel (32 floats = one 128-byte row)
-constexpr int kStages = 3;
+constexpr int kBM = 128, kBK = 32;  // tile rows, K panel (32 floats = one 128-byte row)
 constexpr int kThreads = 192;
 constexpr int kABytes = kBM * kBK * 4;  // 16 KB per stage
-constexpr int kBBytes = kBN * kBK * 4;  // 16 KB per stage
-constexpr int kOffB = kStages * kABytes;
-constexpr int kOffBar = kOffB + kStages * kBBytes;  // full[kStages], empty[kStages], acc
-constexpr int kOffMisc = kOffBar + 8 * (2 * kStages + 1);
-constexpr int kSmemBytes = kOffMisc + 16 + 1024;  // + alignment slack of the dynamic window
 constexpr long long kSpin = 1ll << 22;
 
-// instruction descriptor, kind::tf32: D f32 (bit 4), A and B tf32 (format 2
-// at bits 7 and 10), both K-major, N >> 3 at bit 17, M >> 4 at bit 24
-constexpr uint32_t kIdesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(kBN >> 3) << 17) |
-                            ((uint32_t)(kBM >> 4) << 24);
+// Tile shape of one variant: BN columns of C per CTA (the MMA's N and the
+// tensor-memory columns), STAGES K panels in flight.  64 x 4 stages: 96 KB,
+// two CTAs per SM; 128 x 3: 97 KB, two CTAs; 256 x 3: 145 KB, one CTA.
+template <int BN, int STAGES>
+struct Tile {
+  static constexpr int kBBytes = BN * kBK * 4;
+  static constexpr int kOffB = STAGES * kABytes;
+  static constexpr int kOffBar = kOffB + STAGES * kBBytes;  // full[STAGES], empty[STAGES], acc
+  static constexpr int kOffMisc = kOffBar + 8 * (2 * STAGES + 1);
+  static constexpr int kSmemBytes = kOffMisc + 16 + 1024;  // + alignment slack of the dynamic window
+  // instruction descriptor, kind::tf32: D f32 (bit 4), A and B tf32 (format 2
+  // at bits 7 and 10), both K-major, N >> 3 at bit 17, M >> 4 at bit 24
+  static constexpr uint32_t kIdesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(BN >> 3) << 17) |
+                                     ((uint32_t)(kBM >> 4) << 24);
+};
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -88,9 +95,14 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&v)[16]) {
       : "r"(taddr));
 }
 
-__global__ void __launch_bounds__(kThreads, 2)
+template <int BN, int STAGES>
+__global__ void __launch_bounds__(kThreads, 1)
     k_gemm_tf32(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, float* __restrict__ C,
                 int ldc, int M, int N, int K, float alpha, float beta, int c_rowmajor, int* err) {
+  using T = Tile<BN, STAGES>;
+  constexpr int kBN = BN, kStages = STAGES, kBBytes = T::kBBytes, kOffB = T::kOffB, kOffBar = T::kOffBar,
+                kOffMisc = T::kOffMisc;
+  constexpr uint32_t kIdesc = T::kIdesc;
   extern __shared__ unsigned char smem_raw[];
   unsigned char* smem = smem_raw + ((1024 - (smem_u32(smem_raw) & 1023)) & 1023);  // 1024-aligned window
   const uint32_t sbase = smem_u32(smem);
@@ -183,6 +195,20 @@ __global__ void __launch_bounds__(kThreads, 2)
     }
   } else {  // epilogue: warps 2-5, warp w reads tensor-memory lanes 32 (w % 4) ...
     const int q = warp & 3, row = m0 + 32 * q + lane;
+    const bool live = row < M;
+    // C of one 16-column chunk into registers: all loads issued before any
+    // store of the tile, so they overlap (the first chunk's under the main loop)
+    auto load_chunk = [&](int c0, float (&cv)[16]) {
+#pragma unroll
+      for (int j = 0; j < 16; ++j) {
+        const int col = n0 + c0 + j;
+        cv[j] = (beta != 0.0f && live && col < N)
+                    ? (c_rowmajor ? C[(size_t)row * ldc + col] : C[(size_t)col * ldc + row])
+                    : 0.0f;
+      }
+    };
+    float cn[16];
+    load_chunk(0, cn);
     bool ok = mbar_wait(bar_acc, 0, abort_flag);
     if (!ok) {
       atomicOr(err, 1);
@@ -194,17 +220,20 @@ __global__ void __launch_bounds__(kThreads, 2)
       const uint32_t trow = tbase + ((uint32_t)(32 * q) << 16);
 #pragma unroll 1
       for (int c0 = 0; c0 < kBN; c0 += 16) {
+        float cc[16];
+#pragma unroll
+        for (int j = 0; j < 16; ++j) cc[j] = cn[j];
+        if (c0 + 16 < kBN) load_chunk(c0 + 16, cn);  // in flight while this chunk is written
         uint32_t v[16];
         tmem_ld16(trow + (uint32_t)c0, v);
         asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-        if (row < M) {
+        if (live) {
 #pragma unroll
           for (int j = 0; j < 16; ++j) {
             const int col = n0 + c0 + j;
             if (col < N) {
               float* dst = c_rowmajor ? C + (size_t)row * ldc + col : C + (size_t)col * ldc + row;
-              const float a = __uint_as_float(v[j]);
-              *dst = beta == 0.0f ? alpha * a : fmaf(alpha, a, beta * *dst);
+              *dst = fmaf(alpha, __uint_as_float(v[j]), beta * cc[j]);
             }
           }
         }
@@ -249,28 +278,163 @@ bool make_map(CUtensorMap* tm, const float* base, int k, int rows, int ld, int b
 
 }  // namespace
 
-int gemm_tf32(cudaStream_t st, int m, int n, int k, float alpha, const float* A, int lda, const float* B, int ldb,
-              float beta, float* C, int ldc, bool c_rowmajor, int* err) {
-  if (m <= 0 || n <= 0) return 0;
-  if (k <= 0 || (reinterpret_cast<uintptr_t>(A) & 15) || (reinterpret_cast<uintptr_t>(B) & 15) || (lda & 3) ||
-      (ldb & 3) || lda < k || ldb < k)
-    return 1;
+namespace {
+
+template <int BN, int STAGES>
+int launch(cudaStream_t st, int dev, int m, int n, int k, float alpha, const float* A, int lda, const float* B, int ldb,
+           float beta, float* C, int ldc, bool c_rowmajor, int* err) {
+  using T = Tile<BN, STAGES>;
   // the shared-memory opt-in, once per device
   static std::mutex mu;
   static bool attr_set[64] = {};
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 1;
   {
     std::lock_guard<std::mutex> lock(mu);
     if (!attr_set[dev]) {
-      if (cudaFuncSetAttribute(k_gemm_tf32, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes) != cudaSuccess)
+      if (cudaFuncSetAttribute(k_gemm_tf32<BN, STAGES>, cudaFuncAttributeMaxDynamicSharedMemorySize, T::kSmemBytes) !=
+          cudaSuccess)
         return 1;
       attr_set[dev] = true;
     }
   }
   CUtensorMap ta, tb;
-  if (!make_map(&ta, A, k, m, lda, kBM) || !make_map(&tb, B, k, n, ldb, kBN)) return 1;
-  dim3 grid((unsigned)((m + kBM - 1) / kBM), (unsigned)((n + kBN - 1) / kBN));
-  k_gemm_tf32<<<grid, kThreads, kSmemBytes, st>>>(ta, tb, C, ldc, m, n, k, alpha, beta, c_rowmajor ? 1 : 0, err);
+  if (!make_map(&ta, A, k, m, lda, kBM) || !make_map(&tb, B, k, n, ldb, BN)) return 1;
+  dim3 grid((unsigned)((m + kBM - 1) / kBM), (unsigned)((n + BN - 1) / BN));
+  k_gemm_tf32<BN, STAGES><<<grid, kThreads, T::kSmemBytes, st>>>(ta, tb, C, ldc, m, n, k, alpha, beta,
+                                                                   c_rowmajor ? 1 : 0, err);
   return cudaGetLastError() == cudaSuccess ? 0 : 1;
+}
+
+}  // namespace
+
+int gemm_tf32_variant(cudaStream_t st, int variant, int m, int n, int k, float alpha, const float* A, int lda,
+                      const float* B, int ldb, float beta, float* C, int ldc, bool c_rowmajor, int* err) {
+  if (m <= 0 || n <= 0) return 0;
+  if (k <= 0 || (reinterpret_cast<uintptr_t>(A) & 15) || (reinterpret_cast<uintptr_t>(B) & 15) || (lda & 3) ||
+      (ldb & 3) || lda < k || ldb < k)
+    return 1;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 1;
+  switch (variant) {
+    case 0: return launch<64, 4>(st, dev, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, c_rowmajor, err);
+    case 1: return launch<128, 3>(st, dev, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, c_rowmajor, err);
+    case 2: return launch<256, 3>(st, dev, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, c_rowmajor, err);
+    default: return 1;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Autotuner: the tile variant of each shape class, measured on the device
+// ---------------------------------------------------------------------------
+namespace {
+
+// shape class: M in 128-row tiles, N in 64-column tiles, both by powers of
+// two, and K in 128-wide steps
+struct Key {
+  int dev, cm, cn, ck;
+  bool operator<(const Key& o) const {
+    return dev != o.dev ? dev < o.dev : cm != o.cm ? cm < o.cm : cn != o.cn ? cn < o.cn : ck < o.ck;
+  }
+};
+int ceil_log2(long long x) {
+  int c = 0;
+  while ((1LL << c) < x) ++c;
+  return c;
+}
+Key key_of(int dev, int m, int n, int k) {
+  return Key{dev, ceil_log2((m + kBM - 1) / kBM), ceil_log2((n + 63) / 64), std::min((k + 127) / 128, 8)};
+}
+std::mutex g_tune_mu;
+std::map<Key, int> g_tuned;
+
+// the variant used before a class has been measured: the narrowest tile that
+// still gives every SM work, else the widest
+int heuristic(int m, int n) {
+  const long long tiles128 = (long long)((m + kBM - 1) / kBM) * ((n + 127) / 128);
+  if (n <= 64) return 0;
+  if (tiles128 < 2 * 148) return n <= 128 ? 1 : 0;
+  return tiles128 >= 8 * 148 ? 2 : 1;
+}
+
+}  // namespace
+
+int gemm_tf32_pick(int m, int n, int k) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lock(g_tune_mu);
+  auto it = g_tuned.find(key_of(dev, m, n, k));
+  return it != g_tuned.end() ? it->second : heuristic(m, n);
+}
+
+int gemm_tf32_autotune(cudaStream_t st, int nshape, const int* shapes) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return 1;
+  std::lock_guard<std::mutex> lock(g_tune_mu);
+  // the classes not measured yet, each with its largest shape
+  std::map<Key, int3> todo;
+  for (int s = 0; s < nshape; ++s) {
+    const int m = shapes[3 * s], n = shapes[3 * s + 1], k = shapes[3 * s + 2];
+    if (m <= 0 || n <= 0 || k <= 0) continue;
+    const Key key = key_of(dev, m, n, k);
+    if (g_tuned.count(key)) continue;
+    int3& big = todo[key];
+    if ((long long)m * n * k > (long long)big.x * big.y * big.z) big = make_int3(m, n, k);
+  }
+  if (todo.empty()) return 0;
+  size_t na = 0, nb = 0, nc = 0;
+  for (auto& t : todo) {
+    const int ld = (t.second.z + 3) / 4 * 4;
+    na = std::max(na, (size_t)t.second.x * ld);
+    nb = std::max(nb, (size_t)t.second.y * ld);
+    nc = std::max(nc, (size_t)t.second.x * t.second.y);
+  }
+  float *a = nullptr, *b = nullptr, *c = nullptr;
+  int* err = nullptr;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  int rc = 0;
+  if (cudaMalloc(&a, na * 4) != cudaSuccess || cudaMalloc(&b, nb * 4) != cudaSuccess ||
+      cudaMalloc(&c, nc * 4) != cudaSuccess || cudaMalloc(&err, sizeof(int)) != cudaSuccess ||
+      cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess)
+    rc = 1;
+  if (!rc && (cudaMemsetAsync(a, 0, na * 4, st) != cudaSuccess || cudaMemsetAsync(b, 0, nb * 4, st) != cudaSuccess ||
+              cudaMemsetAsync(err, 0, sizeof(int), st) != cudaSuccess))
+    rc = 1;
+  for (auto it = todo.begin(); !rc && it != todo.end(); ++it) {
+    const int m = it->second.x, n = it->second.y, k = it->second.z, ld = (k + 3) / 4 * 4;
+    float best = 1e30f;
+    int pick = heuristic(m, n);
+    for (int v = 0; v < 3 && !rc; ++v) {
+      float tot = 0.0f;
+      for (int rep = 0; rep < 4 && !rc; ++rep) {  // the first run warms up, the next three are timed
+        if (rep == 1 && cudaEventRecord(e0, st) != cudaSuccess) rc = 1;
+        if (!rc && gemm_tf32_variant(st, v, m, n, k, -1.0f, a, ld, b, ld, 1.0f, c, m, false, err)) rc = 1;
+      }
+      if (!rc && (cudaEventRecord(e1, st) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
+                  cudaEventElapsedTime(&tot, e0, e1) != cudaSuccess))
+        rc = 1;
+      if (!rc && tot < best) {
+        best = tot;
+        pick = v;
+      }
+    }
+    if (!rc) g_tuned[it->first] = pick;
+  }
+  int werr = 0;
+  if (err && cudaMemcpy(&werr, err, sizeof(int), cudaMemcpyDeviceToHost) == cudaSuccess && werr) rc = 1;
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  cudaFree(a);
+  cudaFree(b);
+  cudaFree(c);
+  cudaFree(err);
+  return rc;
+}
+
+int gemm_tf32_tuned_count() {
+  std::lock_guard<std::mutex> lock(g_tune_mu);
+  return (int)g_tuned.size();
+}
+
+int gemm_tf32(cudaStream_t st, int m, int n, int k, float alpha, const float* A, int lda, const float* B, int ldb,
+              float beta, float* C, int ldc, bool c_rowmajor, int* err) {
+  return gemm_tf32_variant(st, gemm_tf32_pick(m, n, k), m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, c_rowmajor, err);
 }

@@ -16,3 +16,19 @@
 // Returns 0, or 1 on a launch or tensor-map error.
 int gemm_tf32(cudaStream_t st, int m, int n, int k, float alpha, const float* A, int lda, const float* B, int ldb,
               float beta, float* C, int ldc, bool c_rowmajor, int* err);
+
+// The same product with an explicit tile variant: 0 = 128 x 64, 1 = 128 x 128,
+// 2 = 128 x 256 (rows x columns of C per CTA).  Every variant sums each
+// element over the K panels in the same order.
+int gemm_tf32_variant(cudaStream_t st, int variant, int m, int n, int k, float alpha, const float* A, int lda,
+                      const float* B, int ldb, float beta, float* C, int ldc, bool c_rowmajor, int* err);
+
+// The autotuner.  gemm_tf32 takes the variant measured fastest for the shape
+// class of (m, n, k) on this device (M by powers of two of 128-row tiles, N of
+// 64-column tiles, K by 128), or a size heuristic for a class not measured.
+// gemm_tf32_autotune measures the classes of the nshape shapes (m, n, k) not
+// measured yet, each on scratch operands of its largest shape (three timed
+// runs per variant on stream st), and records the fastest.  Returns 0 or 1.
+int gemm_tf32_pick(int m, int n, int k);
+int gemm_tf32_autotune(cudaStream_t st, int nshape, const int* shapes);
+int gemm_tf32_tuned_count();

@@ -213,10 +213,43 @@ __global__ void __launch_bounds__(1024) k_sample_err(const double2* __restrict__
   }
 }
 
-// The sensitivity probe: in place, every pair the surrogate evaluates (the
+// The network's error is modelled per cell of its input domain: R/h (log,
+// kJX cells) x source depth x field depth ((z + h)/h, kJZ cells each).
+constexpr int kJX = 24, kJZ = 3, kJCells = kJX * kJZ * kJZ;
+
+__device__ __forceinline__ int judge_cell(double X, double Zq, double Zp) {
+  const int cx = min(kJX - 1, max(0, (int)(kJX * log(X / sg::kXmin) / log(sg::kXmax / sg::kXmin))));
+  const int cq = min(kJZ - 1, max(0, (int)(kJZ * (Zq - sg::kZmin) / (sg::kZmax - sg::kZmin))));
+  const int cp = min(kJZ - 1, max(0, (int)(kJZ * (Zp - sg::kZmin) / (sg::kZmax - sg::kZmin))));
+  return cx + kJX * (cq + kJZ * cp);
+}
+
+__device__ __forceinline__ int pair_cell(const DevGeom& g, double h, size_t p) {
+  const int i = (int)(p % (size_t)g.tn), j = (int)(p / (size_t)g.tn);
+  const double dx = g.xq[j] - g.fxyz[i], dy = g.xq[j + g.n] - g.fxyz[i + g.tn];
+  return judge_cell(sqrt(dx * dx + dy * dy) / h, (g.xq[j + 2 * g.n] + h) / h, (g.fxyz[i + 2 * g.tn] + h) / h);
+}
+
+// Per cell, the least-squares factor m of (network - series) = m Re(series)
+// over the samples, for A and for S: acc[4c..4c+3] += {dA Re A, (Re A)^2,
+// dS Re S, (Re S)^2} (acc zeroed by the caller).
+__global__ void k_judge_fit(DevGeom g, double h, const uint32_t* __restrict__ list, int ns,
+                            const double2* __restrict__ g1, const double2* __restrict__ g2, double* __restrict__ acc) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= ns) return;
+  const int c = pair_cell(g, h, list[k]);
+  const double2 a1 = g1[k], a2 = g2[k], s1 = g1[ns + k], s2 = g2[ns + k];
+  atomicAdd(acc + 4 * c, (a1.x - a2.x) * a2.x);
+  atomicAdd(acc + 4 * c + 1, a2.x * a2.x);
+  atomicAdd(acc + 4 * c + 2, (s1.x - s2.x) * s2.x);
+  atomicAdd(acc + 4 * c + 3, s2.x * s2.x);
+}
+
+// The error probe: in place, every pair the surrogate evaluates (the
 // criterion of k_pair_keys' bins 4 and 5, copied body blocks included)
-// becomes eps times the real part of its A and S entries, every other pair 0.
-__global__ void k_probe_far(DevGeom g, double h, double far, double eps, double2* __restrict__ A,
+// becomes its cell's modelled network error, m Re(entry), for A and S;
+// every other pair 0.
+__global__ void k_probe_far(DevGeom g, double h, double far, const double* __restrict__ acc, double2* __restrict__ A,
                             double2* __restrict__ S) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y;
   if (i >= g.tn) return;
@@ -224,13 +257,18 @@ __global__ void k_probe_far(DevGeom g, double h, double far, double eps, double2
   const double dx = g.xq[j] - g.fxyz[i], dy = g.xq[j + g.n] - g.fxyz[i + g.tn];
   const double rr = sqrt(dx * dx + dy * dy);
   const int b = hams::fin_branch(rr, h);
-  bool on = false;
+  double ma = 0.0, ms = 0.0;
   if (b == hams::kEigenE || b == hams::kEigen) {
     const double zq = g.xq[j + 2 * g.n], zp = g.fxyz[i + 2 * g.tn], dz = zq - zp;
-    on = sqrt(dx * dx + dy * dy + dz * dz) > far * g.pnsz[j] && sg::in_domain(rr / h, (zq + h) / h, (zp + h) / h, sg::kKmin);
+    if (sqrt(dx * dx + dy * dy + dz * dz) > far * g.pnsz[j] &&
+        sg::in_domain(rr / h, (zq + h) / h, (zp + h) / h, sg::kKmin)) {
+      const int c = judge_cell(rr / h, (zq + h) / h, (zp + h) / h);
+      ma = acc[4 * c + 1] > 0.0 ? acc[4 * c] / acc[4 * c + 1] : 0.0;
+      ms = acc[4 * c + 3] > 0.0 ? acc[4 * c + 2] / acc[4 * c + 3] : 0.0;
+    }
   }
-  A[p] = make_double2(on ? eps * A[p].x : 0.0, 0.0);
-  S[p] = make_double2(on ? eps * S[p].x : 0.0, 0.0);
+  A[p] = make_double2(ma * A[p].x, 0.0);
+  S[p] = make_double2(ms * S[p].x, 0.0);
 }
 
 template <int BR>
@@ -748,7 +786,7 @@ struct hams_ctx {
   DBuf<uint32_t> sg_samp;  // sampled surrogate pairs: sg_ns4 of bin 4, then sg_ns5 of bin 5
   int sg_ns4 = 0, sg_ns5 = 0;
   DBuf<double2> sg_g1, sg_g2;  // the sampled A and S entries from the network, then from the series
-  DBuf<double> sg_red, outbuf2;
+  DBuf<double> sg_red, sg_cells, outbuf2;
   double sg_judge[8] = {};  // e_A, e_S, kappa_A, kappa_B, kappa_X, estimate, re-solved with the series, samples
   std::string note;  // what the last solve changed on its own (fallbacks), or empty
   bool unfolded = false;  // built from a half mesh (ISX or ISY = 1), see unfold_symmetry
@@ -1158,6 +1196,15 @@ extern "C" int hams_ctx_create(const hams_geom* geo, const hams_opts* opts, hams
   c->xyz_p.assign(geo->xyz_p, geo->xyz_p + (size_t)3 * geo->nelem);
   int rc = ctx_handles(c);
   if (!rc) rc = ctx_setup(c, geo);
+  if (!rc && c->opts.precision == HAMS_PREC_MIXED && c->opts.solver != HAMS_SOLVER_GMRES &&
+      c->opts.lu_kind == HAMS_LU_BLOCK_TF32) {
+    // tile variants of the block LU's GEMMs for this order (classes measured
+    // once per device and process)
+    std::vector<int> shapes;
+    mixed_lu_gemm_shapes(c->n, shapes);
+    if (gemm_tf32_autotune(c->st, (int)shapes.size() / 3, shapes.data()))
+      rc = fail(HAMS_ERR_CUDA, "GEMM autotuner failed: %s", cudaGetErrorString(cudaGetLastError()));
+  }
   if (rc < 0) {
     std::string keep = g_err;
     hams_ctx_destroy(c);
@@ -1245,7 +1292,10 @@ static int assemble_dev(hams_ctx* c, const hams_wave* w, int nbeta, bool force_s
           TRY(launch_check(c, (c->sg_ns4 > 0) + (c->sg_ns5 > 0)));
           k_gather_pairs<<<gb, 256, 0, c->st>>>(c->sg_samp.p, ns, c->A.p, c->S.p, c->sg_g2.p);
           k_sample_err<<<1, 1024, 0, c->st>>>(c->sg_g1.p, c->sg_g2.p, ns, c->sg_red.p);
-          TRY(launch_check(c, 2));
+          TRY(c->sg_cells.alloc(4 * kJCells));
+          CU(cudaMemsetAsync(c->sg_cells.p, 0, 4 * kJCells * sizeof(double), c->st));
+          k_judge_fit<<<gb, 256, 0, c->st>>>(c->g, hh, c->sg_samp.p, ns, c->sg_g1.p, c->sg_g2.p, c->sg_cells.p);
+          TRY(launch_check(c, 3));
         }
       } else {
         long long ce = c->bin_off[5] - c->bin_off[4], cg = c->bin_off[6] - c->bin_off[5];
@@ -1757,7 +1807,7 @@ static int mixed_apply(hams_ctx* c, int nrhs) {
 }
 
 // Safety factor of the judgement: the largest ratio of a frequency's true
-// error (against the plain series) to its estimate e kappa, observed on the
+// error (against the plain series) to its estimate, observed on the
 // 5,400-panel 3 x 3 array of cylinders (h = 50 m) over 0.2-2.5 rad/s, rounded up.
 constexpr double kJudgeSafety = 1.0;
 
@@ -1765,19 +1815,24 @@ constexpr double kJudgeSafety = 1.0;
 // of the surrogate's relative error in added mass, damping and excitation.
 //   e      the network's relative error on the far-pair entries of A and S,
 //          from the pairs sampled during the assembly (k_sample_err);
-//   kappa  the outputs' sensitivity to the far-pair entries: every entry the
-//          network produced is perturbed by eps of its real part (the part
-//          the network changes), and the first-order change of the solution,
-//          dX = (L U)^-1 (dB - dA X), is carried through the force
-//          reductions; kappa = |output change| / (eps |output|) per output.
-// The estimate is kJudgeSafety e max(kappa).  A and S are overwritten (the
-// frequency does not read them again).  Requires the mixed solve's factors.
+//   the error model: per cell of the network's input domain (R/h x source
+//          depth x field depth), the factor m with network - series =
+//          m Re(series) fitted to the samples of that cell (k_judge_fit);
+//   the probe: every far-pair entry of A and S replaced by its cell's
+//          modelled error m Re(entry) (k_probe_far), the first-order change
+//          of the solution, dX = (L U)^-1 (dB - dA X), carried through the
+//          force reductions: the estimated change of each output, relative
+//          to the output.
+// The estimate is kJudgeSafety times the largest of the three.  A and S are
+// overwritten (the frequency does not read them again).  Requires the mixed
+// solve's factors.
 static int surrogate_judge(hams_ctx* c, const hams_wave* w, int nbeta) {
   const int n = c->n, tn = c->tn, nb = c->nb, ndof = 6 * nb, nrhs = ndof + nbeta;
-  const double eps = 1e-3;
+  const double eps = 1.0;  // the probe is the modelled error itself
   const cuDoubleComplex one = make_cuDoubleComplex(1.0, 0.0), mone = make_cuDoubleComplex(-1.0, 0.0);
   WaveDev wd = wave_dev(c, w);
-  k_probe_far<<<dim3((tn + 127) / 128, n), 128, 0, c->st>>>(c->g, c->opts.depth, c->sg_far, eps, c->A.p, c->S.p);
+  k_probe_far<<<dim3((tn + 127) / 128, n), 128, 0, c->st>>>(c->g, c->opts.depth, c->sg_far, c->sg_cells.p, c->A.p,
+                                                            c->S.p);
   TRY(launch_check(c));
   // dB: the right-hand sides of the probe's S (this frequency's diffraction weights are still in wd)
   const int nch = (int)c->chunks_h.size();
@@ -1819,13 +1874,13 @@ static int surrogate_judge(hams_ctx* c, const hams_wave* w, int nbeta) {
     return r > 0.0 ? std::sqrt(d / r) / eps : 0.0;
   };
   const size_t na = (size_t)ndof * ndof;
-  double* j = c->sg_judge;
+  double* j = c->sg_judge;  // e_A, e_S (sampled), the estimated error of A, B, X, the estimate
   j[0] = red[1] > 0.0 ? std::sqrt(red[0] / red[1]) : 0.0;
   j[1] = red[3] > 0.0 ? std::sqrt(red[2] / red[3]) : 0.0;
   j[2] = kappa(0, na);
   j[3] = kappa(na, na);
   j[4] = nbeta > 0 ? kappa(2 * na, 2 * (size_t)ndof * nbeta) : 0.0;
-  j[5] = kJudgeSafety * std::max(j[0], j[1]) * std::max(j[2], std::max(j[3], j[4]));
+  j[5] = kJudgeSafety * std::max(j[2], std::max(j[3], j[4]));
   j[7] = (double)(c->sg_ns4 + c->sg_ns5);
   return 0;
 }
@@ -2366,10 +2421,10 @@ extern "C" int hams_measure_fp64_peak(int32_t device, double* tflops) {
 // ---------------------------------------------------------------------------
 extern "C" int hams_diag_gemm_tf32(int32_t device, int32_t m, int32_t n, int32_t k, float alpha, const float* a,
                                    int32_t lda, const float* b, int32_t ldb, float beta, float* c, int32_t ldc,
-                                   int32_t c_rowmajor) {
+                                   int32_t c_rowmajor, int32_t variant) {
   g_err.clear();
   if (m < 1 || n < 1 || k < 1 || !a || !b || !c || lda < k || ldb < k || (lda & 3) || (ldb & 3) ||
-      ldc < (c_rowmajor ? n : m))
+      ldc < (c_rowmajor ? n : m) || variant < -1 || variant > 2)
     return fail(HAMS_ERR_ARG, "bad GEMM arguments");
   if (cudaSetDevice(device) != cudaSuccess) return fail(HAMS_ERR_CUDA, "cudaSetDevice(%d) failed", device);
   const size_t na = (size_t)m * lda, nb = (size_t)n * ldb, nc = c_rowmajor ? (size_t)m * ldc : (size_t)n * ldc;
@@ -2383,11 +2438,53 @@ extern "C" int hams_diag_gemm_tf32(int32_t device, int32_t m, int32_t n, int32_t
   CU(cudaMemcpy(db.p, b, nb * 4, cudaMemcpyHostToDevice));
   CU(cudaMemcpy(dc.p, c, nc * 4, cudaMemcpyHostToDevice));
   CU(cudaMemset(derr.p, 0, sizeof(int)));
-  if (gemm_tf32(0, m, n, k, alpha, da.p, lda, db.p, ldb, beta, dc.p, ldc, c_rowmajor != 0, derr.p))
+  const int v = variant >= 0 ? variant : gemm_tf32_pick(m, n, k);
+  if (gemm_tf32_variant(0, v, m, n, k, alpha, da.p, lda, db.p, ldb, beta, dc.p, ldc, c_rowmajor != 0, derr.p))
     return fail(HAMS_ERR_CUDA, "gemm_tf32 launch failed: %s", cudaGetErrorString(cudaGetLastError()));
   int err = 0;
   CU(cudaMemcpy(&err, derr.p, sizeof(int), cudaMemcpyDeviceToHost));
   CU(cudaMemcpy(c, dc.p, nc * 4, cudaMemcpyDeviceToHost));
   if (err) return fail(HAMS_ERR_CUDA, "gemm_tf32: a pipeline wait gave up (%d)", err);
+  return 0;
+}
+
+// Diagnostic: device time of the block LU's GEMM (variant as above) on
+// device-resident operands of the given shape, mean of reps launches after
+// one untimed launch.
+extern "C" int hams_diag_gemm_tf32_time(int32_t device, int32_t variant, int32_t m, int32_t n, int32_t k,
+                                        int32_t reps, double* ms) {
+  g_err.clear();
+  if (m < 1 || n < 1 || k < 1 || reps < 1 || !ms || variant < -1 || variant > 2)
+    return fail(HAMS_ERR_ARG, "bad GEMM arguments");
+  if (cudaSetDevice(device) != cudaSuccess) return fail(HAMS_ERR_CUDA, "cudaSetDevice(%d) failed", device);
+  const int ld = (k + 3) / 4 * 4;
+  DBuf<float> da, db, dc;
+  DBuf<int> derr;
+  TRY(da.alloc((size_t)m * ld));
+  TRY(db.alloc((size_t)n * ld));
+  TRY(dc.alloc((size_t)m * n));
+  TRY(derr.alloc(1));
+  CU(cudaMemset(da.p, 0, (size_t)m * ld * 4));
+  CU(cudaMemset(db.p, 0, (size_t)n * ld * 4));
+  CU(cudaMemset(dc.p, 0, (size_t)m * n * 4));
+  CU(cudaMemset(derr.p, 0, sizeof(int)));
+  const int v = variant >= 0 ? variant : gemm_tf32_pick(m, n, k);
+  cudaEvent_t e0, e1;
+  CU(cudaEventCreate(&e0));
+  CU(cudaEventCreate(&e1));
+  int rc = gemm_tf32_variant(0, v, m, n, k, -1.0f, da.p, ld, db.p, ld, 1.0f, dc.p, m, false, derr.p);
+  cudaEventRecord(e0, 0);
+  for (int r = 0; r < reps && !rc; ++r)
+    rc = gemm_tf32_variant(0, v, m, n, k, -1.0f, da.p, ld, db.p, ld, 1.0f, dc.p, m, false, derr.p);
+  cudaEventRecord(e1, 0);
+  cudaEventSynchronize(e1);
+  float t = 0.0f;
+  cudaEventElapsedTime(&t, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  int err = 0;
+  CU(cudaMemcpy(&err, derr.p, sizeof(int), cudaMemcpyDeviceToHost));
+  if (rc || err) return fail(HAMS_ERR_CUDA, "gemm_tf32 failed (%d, %d)", rc, err);
+  *ms = t / reps;
   return 0;
 }

@@ -301,31 +301,52 @@ __global__ void k_apply_perm(float2* A, int lda, int n, int k0, int nbk, const i
 // ---------------------------------------------------------------------------
 // Block triangular solves
 // ---------------------------------------------------------------------------
-constexpr int kNC = 16;  // right-hand sides per CTA
-constexpr int kTrsmSmem = (kNB * (kNB + 1) + 2 * kNB * kNC) * (int)sizeof(float2);
+constexpr int kNC = 64;        // right-hand sides per ticket
+constexpr int kTLd = kNB + 4;  // column stride of a shared 64 x 64 block (float2; 16-byte aligned columns)
+constexpr int kXLd = kNB + 2;  // column stride of the shared right-hand sides
+constexpr int kTrsmSmem = (2 * kNB * kTLd + 2 * kNC * kXLd) * (int)sizeof(float2);
 constexpr long long kFlagSpin = 1ll << 24;
 
-__device__ __forceinline__ float2 csub_mul(float2 s, float2 a, float2 b) {
-  return make_float2(s.x - (a.x * b.x - a.y * b.y), s.y - (a.x * b.y + a.y * b.x));
+__device__ __forceinline__ void cmac_sub(float2& s, float2 a, float2 b) {
+  s.x -= a.x * b.x - a.y * b.y;
+  s.y -= a.x * b.y + a.y * b.x;
+}
+
+// T = the 64 x 64 block of A at block row b, block column j, into shared
+// memory with asynchronous 16-byte copies (zero-filled outside the n x n
+// matrix); lda is even, so every copy is 16-byte aligned.
+__device__ __forceinline__ void prefetch_block(float2* sT, const float2* __restrict__ A, int lda, int n, int b, int j) {
+  for (int e = threadIdx.x; e < kNB * kNB / 2; e += 256) {
+    const int cc = e / (kNB / 2), rr = 2 * (e % (kNB / 2)), gr = b * kNB + rr, gc = j * kNB + cc;
+    const int bytes = gc < n ? (gr + 1 < n ? 16 : (gr < n ? 8 : 0)) : 0;
+    const float2* src = bytes ? A + (size_t)gc * lda + gr : A;
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"((uint32_t)__cvta_generic_to_shared(
+                     sT + cc * kTLd + rr)),
+                 "l"(src), "r"(bytes)
+                 : "memory");
+  }
+  asm volatile("cp.async.commit_group;" ::: "memory");
 }
 
 // One launch solves one triangle for all right-hand sides.  lower: unit L,
 // blocks in increasing order, the right-hand sides gathered through perm
 // from B; upper: U, blocks in decreasing order, B unpermuted.  X receives
 // the solution (n x nrhs, ld n).  flags (nblk x nch) and ticket start at 0.
-// The grid is small and persistent: each CTA takes tickets (block row and
-// chunk, in dependency order) until none is left, so CTAs that wait for an
-// earlier block hold few SMs.
-__global__ void __launch_bounds__(256) k_trsm_block(const float2* __restrict__ A, int lda, int n, int nrhs, int nblk,
-                                                    int nch, bool lower, const float2* __restrict__ invc,
-                                                    const int* __restrict__ perm, const float2* __restrict__ B,
-                                                    float2* X, int* flags, unsigned int* ticket, int* err) {
-  extern __shared__ float2 sm[];
-  float2* sT = sm;                    // a 64 x 64 block, column-major, ld kNB + 1
-  float2* sX = sm + kNB * (kNB + 1);  // the published X_j of the chunk (64 x kNC)
-  float2* sAcc = sX + kNB * kNC;      // B_b - sum, the operand of the inverse
+// The grid is small and persistent: each CTA takes tickets (a block row and
+// a chunk of 64 right-hand sides, in dependency order) until none is left,
+// so CTAs that wait for an earlier block hold few SMs.  A thread owns 4 rows
+// x 4 right-hand sides; the next off-diagonal block is copied in while the
+// current one is applied.
+__global__ void __launch_bounds__(256, 1) k_trsm_block(const float2* __restrict__ A, int lda, int n, int nrhs,
+                                                       int nblk, int nch, bool lower, const float2* __restrict__ invc,
+                                                       const int* __restrict__ perm, const float2* __restrict__ B,
+                                                       float2* X, int* flags, unsigned int* ticket, int* err) {
+  extern __shared__ __align__(16) float2 sm[];
+  float2* sT[2] = {sm, sm + kNB * kTLd};  // off-diagonal blocks, column-major
+  float2* sX = sm + 2 * kNB * kTLd;       // the published X_j of the chunk, column-major (kNC columns)
+  float2* sAcc = sX + kNC * kXLd;         // B_b - sum, the operand of the inverse
   __shared__ int s_id, s_abort;
-  const int tid = threadIdx.x;
+  const int tid = threadIdx.x, r0 = (tid % 16) * 4, c0 = (tid / 16) * 4;
   for (;;) {
     __syncthreads();  // the previous ticket's shared data is no longer read
     if (tid == 0) {
@@ -336,25 +357,23 @@ __global__ void __launch_bounds__(256) k_trsm_block(const float2* __restrict__ A
     if (s_id >= nblk * nch) return;
     const int order = s_id / nch, ch = s_id % nch;
     const int b = lower ? order : nblk - 1 - order;
-    const int q0 = ch * kNC, r = tid % kNB, qq = (tid / kNB) * 4;  // this thread: row r, chunk columns qq..qq+3
-    const int row = b * kNB + r;
+    const int q0 = ch * kNC;
+    if (order > 0) prefetch_block(sT[0], A, lda, n, b, lower ? 0 : nblk - 1);
     // the block's right-hand sides
     for (int e = tid; e < kNB * kNC; e += 256) {
       const int rr = e % kNB, q = e / kNB, gr = b * kNB + rr;
       float2 v = make_float2(0.0f, 0.0f);
       if (gr < n && q0 + q < nrhs) v = B[(size_t)(q0 + q) * n + (lower ? perm[gr] : gr)];
-      sAcc[q * kNB + rr] = v;
+      sAcc[q * kXLd + rr] = v;
     }
     __syncthreads();
-    float2 acc[4];
-    for (int u = 0; u < 4; ++u) acc[u] = make_float2(0.0f, 0.0f);
+    float2 acc[4][4];
+    for (int i = 0; i < 4; ++i)
+      for (int u = 0; u < 4; ++u) acc[i][u] = sAcc[(c0 + u) * kXLd + r0 + i];
     for (int step = 0; step < order; ++step) {
       const int j = lower ? step : nblk - 1 - step;
-      // the off-diagonal block T = A[b rows, j columns], read while the flag is awaited
-      for (int e = tid; e < kNB * kNB; e += 256) {
-        const int rr = e % kNB, cc = e / kNB, gr = b * kNB + rr, gc = j * kNB + cc;
-        sT[cc * (kNB + 1) + rr] = (gr < n && gc < n) ? A[(size_t)gc * lda + gr] : make_float2(0.0f, 0.0f);
-      }
+      const bool more = step + 1 < order;
+      if (more) prefetch_block(sT[(step + 1) & 1], A, lda, n, b, lower ? step + 1 : nblk - 2 - step);
       if (tid == 0) {
         const volatile int* f = flags + j * nch + ch;
         long long it = 0;
@@ -372,37 +391,50 @@ __global__ void __launch_bounds__(256) k_trsm_block(const float2* __restrict__ A
       if (s_abort) break;
       for (int e = tid; e < kNB * kNC; e += 256) {
         const int rr = e % kNB, q = e / kNB, gr = j * kNB + rr;
-        sX[q * kNB + rr] =
+        sX[q * kXLd + rr] =
             (gr < n && q0 + q < nrhs) ? __ldcg(X + (size_t)(q0 + q) * n + gr) : make_float2(0.0f, 0.0f);
       }
+      if (more) asm volatile("cp.async.wait_group 1;" ::: "memory");
+      else asm volatile("cp.async.wait_group 0;" ::: "memory");
       __syncthreads();
-  #pragma unroll 4
+      const float2* T = sT[step & 1];
+#pragma unroll 2
       for (int k = 0; k < kNB; ++k) {
-        const float2 t = sT[k * (kNB + 1) + r];
-  #pragma unroll
-        for (int u = 0; u < 4; ++u) acc[u] = csub_mul(acc[u], t, sX[(qq + u) * kNB + k]);
+        const float4 t01 = *reinterpret_cast<const float4*>(T + k * kTLd + r0);
+        const float4 t23 = *reinterpret_cast<const float4*>(T + k * kTLd + r0 + 2);
+        const float2 t[4] = {make_float2(t01.x, t01.y), make_float2(t01.z, t01.w), make_float2(t23.x, t23.y),
+                             make_float2(t23.z, t23.w)};
+        float2 x[4];
+        for (int u = 0; u < 4; ++u) x[u] = sX[(c0 + u) * kXLd + k];
+        for (int i = 0; i < 4; ++i)
+          for (int u = 0; u < 4; ++u) cmac_sub(acc[i][u], t[i], x[u]);
       }
       __syncthreads();
     }
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
     // X_b = T_bb^-1 (B_b - sum)
-    for (int u = 0; u < 4; ++u) {
-      float2& s = sAcc[(qq + u) * kNB + r];
-      s = make_float2(s.x + acc[u].x, s.y + acc[u].y);
-    }
+    for (int i = 0; i < 4; ++i)
+      for (int u = 0; u < 4; ++u) sAcc[(c0 + u) * kXLd + r0 + i] = acc[i][u];
     const float2* inv = invc + (size_t)b * kNB * kNB;
-    for (int e = tid; e < kNB * kNB; e += 256) sT[(e / kNB) * (kNB + 1) + e % kNB] = inv[e];
+    for (int e = tid; e < kNB * kNB; e += 256) sT[0][(e / kNB) * kTLd + e % kNB] = inv[e];
     __syncthreads();
-    float2 out[4];
-    for (int u = 0; u < 4; ++u) out[u] = make_float2(0.0f, 0.0f);
-  #pragma unroll 4
+    float2 out[4][4];
+    for (int i = 0; i < 4; ++i)
+      for (int u = 0; u < 4; ++u) out[i][u] = make_float2(0.0f, 0.0f);
+#pragma unroll 2
     for (int k = 0; k < kNB; ++k) {
-      const float2 t = sT[k * (kNB + 1) + r];
-  #pragma unroll
-      for (int u = 0; u < 4; ++u) out[u] = csub_mul(out[u], t, sAcc[(qq + u) * kNB + k]);
+      float2 t[4], x[4];
+      for (int i = 0; i < 4; ++i) t[i] = sT[0][k * kTLd + r0 + i];
+      for (int u = 0; u < 4; ++u) x[u] = sAcc[(c0 + u) * kXLd + k];
+      for (int i = 0; i < 4; ++i)
+        for (int u = 0; u < 4; ++u) cmac_sub(out[i][u], t[i], x[u]);
     }
-    if (row < n)
-      for (int u = 0; u < 4; ++u)
-        if (q0 + qq + u < nrhs) X[(size_t)(q0 + qq + u) * n + row] = make_float2(-out[u].x, -out[u].y);
+    for (int i = 0; i < 4; ++i) {
+      const int row = b * kNB + r0 + i;
+      if (row < n)
+        for (int u = 0; u < 4; ++u)
+          if (q0 + c0 + u < nrhs) X[(size_t)(q0 + c0 + u) * n + row] = make_float2(-out[i][u].x, -out[i][u].y);
+    }
     __threadfence();
     __syncthreads();
     if (tid == 0) atomicExch(flags + b * nch + ch, 1);  // published (also after an abandoned wait, so no CTA hangs)
@@ -564,6 +596,25 @@ int mixed_lu_factor(cudaStream_t st, cublasHandle_t blas, bool own_gemm, cublasC
   return 0;
 }
 
+void mixed_lu_gemm_shapes(int n, std::vector<int>& shapes) {
+  const int PW = kPB * kNB;
+  auto add = [&](int m, int nn, int k) {
+    if (m > 0 && nn > 0 && k > 0) shapes.insert(shapes.end(), {m, nn, k});
+  };
+  for (int p0 = 0; p0 < n; p0 += PW) {
+    const int p1 = std::min(n, p0 + PW), wt = n - p1;
+    for (int k0 = p0; k0 < p1; k0 += kNB) {
+      const int nbk = std::min(kNB, n - k0), k1 = k0 + nbk, wr = n - k1, wp = p1 - k1, k2 = 2 * nbk;
+      add(2 * wr, k2, k2);
+      add(k2, wp, k2);
+      add(2 * wr, wp, k2);
+      if (k0 > p0) add(k2, wt, 2 * (k0 - p0));
+      add(k2, wt, k2);
+    }
+    add(2 * wt, wt, 2 * (p1 - p0));
+  }
+}
+
 int mixed_lu_solve(cudaStream_t st, int n, int lda, int nrhs, const float2* A, const int* perm, float2* X,
                    float2* work, int* dflag, long long* launches) {
   if (nrhs <= 0) return 0;
@@ -577,9 +628,9 @@ int mixed_lu_solve(cudaStream_t st, int n, int lda, int nrhs, const float2* A, c
   float2* T = (float2*)(ws + L.T);
   int* flags = (int*)(ws + L.flags);
   unsigned int* ticket = (unsigned int*)(flags + nblk * nch);
-  // a few CTAs per chunk column: enough to overlap the block rows' sums, few
-  // enough that waiting CTAs leave the GPU to the other frequencies in flight
-  const unsigned grid = (unsigned)std::min(nblk * nch, 8 * nch);
+  // a few CTAs: enough to overlap the block rows' sums, few enough that
+  // waiting CTAs leave the GPU to the other frequencies in flight
+  const unsigned grid = (unsigned)std::min(nblk * nch, 32);
   // forward: T = L^-1 P X; backward: X = U^-1 T
   if (cudaMemsetAsync(flags, 0, (size_t)(nblk * nch + 1) * sizeof(int), st) != cudaSuccess) return 1;
   k_trsm_block<<<grid, 256, kTrsmSmem, st>>>(A, lda, n, nrhs, nblk, nch, true, invLc, perm, X, T, flags, ticket,

@@ -3,6 +3,8 @@
 #include <cublas_v2.h>
 #include <cuda_runtime.h>
 
+#include <vector>
+
 // Elements (float2) of the workspace mixed_lu_factor / mixed_lu_solve need
 // for order n and nrhs right-hand sides.
 size_t mixed_lu_workspace_elems(int n, int nrhs);
@@ -30,3 +32,7 @@ int mixed_lu_factor(cudaStream_t st, cublasHandle_t blas, bool own_gemm, cublasC
 // Returns 0 or 1 on a launch error.
 int mixed_lu_solve(cudaStream_t st, int n, int lda, int nrhs, const float2* A, const int* perm, float2* X,
                    float2* work, int* dflag, long long* launches);
+
+// The (m, n, k) shapes of the real GEMMs mixed_lu_factor runs for order n,
+// three ints each (the input of the GEMM autotuner).
+void mixed_lu_gemm_shapes(int n, std::vector<int>& shapes);

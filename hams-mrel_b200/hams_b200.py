@@ -106,7 +106,8 @@ def load_library(path=LIB_PATH):
     lib.hams_surrogate_eval.argtypes = [c_int, P_flt, c_int, P_dbl, P_dbl]
     lib.hams_surrogate_grad.argtypes = [c_int, P_flt, c_int, P_flt, P_flt, P_dbl, P_flt]
     lib.hams_diag_gemm_tf32.argtypes = [c_int, c_int, c_int, c_int, ctypes.c_float, P_flt, c_int, P_flt, c_int,
-                                        ctypes.c_float, P_flt, c_int, c_int]
+                                        ctypes.c_float, P_flt, c_int, c_int, c_int]
+    lib.hams_diag_gemm_tf32_time.argtypes = [c_int, c_int, c_int, c_int, c_int, c_int, P_dbl]
     _LIB = lib
     return lib
 
@@ -267,7 +268,7 @@ class Context:
                     pairs_linton=int(ms[11]), pairs_pidcock=int(ms[12]), pairs_eigene=int(ms[13]),
                     pairs_eigen=int(ms[14]), lu_used=int(ms[15]), green_surrogate=ms[16],
                     pairs_surrogate=int(ms[17]), ir_rate=ms[18], pairs_copied=int(ms[19]),
-                    judge_err_a=ms[20], judge_err_s=ms[21], judge_kappa=(ms[22], ms[23], ms[24]),
+                    judge_err_a=ms[20], judge_err_s=ms[21], judge_errors=(ms[22], ms[23], ms[24]),
                     judge_estimate=ms[25], judge_resolved=bool(ms[26]), judge_samples=int(ms[27]))
 
     def set_surrogate(self, params, far_factor=3.0, k_range=None):
@@ -331,8 +332,9 @@ def measure_fp64_peak(device=0):
     return t.value
 
 
-def diag_gemm_tf32(a, b, c=None, alpha=1.0, beta=0.0, c_rowmajor=False, device=0):
-    """The block LU's tensor-core GEMM: alpha a @ b + beta c for float32 a (m x k), b (k x n), c (m x n)."""
+def diag_gemm_tf32(a, b, c=None, alpha=1.0, beta=0.0, c_rowmajor=False, variant=-1, device=0):
+    """The block LU's tensor-core GEMM: alpha a @ b + beta c for float32 a (m x k), b (k x n), c (m x n);
+    variant 0/1/2 = tiles of 64/128/256 columns, -1 = the autotuner's pick."""
     m, k = a.shape
     n = b.shape[1]
     ld = (k + 3) // 4 * 4
@@ -343,8 +345,15 @@ def diag_gemm_tf32(a, b, c=None, alpha=1.0, beta=0.0, c_rowmajor=False, device=0
     C = np.zeros((m, n), dtype=np.float32) if c is None else np.array(c, dtype=np.float32)  # a copy
     Cbuf = np.ascontiguousarray(C) if c_rowmajor else np.ascontiguousarray(C.T)
     _check(load_library().hams_diag_gemm_tf32(device, m, n, k, alpha, _f(A), ld, _f(B), ld, beta, _f(Cbuf),
-                                               n if c_rowmajor else m, int(c_rowmajor)))
+                                               n if c_rowmajor else m, int(c_rowmajor), int(variant)))
     return Cbuf if c_rowmajor else Cbuf.T
+
+
+def diag_gemm_tf32_time(m, n, k, variant=-1, reps=10, device=0):
+    """Mean device time (ms) of the block LU's GEMM on device operands of shape m x n x k."""
+    ms = ctypes.c_double()
+    _check(load_library().hams_diag_gemm_tf32_time(device, variant, m, n, k, reps, ctypes.byref(ms)))
+    return ms.value
 
 
 # ---------------------------------------------------------------------------

@@ -282,19 +282,20 @@ int hams_ctx_set_surrogate_range(hams_ctx *ctx, double kmin, double kmax);
 /* The series judges the surrogate, frequency by frequency (no counterpart in
  * the reference, which has no surrogate).  With tol > 0, every frequency the
  * network serves (mixed precision, LU solver, no lids) is checked after its
- * solve: the series re-evaluates a sample of about 16,000 far pairs, giving
- * the network's relative error e on the far-pair entries of A and S, and a
- * sensitivity probe (those entries perturbed in proportion, the first-order
- * change carried through the factorisation already made and the force
- * reductions) gives each output's amplification kappa.  When the estimate
- * e kappa (times a safety factor calibrated on the 5,400-panel array)
- * exceeds tol, the frequency is assembled again with the series and
- * re-solved; hams_last_note says so and hams_last_timings reports the
- * estimate.  The probe amplifies what the system amplifies: the long-wave
- * damping (a small imaginary part of large potentials) and the bands around
- * irregular frequencies, where the hand-picked K range of
- * hams_ctx_set_surrogate_range would otherwise be needed.  tol = 0 (the
- * default) switches the judgement off. */
+ * solve: the series re-evaluates a sample of about 16,000 far pairs, and
+ * the network's error per cell of its input domain (R/h x source depth x
+ * field depth) is fitted to them as a multiple of the entries; that modelled
+ * error, put in place of every far-pair entry of A and S, is carried to
+ * first order through the factorisation already made and the force
+ * reductions, giving the estimated error of added mass, damping and
+ * excitation.  When the largest (times a safety factor calibrated on the
+ * 5,400-panel array) exceeds tol, the frequency is assembled again with the
+ * series and re-solved; hams_last_note says so and hams_last_timings reports
+ * the estimates.  The probe goes through the same system, so it is amplified
+ * where the system amplifies: the long-wave damping (a small imaginary part
+ * of large potentials) and the bands around irregular frequencies, which
+ * the hand-picked K range of hams_ctx_set_surrogate_range otherwise keeps on
+ * the series.  tol = 0 (the default) switches the judgement off. */
 int hams_ctx_set_surrogate_tolerance(hams_ctx *ctx, double tol);
 
 /* Timing of the last solve in milliseconds: [0] Green/assembly kernels,
@@ -309,10 +310,10 @@ int hams_ctx_set_surrogate_tolerance(hams_ctx *ctx, double tol);
  * [19] pairs copied from identical body blocks (hams_opts.body_blocks),
  * and, for a frequency the surrogate solved with a tolerance set
  * (hams_ctx_set_surrogate_tolerance): [20] the network's sampled relative
- * error on the far-pair entries of A, [21] of S, [22..24] the added mass',
- * damping's and excitation's sensitivity to those entries, [25] the error
- * estimate, [26] 1 if the frequency was re-solved with the series, [27] the
- * pairs sampled.  n is the capacity of ms (28 fills all). Returns the number
+ * error on the far-pair entries of A, [21] of S, [22..24] the estimated
+ * relative error of added mass, damping and excitation, [25] the estimate
+ * the decision uses, [26] 1 if the frequency was re-solved with the series,
+ * [27] the pairs sampled.  n is the capacity of ms (28 fills all). Returns the number
  * written. */
 int hams_last_timings(hams_ctx *ctx, double *ms, int32_t n);
 
@@ -362,9 +363,18 @@ int hams_measure_fp64_peak(int32_t device, double *tflops);
  * tensor-core GEMM (tcgen05.mma kind::tf32, FP32 accumulation) on host
  * arrays, for tests: C = alpha A B + beta C with A m x k row-major (lda, a
  * multiple of 4), B k x n column-major (ldb, a multiple of 4), C m x n
- * column-major, or row-major with c_rowmajor (ldc). */
+ * column-major, or row-major with c_rowmajor (ldc); variant 0, 1, 2 the tile
+ * of 128 x 64, 128 x 128 or 128 x 256 columns of C per CTA, -1 the
+ * autotuner's pick. */
 int hams_diag_gemm_tf32(int32_t device, int32_t m, int32_t n, int32_t k, float alpha, const float *a, int32_t lda,
-                        const float *b, int32_t ldb, float beta, float *c, int32_t ldc, int32_t c_rowmajor);
+                        const float *b, int32_t ldb, float beta, float *c, int32_t ldc, int32_t c_rowmajor,
+                        int32_t variant);
+
+/* Diagnostic (no counterpart in the reference): mean device time in ms of
+ * that GEMM (variant 0-2, or -1 for the autotuner's pick) on device-resident
+ * operands of shape m x n x k, over reps launches after one untimed. */
+int hams_diag_gemm_tf32_time(int32_t device, int32_t variant, int32_t m, int32_t n, int32_t k, int32_t reps,
+                             double *ms);
 
 /* Message of the last failing call on this thread ("" if none). */
 const char *hams_last_error(void);

@@ -4,8 +4,9 @@ block LU and the block triangular solves, through the C ABI.
 GEMM: against the product of the inputs rounded to TF32 the way the tensor
 cores read them, computed in FP64 (relative Frobenius 1e-5: only the FP32
 accumulation differs), and against the unrounded FP64 product within the
-TF32 bound (3e-3); ragged shapes (M, N, K not multiples of the 128 x 128 x 32
-tiles), alpha / beta, row- and column-major results.  LU: solves of odd order
+TF32 bound (3e-3); ragged shapes (M, N, K not multiples of the tiles),
+alpha / beta, row- and column-major results; the three tile variants of the
+autotuner give the same bits.  LU: solves of odd order
 and of several 256-column panels, mixed form with the own GEMM and with
 cuBLAS's FP32 emulation, against the fp64 form (1e-7), with the block LU
 actually used (no fallback to the library LU) and few refinement sweeps.
@@ -53,6 +54,10 @@ def test_gemm_tf32(m, n, k, alpha, beta, rowmajor):
     emul = min(rel(got, alpha * (tf32(a, mode) @ tf32(b, mode)) + beta * c.astype(np.float64))
                for mode in ("trunc", "round"))
     assert emul < 1e-5, emul
+    # the three tile variants the autotuner chooses from sum over K in the same order: the same bits
+    for v in range(3):
+        assert np.array_equal(hams_b200.diag_gemm_tf32(a, b, c, alpha, beta, rowmajor, variant=v).astype(np.float64),
+                              got), v
 
 
 def _array(n_theta, n_z, n_r, nx, ny, spacing):
