@@ -119,12 +119,15 @@ __device__ __forceinline__ uint32_t pack2(float lo, float hi) {
   return *reinterpret_cast<uint32_t*>(&h);
 }
 
-// SiLU as z (1 + tanh(z / 2)) / 2 with the hardware tanh approximation
-// (relative error ~2^-11, below the FP16 rounding of the activations)
-__device__ __forceinline__ float silu(float z) {
+// SiLU of z = 2h from the half pre-activation h (the weights and biases of
+// the layers that feed a SiLU are stored halved, an exact power-of-two
+// scaling): silu(z) = z (1 + tanh(z / 2)) / 2 = h + h tanh(h), one hardware
+// tanh (relative error ~2^-11, below the FP16 rounding of the activations)
+// and one fused multiply-add.
+__device__ __forceinline__ float silu(float h) {
   float t;
-  asm("tanh.approx.f32 %0, %1;" : "=f"(t) : "f"(0.5f * z));
-  return 0.5f * z * (1.0f + t);
+  asm("tanh.approx.f32 %0, %1;" : "=f"(t) : "f"(h));
+  return fmaf(h, t, h);
 }
 
 }  // namespace
@@ -325,16 +328,20 @@ int launch_green_sg(cudaStream_t st, int sms, DevGeom g, WaveDev w, const SgDev&
 
 void pack_surrogate(const float* P, std::vector<__half>& wh, std::vector<float>& w0, std::vector<float>& bias) {
   // layer l's weights as the B operand (N = outputs, K = inputs), rows past
-  // the output layer's three left zero
+  // the output layer's three left zero; the layers that feed a SiLU (all but
+  // the output layer) halved, so that the kernel's accumulators are z / 2
+  auto scale = [](int l) { return l < sg::kLayers - 1 ? 0.5f : 1.0f; };
   wh.assign(kSgHalves, __float2half(0.0f));
   for (int l = 1; l < sg::kLayers; ++l) {
     const int fi = sg::layer_in(l), fo = sg::layer_out(l);
     __half* dst = wh.data() + (size_t)(l - 1) * (kSgOperandBytes / 2);
     for (int o = 0; o < fo; ++o)
-      for (int k = 0; k < fi; ++k) dst[sg_core_off(o, k) / 2] = __float2half(P[sg::w_off(l) + o + fo * k]);
+      for (int k = 0; k < fi; ++k)
+        dst[sg_core_off(o, k) / 2] = __float2half(scale(l) * P[sg::w_off(l) + o + fo * k]);
   }
-  w0.assign(P + sg::w_off(0), P + sg::w_off(0) + sg::kWidth * sg::kIn);
+  w0.resize(sg::kWidth * sg::kIn);
+  for (int e = 0; e < sg::kWidth * sg::kIn; ++e) w0[e] = scale(0) * P[sg::w_off(0) + e];
   bias.assign(kSgBias, 0.0f);
   for (int l = 0; l < sg::kLayers; ++l)
-    for (int o = 0; o < sg::layer_out(l); ++o) bias[l * sg::kWidth + o] = P[sg::b_off(l) + o];
+    for (int o = 0; o < sg::layer_out(l); ++o) bias[l * sg::kWidth + o] = scale(l) * P[sg::b_off(l) + o];
 }

@@ -230,25 +230,27 @@ __device__ __forceinline__ int pair_cell(const DevGeom& g, double h, size_t p) {
   return judge_cell(sqrt(dx * dx + dy * dy) / h, (g.xq[j + 2 * g.n] + h) / h, (g.fxyz[i + 2 * g.tn] + h) / h);
 }
 
-// Per cell, the least-squares factor m of (network - series) = m Re(series)
-// over the samples, for A and for S: acc[4c..4c+3] += {dA Re A, (Re A)^2,
-// dS Re S, (Re S)^2} (acc zeroed by the caller).
+// Per cell, the sampled sums acc[4c..4c+3] += {(network - series)^2,
+// (Re series)^2} of the A entries, then of the S entries (acc zeroed by the
+// caller): the cell's RMS relative error of the network is the square root
+// of their ratio.
 __global__ void k_judge_fit(DevGeom g, double h, const uint32_t* __restrict__ list, int ns,
                             const double2* __restrict__ g1, const double2* __restrict__ g2, double* __restrict__ acc) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= ns) return;
   const int c = pair_cell(g, h, list[k]);
   const double2 a1 = g1[k], a2 = g2[k], s1 = g1[ns + k], s2 = g2[ns + k];
-  atomicAdd(acc + 4 * c, (a1.x - a2.x) * a2.x);
+  atomicAdd(acc + 4 * c, (a1.x - a2.x) * (a1.x - a2.x) + (a1.y - a2.y) * (a1.y - a2.y));
   atomicAdd(acc + 4 * c + 1, a2.x * a2.x);
-  atomicAdd(acc + 4 * c + 2, (s1.x - s2.x) * s2.x);
+  atomicAdd(acc + 4 * c + 2, (s1.x - s2.x) * (s1.x - s2.x) + (s1.y - s2.y) * (s1.y - s2.y));
   atomicAdd(acc + 4 * c + 3, s2.x * s2.x);
 }
 
 // The error probe: in place, every pair the surrogate evaluates (the
 // criterion of k_pair_keys' bins 4 and 5, copied body blocks included)
-// becomes its cell's modelled network error, m Re(entry), for A and S;
-// every other pair 0.
+// becomes its cell's RMS relative error times the real part of the entry,
+// for A and S -- the network's error with its cell's size and the same sign
+// everywhere, the coherent case; every other pair 0.
 __global__ void k_probe_far(DevGeom g, double h, double far, const double* __restrict__ acc, double2* __restrict__ A,
                             double2* __restrict__ S) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y;
@@ -263,8 +265,8 @@ __global__ void k_probe_far(DevGeom g, double h, double far, const double* __res
     if (sqrt(dx * dx + dy * dy + dz * dz) > far * g.pnsz[j] &&
         sg::in_domain(rr / h, (zq + h) / h, (zp + h) / h, sg::kKmin)) {
       const int c = judge_cell(rr / h, (zq + h) / h, (zp + h) / h);
-      ma = acc[4 * c + 1] > 0.0 ? acc[4 * c] / acc[4 * c + 1] : 0.0;
-      ms = acc[4 * c + 3] > 0.0 ? acc[4 * c + 2] / acc[4 * c + 3] : 0.0;
+      ma = acc[4 * c + 1] > 0.0 ? sqrt(acc[4 * c] / acc[4 * c + 1]) : 0.0;
+      ms = acc[4 * c + 3] > 0.0 ? sqrt(acc[4 * c + 2] / acc[4 * c + 3]) : 0.0;
     }
   }
   A[p] = make_double2(ma * A[p].x, 0.0);
@@ -1816,10 +1818,10 @@ constexpr double kJudgeSafety = 1.0;
 //   e      the network's relative error on the far-pair entries of A and S,
 //          from the pairs sampled during the assembly (k_sample_err);
 //   the error model: per cell of the network's input domain (R/h x source
-//          depth x field depth), the factor m with network - series =
-//          m Re(series) fitted to the samples of that cell (k_judge_fit);
+//          depth x field depth), the RMS of (network - series) relative to
+//          the series' real parts over the samples of that cell (k_judge_fit);
 //   the probe: every far-pair entry of A and S replaced by its cell's
-//          modelled error m Re(entry) (k_probe_far), the first-order change
+//          error taken coherent, r Re(entry) (k_probe_far), the first-order change
 //          of the solution, dX = (L U)^-1 (dB - dA X), carried through the
 //          force reductions: the estimated change of each output, relative
 //          to the output.

@@ -282,10 +282,10 @@ int hams_ctx_set_surrogate_range(hams_ctx *ctx, double kmin, double kmax);
 /* The series judges the surrogate, frequency by frequency (no counterpart in
  * the reference, which has no surrogate).  With tol > 0, every frequency the
  * network serves (mixed precision, LU solver, no lids) is checked after its
- * solve: the series re-evaluates a sample of about 16,000 far pairs, and
- * the network's error per cell of its input domain (R/h x source depth x
- * field depth) is fitted to them as a multiple of the entries; that modelled
- * error, put in place of every far-pair entry of A and S, is carried to
+ * solve: the series re-evaluates a sample of about 16,000 far pairs, giving
+ * the network's RMS relative error per cell of its input domain (R/h x
+ * source depth x field depth); that error, taken coherent (every far-pair
+ * entry of A and S replaced by its cell's error times the entry), is carried to
  * first order through the factorisation already made and the force
  * reductions, giving the estimated error of added mass, damping and
  * excitation.  When the largest (times a safety factor calibrated on the
