@@ -43,7 +43,8 @@ UNIT = "freq-solves/s"
 RHO, G = 1025.0, 9.81
 LANES = 8  # frequencies in flight in hams_solve_batch (the library's default)
 SG_FAR = hams_b200.SURROGATE_FAR  # surrogate pairs: centre distance beyond 3 source-panel sizes
-SG_K_RANGE = hams_b200.SURROGATE_K_RANGE
+SG_K_RANGE = hams_b200.SURROGATE_K_RANGE  # the network's whole domain
+SG_TOL = hams_b200.SURROGATE_TOL  # the series judges each frequency against this bar
 
 
 def _peaks():
@@ -273,6 +274,7 @@ def run_form(hb, dev, geom, case, prec, omegas, betas, warmup, steps, barrier, w
                      body_blocks=blocks)
     if sg is not None:
         ctx.set_surrogate(sg, SG_FAR, SG_K_RANGE)
+        ctx.set_surrogate_tolerance(SG_TOL)
     waves = [hb.wave_properties(om, case["depth"], G) for om in omegas]
     if warmup:  # at least one frequency per lane, so that no lane is created inside the timed region
         ctx.solve_batch([waves[s % len(waves)] for s in range(max(warmup, LANES))], betas)
@@ -287,10 +289,12 @@ def run_form(hb, dev, geom, case, prec, omegas, betas, warmup, steps, barrier, w
     launches, libcalls = ctx.launch_count() - l0, ctx.library_call_count() - lib0
     clocks = sampler.stop() if sampler else None
     tm = ctx.timings()  # the context's own last frequency
+    resolved = ctx.note().count("re-solved with the series")  # frequencies the series judgement took back
     barrier()
     ctx.close()
     results = [tuple(r[k] for r in res) for k in range(steps)] if (want_results and res is not None) else []
-    return dict(ms=ms, launches=launches, lib_calls=libcalls, timings=tm, results=results, clocks=clocks)
+    return dict(ms=ms, launches=launches, lib_calls=libcalls, timings=tm, results=results, clocks=clocks,
+                resolved=resolved)
 
 
 def surrogate_kernel_time(hb, dev, geom, case, betas, sg, tol, blocks=0, reps=5):
@@ -323,6 +327,7 @@ def e2e_form(hb, dev, case, xyz, ncn, ncon, cnt, xr, prec, omegas, betas, steps,
                      body_blocks=blocks)
     if sg is not None:
         ctx.set_surrogate(sg, SG_FAR, SG_K_RANGE)
+        ctx.set_surrogate_tolerance(SG_TOL)
     t1 = time.perf_counter()
     # the results are in host memory when solve_batch returns; freeing the context is not timed
     ctx.solve_batch([hb.wave_properties(omegas[s % len(omegas)], case["depth"], G) for s in range(steps)], betas)
@@ -422,6 +427,8 @@ def gpu_arm(args):
         pr, on, _, tol, blocks = FORMS[name]
         forms[name] = {"value": v, "precision": pr, "surrogate": on, "body_blocks": bool(blocks),
                        "refine_tol": tol if pr == "mixed" else None, "rel_err_vs_fp64": None}
+        if on:
+            forms[name]["resolved_with_series"] = f"{r['resolved']} of {args.steps}"
         if "fp64" in runs and name != "fp64":
             # worst of the relative Frobenius errors of added mass, damping and excitation against the
             # plain fp64 form (every pair computed), per frequency
@@ -440,8 +447,10 @@ def gpu_arm(args):
                        "l2": "no flush: the 5400x5400 complex system (0.47 GB) and pair tables exceed the 126 MB L2",
                        "parallelism": f"frequency shards x{ws}, {LANES} frequencies in flight per GPU",
                        "frequencies": "K solves per rank spread evenly over the 40-frequency sweep",
-                       "surrogate": (f"far pairs beyond {SG_FAR} panel sizes, frequencies with K = k0 h tanh(k0 h) in "
-                                     f"[{SG_K_RANGE[0]}, {SG_K_RANGE[1]}]") if sg_main is not None else None,
+                       "surrogate": (f"far pairs beyond {SG_FAR} panel sizes over the network's K = k0 h tanh(k0 h) "
+                                     f"domain [{SG_K_RANGE[0]}, {SG_K_RANGE[1]}]; each frequency judged by the series "
+                                     f"(sampled far pairs, error model carried through the solve) and re-solved with the "
+                                     f"series when the estimate exceeds {SG_TOL:g}") if sg_main is not None else None,
                        "body_blocks": ("Green functions of the 25 distinct (field body, source body) blocks of the "
                                        "81 computed, the others copied (identical translated cylinders)")
                                       if blk_main else None},

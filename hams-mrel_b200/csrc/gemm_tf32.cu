@@ -86,17 +86,19 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatil
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&v)[16]) {
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
   asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
-      "%15}, [%16];"
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+      "%15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
       : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
-        "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+        "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]),
+        "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]),
+        "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
       : "r"(taddr));
 }
 
 template <int BN, int STAGES>
-__global__ void __launch_bounds__(kThreads, 1)
+__global__ void __launch_bounds__(kThreads, BN <= 128 ? 2 : 1)
     k_gemm_tf32(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, float* __restrict__ C,
                 int ldc, int M, int N, int K, float alpha, float beta, int c_rowmajor, int* err) {
   using T = Tile<BN, STAGES>;
@@ -196,18 +198,19 @@ __global__ void __launch_bounds__(kThreads, 1)
   } else {  // epilogue: warps 2-5, warp w reads tensor-memory lanes 32 (w % 4) ...
     const int q = warp & 3, row = m0 + 32 * q + lane;
     const bool live = row < M;
-    // C of one 16-column chunk into registers: all loads issued before any
-    // store of the tile, so they overlap (the first chunk's under the main loop)
-    auto load_chunk = [&](int c0, float (&cv)[16]) {
+    // C of one 32-column chunk into registers, issued ahead of the previous
+    // chunk's stores (the first chunk's under the main loop)
+    constexpr int kCh = kBN < 32 ? kBN : 32;
+    auto load_chunk = [&](int c0, float (&cv)[kCh]) {
 #pragma unroll
-      for (int j = 0; j < 16; ++j) {
+      for (int j = 0; j < kCh; ++j) {
         const int col = n0 + c0 + j;
         cv[j] = (beta != 0.0f && live && col < N)
                     ? (c_rowmajor ? C[(size_t)row * ldc + col] : C[(size_t)col * ldc + row])
                     : 0.0f;
       }
     };
-    float cn[16];
+    float cn[kCh];
     load_chunk(0, cn);
     bool ok = mbar_wait(bar_acc, 0, abort_flag);
     if (!ok) {
@@ -219,17 +222,17 @@ __global__ void __launch_bounds__(kThreads, 1)
     if (ok) {
       const uint32_t trow = tbase + ((uint32_t)(32 * q) << 16);
 #pragma unroll 1
-      for (int c0 = 0; c0 < kBN; c0 += 16) {
-        float cc[16];
+      for (int c0 = 0; c0 < kBN; c0 += kCh) {
+        float cc[kCh];
 #pragma unroll
-        for (int j = 0; j < 16; ++j) cc[j] = cn[j];
-        if (c0 + 16 < kBN) load_chunk(c0 + 16, cn);  // in flight while this chunk is written
-        uint32_t v[16];
-        tmem_ld16(trow + (uint32_t)c0, v);
+        for (int j = 0; j < kCh; ++j) cc[j] = cn[j];
+        if (c0 + kCh < kBN) load_chunk(c0 + kCh, cn);  // in flight while this chunk is written
+        uint32_t v[32];
+        tmem_ld32(trow + (uint32_t)c0, v);
         asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
         if (live) {
 #pragma unroll
-          for (int j = 0; j < 16; ++j) {
+          for (int j = 0; j < kCh; ++j) {
             const int col = n0 + c0 + j;
             if (col < N) {
               float* dst = c_rowmajor ? C + (size_t)row * ldc + col : C + (size_t)col * ldc + row;

@@ -21,10 +21,12 @@ PREC_FP64 = 0
 PREC_MIXED = 1
 LU_BLOCK_TF32, LU_BLOCK_EMU, LU_LIBRARY = 0, 1, 2
 SOLVER_LU, SOLVER_GMRES = 1, 2
-# The surrogate form's defaults: network for pairs farther apart than 3 source-panel sizes, at the
-# frequencies whose K = k0 h tanh(k0 h) lies in SURROGATE_K_RANGE.
+# The surrogate form's defaults: network for pairs farther apart than 3 source-panel sizes, over
+# the network's whole K = k0 h tanh(k0 h) domain, each frequency judged by the series against the
+# 1e-4 bar (hams_ctx_set_surrogate_tolerance) and re-solved with the series above it.
 SURROGATE_FAR = 3.0
-SURROGATE_K_RANGE = (0.3, 21.5)
+SURROGATE_K_RANGE = (0.04, 40.0)
+SURROGATE_TOL = 1e-4
 
 c_int = ctypes.c_int32
 c_dbl = ctypes.c_double
