@@ -289,7 +289,7 @@ def run_form(hb, dev, geom, case, prec, omegas, betas, warmup, steps, barrier, w
     launches, libcalls = ctx.launch_count() - l0, ctx.library_call_count() - lib0
     clocks = sampler.stop() if sampler else None
     tm = ctx.timings()  # the context's own last frequency
-    resolved = ctx.note().count("re-solved with the series")  # frequencies the series judgement took back
+    resolved = ctx.note().count("surrogate estimate")  # frequencies the series judgement took back
     barrier()
     ctx.close()
     results = [tuple(r[k] for r in res) for k in range(steps)] if (want_results and res is not None) else []
@@ -449,8 +449,9 @@ def gpu_arm(args):
                        "frequencies": "K solves per rank spread evenly over the 40-frequency sweep",
                        "surrogate": (f"far pairs beyond {SG_FAR} panel sizes over the network's K = k0 h tanh(k0 h) "
                                      f"domain [{SG_K_RANGE[0]}, {SG_K_RANGE[1]}]; each frequency judged by the series "
-                                     f"(sampled far pairs, error model carried through the solve) and re-solved with the "
-                                     f"series when the estimate exceeds {SG_TOL:g}") if sg_main is not None else None,
+                                     f"(sampled far pairs, error model carried through the solve); above {SG_TOL:g} the series "
+                                     f"takes it back: far pairs from the series, refined from the network's solution "
+                                     f"with the network's factors") if sg_main is not None else None,
                        "body_blocks": ("Green functions of the 25 distinct (field body, source body) blocks of the "
                                        "81 computed, the others copied (identical translated cylinders)")
                                       if blk_main else None},
@@ -592,7 +593,7 @@ def c3_arm(args):
     el = time.perf_counter() - t0
     clocks = sampler.stop()
     nsolve = sum(len(c[0]["omegas"]) for c in cases)
-    line = {"metric": "freq-solves/s, 128 heterogeneous cases (BASELINE config 3)", "value": nsolve / el,
+    line = {"metric": "freq-solves/s, 128 heterogeneous seeded cases (one or two bodies, 220-5,757 panels)", "value": nsolve / el,
             "unit": UNIT, "n_gpus": 1, "steps": nsolve, "warmup": 1, "ms_per_step": 1e3 * el / nsolve,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64 assembly, c64 LU + f64 refinement",
             "data": "synthetic",

@@ -246,31 +246,110 @@ __global__ void k_judge_fit(DevGeom g, double h, const uint32_t* __restrict__ li
   atomicAdd(acc + 4 * c + 3, s2.x * s2.x);
 }
 
-// The error probe: in place, every pair the surrogate evaluates (the
-// criterion of k_pair_keys' bins 4 and 5, copied body blocks included)
-// becomes its cell's RMS relative error times the real part of the entry,
-// for A and S -- the network's error with its cell's size and the same sign
-// everywhere, the coherent case; every other pair 0.
-__global__ void k_probe_far(DevGeom g, double h, double far, const double* __restrict__ acc, double2* __restrict__ A,
-                            double2* __restrict__ S) {
+// The judgement's cell map: for every pair (i, j) (entry i + j tn) the cell
+// of the network's input domain when the network evaluates the pair (the
+// criterion of k_pair_keys' bins 4 and 5, copied body blocks included), else
+// kNoCell.  Frequency-independent: built once with the surrogate.
+constexpr unsigned char kNoCell = 255;
+static_assert(kJCells < kNoCell, "cell index must fit below kNoCell");
+__global__ void k_probe_map(DevGeom g, double h, double far, unsigned char* __restrict__ map) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y;
   if (i >= g.tn) return;
-  const size_t p = (size_t)i + (size_t)j * g.tn;
   const double dx = g.xq[j] - g.fxyz[i], dy = g.xq[j + g.n] - g.fxyz[i + g.tn];
   const double rr = sqrt(dx * dx + dy * dy);
   const int b = hams::fin_branch(rr, h);
-  double ma = 0.0, ms = 0.0;
+  unsigned char cell = kNoCell;
   if (b == hams::kEigenE || b == hams::kEigen) {
     const double zq = g.xq[j + 2 * g.n], zp = g.fxyz[i + 2 * g.tn], dz = zq - zp;
     if (sqrt(dx * dx + dy * dy + dz * dz) > far * g.pnsz[j] &&
-        sg::in_domain(rr / h, (zq + h) / h, (zp + h) / h, sg::kKmin)) {
-      const int c = judge_cell(rr / h, (zq + h) / h, (zp + h) / h);
-      ma = acc[4 * c + 1] > 0.0 ? sqrt(acc[4 * c] / acc[4 * c + 1]) : 0.0;
-      ms = acc[4 * c + 3] > 0.0 ? sqrt(acc[4 * c + 2] / acc[4 * c + 3]) : 0.0;
+        sg::in_domain(rr / h, (zq + h) / h, (zp + h) / h, sg::kKmin))
+      cell = (unsigned char)judge_cell(rr / h, (zq + h) / h, (zp + h) / h);
+  }
+  map[(size_t)i + (size_t)j * g.tn] = cell;
+}
+
+// The probe scales of this frequency: per cell the network's RMS relative
+// error on A (scale[2c]) and S (scale[2c + 1]) from the sampled sums acc.
+// The error probe of an entry is its cell's scale times the entry's real
+// part -- the network's error with its cell's size and the same sign
+// everywhere, the coherent case; 0 for the pairs the network leaves alone.
+__global__ void k_probe_scales(const double* __restrict__ acc, double* __restrict__ scale) {
+  for (int c = threadIdx.x; c < kJCells; c += blockDim.x) {
+    scale[2 * c] = acc[4 * c + 1] > 0.0 ? sqrt(acc[4 * c] / acc[4 * c + 1]) : 0.0;
+    scale[2 * c + 1] = acc[4 * c + 3] > 0.0 ? sqrt(acc[4 * c + 2] / acc[4 * c + 3]) : 0.0;
+  }
+}
+
+// B (tn x nrhs, ld tn) -= PA X with PA the error probe of A and X (n x nrhs,
+// ld n, complex64), the probe never stored; FP32 products and sums (the
+// result is an error estimate).  A block: 32 rows x 64 right-hand sides, j
+// in tiles of 32 through shared memory, each thread 2 rows x 4 right-hand
+// sides.  Grid: ceil(tn / 32) blocks of 256 threads.
+constexpr int kPrRows = 32, kPrCols = 64, kPrJ = 32;
+__global__ void __launch_bounds__(256) k_probe_apply(DevGeom g, const unsigned char* __restrict__ map,
+                                                     const double* __restrict__ scale, const double2* __restrict__ A,
+                                                     const float2* __restrict__ X, int nrhs,
+                                                     double2* __restrict__ B) {
+  __shared__ float sP[kPrJ][kPrRows];
+  __shared__ float2 sX[kPrJ][kPrCols];
+  __shared__ float sScale[kJCells];
+  const int t = threadIdx.x, i0 = blockIdx.x * kPrRows, rg = t & 15, cg = t >> 4;
+  for (int c = t; c < kJCells; c += blockDim.x) sScale[c] = (float)scale[2 * c];
+  for (int k0 = 0; k0 < nrhs; k0 += kPrCols) {
+    float2 a[2][4];
+#pragma unroll
+    for (int r = 0; r < 2; ++r)
+#pragma unroll
+      for (int q = 0; q < 4; ++q) a[r][q] = make_float2(0.0f, 0.0f);
+    for (int j0 = 0; j0 < g.n; j0 += kPrJ) {
+      __syncthreads();
+      {
+        const int il = t & 31, i = i0 + il;
+#pragma unroll
+        for (int q = 0; q < kPrJ / 8; ++q) {
+          const int jl = (t >> 5) + 8 * q, j = j0 + jl;
+          float v = 0.0f;
+          if (i < g.tn && j < g.n) {
+            const size_t p = (size_t)i + (size_t)j * g.tn;
+            const unsigned char cell = map[p];
+            if (cell != kNoCell) v = sScale[cell] * (float)A[p].x;
+          }
+          sP[jl][il] = v;
+        }
+        const int jl = t & 31, j = j0 + jl;
+#pragma unroll
+        for (int q = 0; q < kPrCols / 8; ++q) {
+          const int kl = (t >> 5) + 8 * q, k = k0 + kl;
+          sX[jl][kl] = (j < g.n && k < nrhs) ? X[(size_t)j + (size_t)k * g.n] : make_float2(0.0f, 0.0f);
+        }
+      }
+      __syncthreads();
+#pragma unroll 8
+      for (int jl = 0; jl < kPrJ; ++jl) {
+        const float p0 = sP[jl][2 * rg], p1 = sP[jl][2 * rg + 1];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const float2 x = sX[jl][4 * cg + q];
+          a[0][q].x = fmaf(p0, x.x, a[0][q].x);
+          a[0][q].y = fmaf(p0, x.y, a[0][q].y);
+          a[1][q].x = fmaf(p1, x.x, a[1][q].x);
+          a[1][q].y = fmaf(p1, x.y, a[1][q].y);
+        }
+      }
+    }
+#pragma unroll
+    for (int r = 0; r < 2; ++r) {
+      const int i = i0 + 2 * rg + r;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int k = k0 + 4 * cg + q;
+        if (i < g.tn && k < nrhs) {
+          double2* o = B + (size_t)i + (size_t)k * g.tn;
+          *o = make_double2(o->x - (double)a[r][q].x, o->y - (double)a[r][q].y);
+        }
+      }
     }
   }
-  A[p] = make_double2(ma * A[p].x, 0.0);
-  S[p] = make_double2(ms * S[p].x, 0.0);
 }
 
 template <int BR>
@@ -455,9 +534,15 @@ __global__ void k_dbc_weights(DevGeom g, WaveDev w, IncWave q, const double* __r
 constexpr int kChunk = 256;  // source panels per chunk (chunks never straddle bodies)
 
 // part(c, I, k): k < 6 radiation mode k of the chunk's body, k >= 6 heading k-6.
+// With PROBE the entries of S are replaced by their error probe (the scale
+// of their cell, map and k_probe_scales, times Re S): the right-hand sides of
+// the probe.
+template <bool PROBE>
 __global__ void __launch_bounds__(128) k_rhs_partial(DevGeom g, const double2* __restrict__ S,
                                                      const int2* __restrict__ chunks, const double2* __restrict__ wd,
-                                                     int nbeta, double2* __restrict__ part) {
+                                                     int nbeta, double2* __restrict__ part,
+                                                     const unsigned char* __restrict__ map = nullptr,
+                                                     const double* __restrict__ scale = nullptr) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   int c = blockIdx.y;
   if (i >= g.tn) return;
@@ -467,6 +552,10 @@ __global__ void __launch_bounds__(128) k_rhs_partial(DevGeom g, const double2* _
   double rr[6] = {0, 0, 0, 0, 0, 0}, ri[6] = {0, 0, 0, 0, 0, 0};
   for (int j = j0; j < j1; ++j) {
     double2 s = S[(size_t)i + (size_t)j * g.tn];
+    if (PROBE) {
+      const unsigned char cell = map[(size_t)i + (size_t)j * g.tn];
+      s = make_double2(cell != kNoCell ? scale[2 * cell + 1] * s.x : 0.0, 0.0);
+    }
 #pragma unroll
     for (int m = 0; m < 6; ++m) {
       double nm = g.nrm[j + (size_t)m * g.n];
@@ -480,6 +569,10 @@ __global__ void __launch_bounds__(128) k_rhs_partial(DevGeom g, const double2* _
     int nbb = min(8, nbeta - b0);
     for (int j = j0; j < j1; ++j) {
       double2 s = S[(size_t)i + (size_t)j * g.tn];
+      if (PROBE) {
+        const unsigned char cell = map[(size_t)i + (size_t)j * g.tn];
+        s = make_double2(cell != kNoCell ? scale[2 * cell + 1] * s.x : 0.0, 0.0);
+      }
 #pragma unroll
       for (int b = 0; b < 8; ++b)
         if (b < nbb) {
@@ -788,6 +881,8 @@ struct hams_ctx {
   DBuf<uint32_t> sg_samp;  // sampled surrogate pairs: sg_ns4 of bin 4, then sg_ns5 of bin 5
   int sg_ns4 = 0, sg_ns5 = 0;
   DBuf<double2> sg_g1, sg_g2;  // the sampled A and S entries from the network, then from the series
+  DBuf<unsigned char> sg_map;  // the judgement's cell of every pair the network evaluates (k_probe_map)
+  DBuf<double> sg_scale;       // this frequency's probe scale per cell (k_probe_scales)
   DBuf<double> sg_red, sg_cells, outbuf2;
   double sg_judge[8] = {};  // e_A, e_S, kappa_A, kappa_B, kappa_X, estimate, re-solved with the series, samples
   std::string note;  // what the last solve changed on its own (fallbacks), or empty
@@ -1054,6 +1149,7 @@ static int make_lane(hams_ctx* c, hams_ctx** out) {
     l->sgd = c->sgd;
     l->sg_tol = c->sg_tol;
     l->sg_samp.view(c->sg_samp);
+    l->sg_map.view(c->sg_map);
     l->sg_ns4 = c->sg_ns4;
     l->sg_ns5 = c->sg_ns5;
     l->sms = c->sms;
@@ -1232,6 +1328,36 @@ static WaveDev wave_dev(const hams_ctx* c, const hams_wave* w) {
 // Assemble A (tn x n) and the right-hand sides B (tn x (6nb+nbeta)) on the
 // device; force_series keeps the series for the far pairs of a surrogate
 // context (the re-solve of a frequency the series judged).
+// The far pairs (bins 4 and 5 of k_pair_keys) from the series: EIGENE and
+// EIGEN, as their own bins would (FinGreen3D.f90:413-660).
+static int far_series(hams_ctx* c, const WaveDev& wd) {
+  const long long ce = c->bin_off[5] - c->bin_off[4], cg = c->bin_off[6] - c->bin_off[5];
+  if (ce > 0)
+    launch_green_series(hams::kEigenE, (unsigned)((ce + 127) / 128), c->st, c->g, wd, c->wvn.p, c->mt,
+                        c->pairs.p + c->bin_off[4], ce, c->rs.p, c->rd.p, c->A.p, c->S.p, c->ovf.p);
+  if (cg > 0)
+    k_green_fin<3><<<(unsigned)((cg + 127) / 128), 128, 0, c->st>>>(c->g, wd, c->wvn.p, c->mt,
+                                                                    c->pairs.p + c->bin_off[5], cg, c->rs.p, c->rd.p,
+                                                                    c->A.p, c->S.p, c->ovf.p);
+  return launch_check(c, (ce > 0) + (cg > 0));
+}
+
+// The copies of the identical body blocks, then the right-hand sides B from S
+// and this frequency's diffraction weights (already in wd).
+static int copy_blocks_and_rhs(hams_ctx* c, int nbeta) {
+  const int tn = c->tn, nb = c->nb;
+  if (c->nblk) {
+    dim3 grid((unsigned)std::min((c->blk_rows + 255) / 256, 4), (unsigned)std::min(c->blk_cols, 1024),
+              (unsigned)c->nblk);
+    k_copy_blocks<<<grid, 256, 0, c->st>>>(c->blk_list.p, c->tn, c->A.p, c->S.p);
+    TRY(launch_check(c));
+  }
+  const int nch = (int)c->chunks_h.size();
+  k_rhs_partial<false><<<dim3((tn + 127) / 128, nch), 128, 0, c->st>>>(c->g, c->S.p, c->chunks.p, c->wd.p, nbeta, c->part.p);
+  k_rhs_final<<<(tn + 127) / 128, 128, 0, c->st>>>(tn, nb, nch, c->chunk_body.p, c->part.p, nbeta, c->B.p);
+  return launch_check(c, 2);
+}
+
 static int assemble_dev(hams_ctx* c, const hams_wave* w, int nbeta, bool force_series = false) {
   const int n = c->n, tn = c->tn, nb = c->nb, nrhs = 6 * nb + nbeta;
   WaveDev wd = wave_dev(c, w);
@@ -1300,15 +1426,7 @@ static int assemble_dev(hams_ctx* c, const hams_wave* w, int nbeta, bool force_s
           TRY(launch_check(c, 3));
         }
       } else {
-        long long ce = c->bin_off[5] - c->bin_off[4], cg = c->bin_off[6] - c->bin_off[5];
-        if (ce > 0)
-          launch_green_series(hams::kEigenE, (unsigned)((ce + 127) / 128), c->st, c->g, wd, c->wvn.p, c->mt,
-                              c->pairs.p + c->bin_off[4], ce, c->rs.p, c->rd.p, c->A.p, c->S.p, c->ovf.p);
-        if (cg > 0)
-          k_green_fin<3><<<(unsigned)((cg + 127) / 128), 128, 0, c->st>>>(c->g, wd, c->wvn.p, c->mt,
-                                                                          c->pairs.p + c->bin_off[5], cg, c->rs.p,
-                                                                          c->rd.p, c->A.p, c->S.p, c->ovf.p);
-        TRY(launch_check(c, (ce > 0) + (cg > 0)));
+        TRY(far_series(c, wd));
         c->sg_used = 0;
       }
     }
@@ -1331,11 +1449,77 @@ static int assemble_dev(hams_ctx* c, const hams_wave* w, int nbeta, bool force_s
     k_dbc_weights<<<dim3((n + 127) / 128, nbeta), 128, 0, c->st>>>(c->g, wd, q, c->beta.p, nbeta, c->wd.p);
     TRY(launch_check(c));
   }
-  k_rhs_partial<<<dim3((tn + 127) / 128, nch), 128, 0, c->st>>>(c->g, c->S.p, c->chunks.p, c->wd.p, nbeta, c->part.p);
+  k_rhs_partial<false><<<dim3((tn + 127) / 128, nch), 128, 0, c->st>>>(c->g, c->S.p, c->chunks.p, c->wd.p, nbeta, c->part.p);
   TRY(launch_check(c));
   k_rhs_final<<<(tn + 127) / 128, 128, 0, c->st>>>(tn, nb, nch, c->chunk_body.p, c->part.p, nbeta, c->B.p);
   TRY(launch_check(c));
   CU(cudaEventRecord(c->ev[2], c->st));
+  return 0;
+}
+
+// Xf (n x nrhs) <- (L U)^-1 Xf with the factors the last mixed solve left in Af.
+static int mixed_apply(hams_ctx* c, int nrhs) {
+  const int n = c->n, lda = mixed_lu_ld(n);
+  if (c->lu_used == HAMS_LU_LIBRARY) {
+    CUS(cusolverDnCgetrs(c->solver, CUBLAS_OP_N, n, nrhs, (cuComplex*)c->Af.p, lda, c->ipiv.p, (cuComplex*)c->Xf.p, n,
+                         c->info.p));
+    c->lib_calls += 1;
+    return 0;
+  }
+  long long la = 0, lb = 0;
+  const int rc = mixed_lu_solve(c->st, c->blas, c->lu_used == HAMS_LU_BLOCK_TF32, CUBLAS_COMPUTE_32F_EMULATED_16BFX9,
+                                n, lda, nrhs, c->Af.p, c->perm.p, c->Xf.p, c->luw.p, c->info.p + 1, &la, &lb);
+  c->launches += la;
+  c->lib_calls += lb;
+  if (rc) return fail(HAMS_ERR_CUDA, "block LU solve failed (%d)", rc);
+  return 0;
+}
+
+// FP64 iterative refinement of X (n x nrhs) for M X = rhs (ld ldr = n) with
+// the complex64 factors in Af: R = rhs - M X, X += (L U)^-1 R until the
+// residual of every column is below refine_tol of that column's scale.  X
+// may come from another matrix close to M (the correction then carries the
+// difference as well).  Returns HAMS_ERR_NUMERIC when the refinement stalls.
+static int mixed_refine(hams_ctx* c, const double2* M, const double2* rhs, int ldr, int nrhs) {
+  const int n = c->n;
+  const cuDoubleComplex one = make_cuDoubleComplex(1.0, 0.0), mone = make_cuDoubleComplex(-1.0, 0.0);
+  const size_t nx = (size_t)n * nrhs;
+  const bool block = c->lu_used != HAMS_LU_LIBRARY;
+  const double tol = c->opts.refine_tol > 0.0 ? c->opts.refine_tol : 1e-12;
+  const int maxit = c->opts.refine_max > 0 ? c->opts.refine_max : 30;
+  std::vector<double> ratio(nrhs);
+  double prev = 1e300;
+  c->refine_sweeps = 0;
+  c->ir_rate = 0.0;
+  for (int it = 0;; ++it) {
+    // R = rhs - M_fp64 X   (M still holds the FP64 matrix)
+    CU(cudaMemcpy2DAsync(c->R.p, (size_t)n * 16, rhs, (size_t)ldr * 16, (size_t)n * 16, nrhs, cudaMemcpyDeviceToDevice, c->st));
+    CUB_(cublasZgemm(c->blas, CUBLAS_OP_N, CUBLAS_OP_N, n, nrhs, n, &mone, (const cuDoubleComplex*)M, n,
+                     (cuDoubleComplex*)c->X.p, n, &one, (cuDoubleComplex*)c->R.p, n));
+    c->lib_calls += 1;
+    k_colnorm_ratio<<<nrhs, 256, 0, c->st>>>(c->R.p, rhs, n, n, c->colratio.p);  // ldr == n here
+    TRY(launch_check(c));
+    // the relative residual is checked against the rhs column scale
+    CU(cudaMemcpyAsync(ratio.data(), c->colratio.p, nrhs * 8, cudaMemcpyDeviceToHost, c->st));
+    int werr = 0;
+    if (block) CU(cudaMemcpyAsync(&werr, c->info.p + 1, sizeof(int), cudaMemcpyDeviceToHost, c->st));
+    CU(cudaStreamSynchronize(c->st));
+    if (werr) return fail(HAMS_ERR_CUDA, "block LU solve: a tensor-core GEMM gave up waiting on its pipeline (%d)", werr);
+    double worst = 0.0;
+    for (double r : ratio) worst = std::max(worst, r);
+    c->refine_sweeps = it;
+    if (it > 0 && prev > 0.0) c->ir_rate = std::max(c->ir_rate, worst / prev);
+    if (!(worst == worst)) return fail(HAMS_ERR_NUMERIC, "non-finite residual in iterative refinement");
+    if (worst <= tol) break;
+    if (it >= maxit) return fail(HAMS_ERR_NUMERIC, "iterative refinement: %.3e after %d sweeps", worst, it);
+    if (it > 4 && worst > 0.5 * prev) return fail(HAMS_ERR_NUMERIC, "iterative refinement stalled at %.3e", worst);
+    prev = worst;
+    k_z2c<<<592, 256, 0, c->st>>>(c->R.p, c->Xf.p, nx);
+    TRY(launch_check(c));
+    TRY(mixed_apply(c, nrhs));
+    k_c2z_add<<<592, 256, 0, c->st>>>(c->Xf.p, c->X.p, nx);
+    TRY(launch_check(c));
+  }
   return 0;
 }
 
@@ -1347,7 +1531,6 @@ static int assemble_dev(hams_ctx* c, const hams_wave* w, int nbeta, bool force_s
 // factorisation breaks down or the refinement stalls.
 static int mixed_solve(hams_ctx* c, double2* M, const double2* rhs, int ldr, int nrhs, int kind, int* info_host) {
   const int n = c->n, lda = mixed_lu_ld(n);
-  const cuDoubleComplex one = make_cuDoubleComplex(1.0, 0.0), mone = make_cuDoubleComplex(-1.0, 0.0);
   const size_t nx = (size_t)n * nrhs;
   TRY(c->Af.alloc((size_t)lda * n));
   TRY(c->Xf.alloc(nx));
@@ -1386,61 +1569,12 @@ static int mixed_solve(hams_ctx* c, double2* M, const double2* rhs, int ldr, int
     CU(cudaMemcpyAsync(info_host, c->info.p, sizeof(int), cudaMemcpyDeviceToHost, c->st));
   }
   CU(cudaEventRecord(c->evf, c->st));
-  // Xf <- LU^-1 Xf
-  auto lu_solve = [&]() -> int {
-    if (block) {
-      long long la = 0;
-      int rc = mixed_lu_solve(c->st, n, lda, nrhs, c->Af.p, c->perm.p, c->Xf.p, c->luw.p, c->info.p + 1, &la);
-      c->launches += la;
-      if (rc) return fail(HAMS_ERR_CUDA, "block LU solve failed");
-      return 0;
-    }
-    CUS(cusolverDnCgetrs(c->solver, CUBLAS_OP_N, n, nrhs, (cuComplex*)c->Af.p, lda, c->ipiv.p, (cuComplex*)c->Xf.p, n,
-                         c->info.p));
-    c->lib_calls += 1;
-    return 0;
-  };
   k_z2c<<<592, 256, 0, c->st>>>(c->X.p, c->Xf.p, nx);
   TRY(launch_check(c));
-  TRY(lu_solve());
+  TRY(mixed_apply(c, nrhs));
   k_c2z<<<592, 256, 0, c->st>>>(c->Xf.p, c->X.p, nx);
   TRY(launch_check(c));
-  const double tol = c->opts.refine_tol > 0.0 ? c->opts.refine_tol : 1e-12;
-  const int maxit = c->opts.refine_max > 0 ? c->opts.refine_max : 30;
-  std::vector<double> ratio(nrhs);
-  double prev = 1e300;
-  c->refine_sweeps = 0;
-  c->ir_rate = 0.0;
-  for (int it = 0;; ++it) {
-    // R = rhs - M_fp64 X   (M still holds the FP64 matrix)
-    CU(cudaMemcpy2DAsync(c->R.p, (size_t)n * 16, rhs, (size_t)ldr * 16, (size_t)n * 16, nrhs, cudaMemcpyDeviceToDevice, c->st));
-    CUB_(cublasZgemm(c->blas, CUBLAS_OP_N, CUBLAS_OP_N, n, nrhs, n, &mone, (cuDoubleComplex*)M, n,
-                     (cuDoubleComplex*)c->X.p, n, &one, (cuDoubleComplex*)c->R.p, n));
-    c->lib_calls += 1;
-    k_colnorm_ratio<<<nrhs, 256, 0, c->st>>>(c->R.p, rhs, n, n, c->colratio.p);  // ldr == n here
-    TRY(launch_check(c));
-    // the relative residual is checked against the rhs column scale
-    CU(cudaMemcpyAsync(ratio.data(), c->colratio.p, nrhs * 8, cudaMemcpyDeviceToHost, c->st));
-    int werr = 0;
-    if (block) CU(cudaMemcpyAsync(&werr, c->info.p + 1, sizeof(int), cudaMemcpyDeviceToHost, c->st));
-    CU(cudaStreamSynchronize(c->st));
-    if (werr) return fail(HAMS_ERR_CUDA, "block LU solve: a wait on another block gave up (%d)", werr);
-    double worst = 0.0;
-    for (double r : ratio) worst = std::max(worst, r);
-    c->refine_sweeps = it;
-    if (it > 0 && prev > 0.0) c->ir_rate = std::max(c->ir_rate, worst / prev);
-    if (!(worst == worst)) return fail(HAMS_ERR_NUMERIC, "non-finite residual in iterative refinement");
-    if (worst <= tol) break;
-    if (it >= maxit) return fail(HAMS_ERR_NUMERIC, "iterative refinement: %.3e after %d sweeps", worst, it);
-    if (it > 4 && worst > 0.5 * prev) return fail(HAMS_ERR_NUMERIC, "iterative refinement stalled at %.3e", worst);
-    prev = worst;
-    k_z2c<<<592, 256, 0, c->st>>>(c->R.p, c->Xf.p, nx);
-    TRY(launch_check(c));
-    TRY(lu_solve());
-    k_c2z_add<<<592, 256, 0, c->st>>>(c->Xf.p, c->X.p, nx);
-    TRY(launch_check(c));
-  }
-  return 0;
+  return mixed_refine(c, M, rhs, ldr, nrhs);
 }
 
 // GMRES (IterativeSolvers.f90:324-484, ZGMRES_SOLVE): X (n x nrhs) from the
@@ -1792,22 +1926,6 @@ static int field_dev(hams_ctx* c, const hams_wave* w, int nbeta) {
   return 0;
 }
 
-// Xf (n x nrhs) <- (L U)^-1 Xf with the factors the last mixed solve left in Af.
-static int mixed_apply(hams_ctx* c, int nrhs) {
-  const int n = c->n, lda = mixed_lu_ld(n);
-  if (c->lu_used == HAMS_LU_LIBRARY) {
-    CUS(cusolverDnCgetrs(c->solver, CUBLAS_OP_N, n, nrhs, (cuComplex*)c->Af.p, lda, c->ipiv.p, (cuComplex*)c->Xf.p, n,
-                         c->info.p));
-    c->lib_calls += 1;
-    return 0;
-  }
-  long long la = 0;
-  const int rc = mixed_lu_solve(c->st, n, lda, nrhs, c->Af.p, c->perm.p, c->Xf.p, c->luw.p, c->info.p + 1, &la);
-  c->launches += la;
-  if (rc) return fail(HAMS_ERR_CUDA, "block LU solve failed");
-  return 0;
-}
-
 // Safety factor of the judgement: the largest ratio of a frequency's true
 // error (against the plain series) to its estimate, observed on the
 // 5,400-panel 3 x 3 array of cylinders (h = 50 m) over 0.2-2.5 rad/s, rounded up.
@@ -1821,35 +1939,34 @@ constexpr double kJudgeSafety = 1.0;
 //          depth x field depth), the RMS of (network - series) relative to
 //          the series' real parts over the samples of that cell (k_judge_fit);
 //   the probe: every far-pair entry of A and S replaced by its cell's
-//          error taken coherent, r Re(entry) (k_probe_far), the first-order change
+//          error taken coherent, r Re(entry) (k_probe_scales), the first-order change
 //          of the solution, dX = (L U)^-1 (dB - dA X), carried through the
 //          force reductions: the estimated change of each output, relative
 //          to the output.
-// The estimate is kJudgeSafety times the largest of the three.  A and S are
-// overwritten (the frequency does not read them again).  Requires the mixed
-// solve's factors.
+// The estimate is kJudgeSafety times the largest of the three.  A, S and X
+// are kept, B is overwritten.  Requires the mixed solve's factors.
 static int surrogate_judge(hams_ctx* c, const hams_wave* w, int nbeta) {
   const int n = c->n, tn = c->tn, nb = c->nb, ndof = 6 * nb, nrhs = ndof + nbeta;
   const double eps = 1.0;  // the probe is the modelled error itself
-  const cuDoubleComplex one = make_cuDoubleComplex(1.0, 0.0), mone = make_cuDoubleComplex(-1.0, 0.0);
   WaveDev wd = wave_dev(c, w);
-  k_probe_far<<<dim3((tn + 127) / 128, n), 128, 0, c->st>>>(c->g, c->opts.depth, c->sg_far, c->sg_cells.p, c->A.p,
-                                                            c->S.p);
-  TRY(launch_check(c));
-  // dB: the right-hand sides of the probe's S (this frequency's diffraction weights are still in wd)
+  if (!c->sg_map.p) return fail(HAMS_ERR_ARG, "surrogate judgement without its cell map");
+  TRY(c->sg_scale.alloc(2 * kJCells));
+  k_probe_scales<<<1, 256, 0, c->st>>>(c->sg_cells.p, c->sg_scale.p);
+  // dB: the right-hand sides of the probe of S (this frequency's diffraction weights are still in wd)
   const int nch = (int)c->chunks_h.size();
-  k_rhs_partial<<<dim3((tn + 127) / 128, nch), 128, 0, c->st>>>(c->g, c->S.p, c->chunks.p, c->wd.p, nbeta, c->part.p);
+  k_rhs_partial<true><<<dim3((tn + 127) / 128, nch), 128, 0, c->st>>>(c->g, c->S.p, c->chunks.p, c->wd.p, nbeta,
+                                                                      c->part.p, c->sg_map.p, c->sg_scale.p);
   k_rhs_final<<<(tn + 127) / 128, 128, 0, c->st>>>(tn, nb, nch, c->chunk_body.p, c->part.p, nbeta, c->B.p);
-  TRY(launch_check(c, 2));
-  // r = dB - dA X, then dX = (L U)^-1 r
-  CUB_(cublasZgemm(c->blas, CUBLAS_OP_N, CUBLAS_OP_N, n, nrhs, n, &mone, (cuDoubleComplex*)c->A.p, tn,
-                   (cuDoubleComplex*)c->X.p, n, &one, (cuDoubleComplex*)c->B.p, tn));
-  c->lib_calls += 1;
+  // r = dB - dA X (X rounded to complex64 in R's storage), then dX = (L U)^-1 r
   const size_t nx = (size_t)n * nrhs;
-  k_z2c<<<592, 256, 0, c->st>>>(c->B.p, c->Xf.p, nx);  // tn == n: B is n x nrhs, contiguous
-  TRY(launch_check(c));
-  TRY(mixed_apply(c, nrhs));
   TRY(c->R.alloc(nx));
+  float2* xs = reinterpret_cast<float2*>(c->R.p);
+  k_z2c<<<592, 256, 0, c->st>>>(c->X.p, xs, nx);
+  k_probe_apply<<<(tn + kPrRows - 1) / kPrRows, 256, 0, c->st>>>(c->g, c->sg_map.p, c->sg_scale.p, c->A.p, xs,
+                                                                  nrhs, c->B.p);
+  k_z2c<<<592, 256, 0, c->st>>>(c->B.p, c->Xf.p, nx);  // tn == n: B is n x nrhs, contiguous
+  TRY(launch_check(c, 6));
+  TRY(mixed_apply(c, nrhs));
   CU(cudaMemcpyAsync(c->R.p, c->X.p, nx * 16, cudaMemcpyDeviceToDevice, c->st));
   k_c2z_add<<<592, 256, 0, c->st>>>(c->Xf.p, c->R.p, nx);
   TRY(launch_check(c));
@@ -1887,6 +2004,20 @@ static int surrogate_judge(hams_ctx* c, const hams_wave* w, int nbeta) {
   return 0;
 }
 
+// A frequency the judgement gave to the series, without a new factorisation:
+// the far pairs again from the series (the near pairs of A and S are the
+// series' already), the block copies and right-hand sides again, then FP64
+// refinement from the network's solution with the network's factors -- the
+// network's matrix is within its error of the series' one, so the factors
+// are as good a preconditioner for it as for their own.  HAMS_ERR_NUMERIC
+// when the refinement stalls (the caller then factors the series' matrix).
+static int series_refine(hams_ctx* c, const hams_wave* w, int nbeta) {
+  const int nrhs = 6 * c->nb + nbeta;
+  TRY(far_series(c, wave_dev(c, w)));
+  TRY(copy_blocks_and_rhs(c, nbeta));
+  return mixed_refine(c, c->A.p, c->B.p, c->tn, nrhs);
+}
+
 static int solve_one(hams_ctx* c, const hams_wave* w, int nbeta, const double* beta, double* amas, double* bdmp,
                      double* exfc) {
   const int ndof = 6 * c->nb;
@@ -1905,14 +2036,21 @@ static int solve_one(hams_ctx* c, const hams_wave* w, int nbeta, const double* b
     TRY(surrogate_judge(c, w, nbeta));
     if (c->sg_judge[5] > c->sg_tol) {  // the series takes this frequency
       const std::string keep = c->note;
-      TRY(assemble_dev(c, w, nbeta, true));
-      TRY(solve_dev(c, ndof + nbeta, &info));
+      const char* how = "refined to the series";
+      int rc = series_refine(c, w, nbeta);
+      if (rc == HAMS_ERR_NUMERIC) {  // the refinement stalled: factor the series' matrix
+        g_err.clear();
+        how = "re-solved with the series";
+        TRY(assemble_dev(c, w, nbeta, true));
+        TRY(solve_dev(c, ndof + nbeta, &info));
+      } else if (rc) {
+        return rc;
+      }
       CU(cudaEventRecord(c->ev[3], c->st));
       TRY(forces_dev(c, w, nbeta));
       c->sg_judge[6] = 1.0;
       char buf[160];
-      std::snprintf(buf, sizeof buf, "surrogate estimate %.2e > %.2e: re-solved with the series", c->sg_judge[5],
-                    c->sg_tol);
+      std::snprintf(buf, sizeof buf, "surrogate estimate %.2e > %.2e: %s", c->sg_judge[5], c->sg_tol, how);
       c->note = keep.empty() ? std::string(buf) : keep + "; " + buf;
     }
   }
@@ -2250,6 +2388,11 @@ extern "C" int hams_ctx_set_surrogate(hams_ctx* c, const float* params, int32_t 
   }
   TRY(build_pairs(c));
   TRY(build_judge_samples(c));
+  if (c->sg_on) {
+    TRY(c->sg_map.alloc((size_t)c->tn * c->n));
+    k_probe_map<<<dim3((c->tn + 127) / 128, c->n), 128, 0, c->st>>>(c->g, c->opts.depth, c->sg_far, c->sg_map.p);
+    TRY(launch_check(c));
+  }
   int nmode = c->mt.nmode;
   if (c->bin_off[3] > c->bin_off[2] || c->bin_off[5] > c->bin_off[4]) nmode = std::max(nmode, hams::kEigenEMax + 1);
   c->mt.nmode = nmode;
@@ -2262,6 +2405,7 @@ extern "C" int hams_ctx_set_surrogate(hams_ctx* c, const float* params, int32_t 
     l->sg_kmax = c->sg_kmax;
     l->sgd = c->sgd;
     l->sg_samp.view(c->sg_samp);
+    l->sg_map.view(c->sg_map);
     l->sg_ns4 = c->sg_ns4;
     l->sg_ns5 = c->sg_ns5;
     l->mt.nmode = nmode;

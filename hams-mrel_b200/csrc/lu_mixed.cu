@@ -32,14 +32,14 @@
 // refinement checks the result, and the caller falls back to a partially
 // pivoted LU if the refinement does not converge.
 //
-// The solve (ZGETRS's part) runs as two launches of a block triangular-solve
-// kernel, one per triangle, on the diagonal-block inverses the factorisation
-// keeps: the CTA of block row b and a chunk of 16 right-hand sides subtracts
-// T_bj X_j as each earlier block's X_j is published (a flag per block and
-// chunk), then forms X_b = T_bb^-1 (B_b - sum).  CTAs take their block rows
-// from an atomic ticket in dependency order, so every block a CTA waits for
-// belongs to a CTA that is already running; each wait is bounded and a wait
-// that gives up sets an error bit.
+// The solve (ZGETRS's part) is GEMMs as well.  The factorisation ends with
+// k_panel_inverse, which forms the inverse of every panel's 256 x 256
+// diagonal block of L and of U from the inverses of its four 64 x 64 blocks
+// (one CTA per panel and triangle, written expanded and row-major).  Each
+// triangle is then one pass over the panels: X_p = T_pp^-1 Y_p (one GEMM),
+// and the rest of the right-hand sides take T's panel column times X_p (the
+// column expanded by k_expand_rm, one GEMM) -- two GEMMs per panel on the
+// full GPU, no waits between CTAs.
 #include <cublas_v2.h>
 #include <cuda_runtime.h>
 
@@ -299,146 +299,129 @@ __global__ void k_apply_perm(float2* A, int lda, int n, int k0, int nbk, const i
 }
 
 // ---------------------------------------------------------------------------
-// Block triangular solves
+// Panel inverses and the GEMM triangular solves
 // ---------------------------------------------------------------------------
-constexpr int kNC = 64;        // right-hand sides per ticket
 constexpr int kTLd = kNB + 4;  // column stride of a shared 64 x 64 block (float2; 16-byte aligned columns)
-constexpr int kXLd = kNB + 2;  // column stride of the shared right-hand sides
-constexpr int kTrsmSmem = (2 * kNB * kTLd + 2 * kNC * kXLd) * (int)sizeof(float2);
-constexpr long long kFlagSpin = 1ll << 24;
+constexpr int kPW = kPB * kNB;  // panel width (columns)
+constexpr int kPLd = 2 * kPW;   // leading dimension of an expanded panel inverse (floats)
+constexpr int kInvSmem = 6 * kNB * kTLd * (int)sizeof(float2);
 
-__device__ __forceinline__ void cmac_sub(float2& s, float2 a, float2 b) {
-  s.x -= a.x * b.x - a.y * b.y;
-  s.y -= a.x * b.y + a.y * b.x;
+__device__ __forceinline__ void cmac_add(float2& s, float2 a, float2 b) {
+  s.x += a.x * b.x - a.y * b.y;
+  s.y += a.x * b.y + a.y * b.x;
 }
 
-// T = the 64 x 64 block of A at block row b, block column j, into shared
-// memory with asynchronous 16-byte copies (zero-filled outside the n x n
-// matrix); lda is even, so every copy is 16-byte aligned.
-__device__ __forceinline__ void prefetch_block(float2* sT, const float2* __restrict__ A, int lda, int n, int b, int j) {
-  for (int e = threadIdx.x; e < kNB * kNB / 2; e += 256) {
-    const int cc = e / (kNB / 2), rr = 2 * (e % (kNB / 2)), gr = b * kNB + rr, gc = j * kNB + cc;
-    const int bytes = gc < n ? (gr + 1 < n ? 16 : (gr < n ? 8 : 0)) : 0;
-    const float2* src = bytes ? A + (size_t)gc * lda + gr : A;
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"((uint32_t)__cvta_generic_to_shared(
-                     sT + cc * kTLd + rr)),
-                 "l"(src), "r"(bytes)
-                 : "memory");
+// dst (64 x 64, column-major, ld kTLd) <- the rows x cols block at src (ld
+// lds, column-major), zero outside it.
+__device__ __forceinline__ void load_block(float2* dst, const float2* __restrict__ src, size_t lds, int rows,
+                                           int cols) {
+  for (int e = threadIdx.x; e < kNB * kNB; e += 256) {
+    const int r = e % kNB, c = e / kNB;
+    dst[c * kTLd + r] = (r < rows && c < cols) ? src[(size_t)c * lds + r] : make_float2(0.0f, 0.0f);
   }
-  asm volatile("cp.async.commit_group;" ::: "memory");
 }
 
-// One launch solves one triangle for all right-hand sides.  lower: unit L,
-// blocks in increasing order, the right-hand sides gathered through perm
-// from B; upper: U, blocks in decreasing order, B unpermuted.  X receives
-// the solution (n x nrhs, ld n).  flags (nblk x nch) and ticket start at 0.
-// The grid is small and persistent: each CTA takes tickets (a block row and
-// a chunk of 64 right-hand sides, in dependency order) until none is left,
-// so CTAs that wait for an earlier block hold few SMs.  A thread owns 4 rows
-// x 4 right-hand sides; the next off-diagonal block is copied in while the
-// current one is applied.
-__global__ void __launch_bounds__(256, 1) k_trsm_block(const float2* __restrict__ A, int lda, int n, int nrhs,
-                                                       int nblk, int nch, bool lower, const float2* __restrict__ invc,
-                                                       const int* __restrict__ perm, const float2* __restrict__ B,
-                                                       float2* X, int* flags, unsigned int* ticket, int* err) {
+// acc (this thread's 4 rows x 4 columns of a 64 x 64 product) += X Y, X and
+// Y column-major in shared memory (ld kTLd).
+__device__ __forceinline__ void block_mac(float2 (&acc)[4][4], const float2* X, const float2* Y, int r0, int c0) {
+#pragma unroll 4
+  for (int k = 0; k < kNB; ++k) {
+    const float4 t01 = *reinterpret_cast<const float4*>(X + k * kTLd + r0);
+    const float4 t23 = *reinterpret_cast<const float4*>(X + k * kTLd + r0 + 2);
+    const float2 t[4] = {make_float2(t01.x, t01.y), make_float2(t01.z, t01.w), make_float2(t23.x, t23.y),
+                         make_float2(t23.z, t23.w)};
+    float2 y[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) y[u] = Y[(c0 + u) * kTLd + k];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int u = 0; u < 4; ++u) cmac_add(acc[i][u], t[i], y[u]);
+  }
+}
+
+// The inverses of the diagonal blocks of the panels (kPW columns), from the
+// inverses of their kNB diagonal blocks: blockIdx.x the panel, blockIdx.y 0
+// the unit lower L_pp (block (i, j), i > j: -L_ii^-1 sum_{k=j..i-1} L_ik
+// Z_kj), 1 the upper U_pp (block (i, j), i < j: -U_ii^-1 sum_{k=i+1..j}
+// U_ik Z_kj), column by column of blocks.  Each is written expanded and
+// row-major (kPLd x kPLd, zero outside the panel's width): the left operand
+// of the solve's diagonal GEMM.  256 threads, kInvSmem bytes of shared memory.
+__global__ void __launch_bounds__(256, 1) k_panel_inverse(const float2* __restrict__ A, int lda, int n,
+                                                          const float2* __restrict__ invLc,
+                                                          const float2* __restrict__ invUc, float* __restrict__ invLp,
+                                                          float* __restrict__ invUp) {
   extern __shared__ __align__(16) float2 sm[];
-  float2* sT[2] = {sm, sm + kNB * kTLd};  // off-diagonal blocks, column-major
-  float2* sX = sm + 2 * kNB * kTLd;       // the published X_j of the chunk, column-major (kNC columns)
-  float2* sAcc = sX + kNC * kXLd;         // B_b - sum, the operand of the inverse
-  __shared__ int s_id, s_abort;
-  const int tid = threadIdx.x, r0 = (tid % 16) * 4, c0 = (tid / 16) * 4;
-  for (;;) {
-    __syncthreads();  // the previous ticket's shared data is no longer read
-    if (tid == 0) {
-      s_id = (int)atomicAdd(ticket, 1u);
-      s_abort = 0;
+  float2* Z[kPB];
+  for (int b = 0; b < kPB; ++b) Z[b] = sm + b * kNB * kTLd;
+  float2* sB = sm + kPB * kNB * kTLd;  // the current block of A, then the sum
+  float2* sI = sB + kNB * kTLd;         // the current diagonal-block inverse
+  const int p = blockIdx.x, tid = threadIdx.x, r0 = (tid % 16) * 4, c0 = (tid / 16) * 4;
+  const bool lower = blockIdx.y == 0;
+  const int p0 = p * kPW, pw = min(kPW, n - p0), nbk = (pw + kNB - 1) / kNB;
+  const float2* invc = lower ? invLc : invUc;
+  float* out = (lower ? invLp : invUp) + (size_t)p * kPLd * kPLd;
+  for (int e = tid; e < kPLd * kPLd / 4; e += 256) reinterpret_cast<float4*>(out)[e] = make_float4(0.f, 0.f, 0.f, 0.f);
+  auto width = [&](int b) { return min(kNB, pw - b * kNB); };
+  auto write_block = [&](const float2* zb, int bi, int bj) {
+    for (int e = tid; e < kNB * kNB; e += 256) {
+      const int r = e % kNB, c = e / kNB;
+      if (r < width(bi) && c < width(bj)) put_expanded_rm(out, kPLd, bi * kNB + r, bj * kNB + c, zb[c * kTLd + r]);
     }
+  };
+  __syncthreads();  // the zero fill before the blocks' writes
+  for (int j = 0; j < nbk; ++j) {
+    const int bj = p * kPB + j;
+    load_block(Z[j], invc + (size_t)bj * kNB * kNB, kNB, width(j), width(j));
     __syncthreads();
-    if (s_id >= nblk * nch) return;
-    const int order = s_id / nch, ch = s_id % nch;
-    const int b = lower ? order : nblk - 1 - order;
-    const int q0 = ch * kNC;
-    if (order > 0) prefetch_block(sT[0], A, lda, n, b, lower ? 0 : nblk - 1);
-    // the block's right-hand sides
-    for (int e = tid; e < kNB * kNC; e += 256) {
-      const int rr = e % kNB, q = e / kNB, gr = b * kNB + rr;
-      float2 v = make_float2(0.0f, 0.0f);
-      if (gr < n && q0 + q < nrhs) v = B[(size_t)(q0 + q) * n + (lower ? perm[gr] : gr)];
-      sAcc[q * kXLd + rr] = v;
-    }
-    __syncthreads();
-    float2 acc[4][4];
-    for (int i = 0; i < 4; ++i)
-      for (int u = 0; u < 4; ++u) acc[i][u] = sAcc[(c0 + u) * kXLd + r0 + i];
-    for (int step = 0; step < order; ++step) {
-      const int j = lower ? step : nblk - 1 - step;
-      const bool more = step + 1 < order;
-      if (more) prefetch_block(sT[(step + 1) & 1], A, lda, n, b, lower ? step + 1 : nblk - 2 - step);
-      if (tid == 0) {
-        const volatile int* f = flags + j * nch + ch;
-        long long it = 0;
-        while (*f == 0) {
-          if (++it > kFlagSpin) {
-            atomicOr(err, 2);
-            s_abort = 1;
-            break;
-          }
-          __nanosleep(64);
-        }
-        __threadfence();
+    write_block(Z[j], j, j);
+    for (int s = 1; s <= (lower ? nbk - 1 - j : j); ++s) {
+      const int i = lower ? j + s : j - s;  // the block row to form
+      float2 acc[4][4];
+#pragma unroll
+      for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int u = 0; u < 4; ++u) acc[a][u] = make_float2(0.0f, 0.0f);
+      const int ka = lower ? j : i + 1, kb = lower ? i - 1 : j;
+      for (int k = ka; k <= kb; ++k) {
+        __syncthreads();  // sB is free
+        load_block(sB, A + (size_t)(p0 + k * kNB) * lda + p0 + i * kNB, lda, width(i), width(k));
+        __syncthreads();
+        block_mac(acc, sB, Z[k], r0, c0);
       }
       __syncthreads();
-      if (s_abort) break;
-      for (int e = tid; e < kNB * kNC; e += 256) {
-        const int rr = e % kNB, q = e / kNB, gr = j * kNB + rr;
-        sX[q * kXLd + rr] =
-            (gr < n && q0 + q < nrhs) ? __ldcg(X + (size_t)(q0 + q) * n + gr) : make_float2(0.0f, 0.0f);
-      }
-      if (more) asm volatile("cp.async.wait_group 1;" ::: "memory");
-      else asm volatile("cp.async.wait_group 0;" ::: "memory");
+      for (int a = 0; a < 4; ++a)
+        for (int u = 0; u < 4; ++u) sB[(c0 + u) * kTLd + r0 + a] = acc[a][u];
+      load_block(sI, invc + (size_t)(p * kPB + i) * kNB * kNB, kNB, width(i), width(i));
       __syncthreads();
-      const float2* T = sT[step & 1];
-#pragma unroll 2
-      for (int k = 0; k < kNB; ++k) {
-        const float4 t01 = *reinterpret_cast<const float4*>(T + k * kTLd + r0);
-        const float4 t23 = *reinterpret_cast<const float4*>(T + k * kTLd + r0 + 2);
-        const float2 t[4] = {make_float2(t01.x, t01.y), make_float2(t01.z, t01.w), make_float2(t23.x, t23.y),
-                             make_float2(t23.z, t23.w)};
-        float2 x[4];
-        for (int u = 0; u < 4; ++u) x[u] = sX[(c0 + u) * kXLd + k];
-        for (int i = 0; i < 4; ++i)
-          for (int u = 0; u < 4; ++u) cmac_sub(acc[i][u], t[i], x[u]);
-      }
+      float2 z[4][4];
+#pragma unroll
+      for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int u = 0; u < 4; ++u) z[a][u] = make_float2(0.0f, 0.0f);
+      block_mac(z, sI, sB, r0, c0);
+      for (int a = 0; a < 4; ++a)
+        for (int u = 0; u < 4; ++u) Z[i][(c0 + u) * kTLd + r0 + a] = make_float2(-z[a][u].x, -z[a][u].y);
       __syncthreads();
+      write_block(Z[i], i, j);
     }
-    asm volatile("cp.async.wait_group 0;" ::: "memory");
-    // X_b = T_bb^-1 (B_b - sum)
-    for (int i = 0; i < 4; ++i)
-      for (int u = 0; u < 4; ++u) sAcc[(c0 + u) * kXLd + r0 + i] = acc[i][u];
-    const float2* inv = invc + (size_t)b * kNB * kNB;
-    for (int e = tid; e < kNB * kNB; e += 256) sT[0][(e / kNB) * kTLd + e % kNB] = inv[e];
     __syncthreads();
-    float2 out[4][4];
-    for (int i = 0; i < 4; ++i)
-      for (int u = 0; u < 4; ++u) out[i][u] = make_float2(0.0f, 0.0f);
-#pragma unroll 2
-    for (int k = 0; k < kNB; ++k) {
-      float2 t[4], x[4];
-      for (int i = 0; i < 4; ++i) t[i] = sT[0][k * kTLd + r0 + i];
-      for (int u = 0; u < 4; ++u) x[u] = sAcc[(c0 + u) * kXLd + k];
-      for (int i = 0; i < 4; ++i)
-        for (int u = 0; u < 4; ++u) cmac_sub(out[i][u], t[i], x[u]);
-    }
-    for (int i = 0; i < 4; ++i) {
-      const int row = b * kNB + r0 + i;
-      if (row < n)
-        for (int u = 0; u < 4; ++u)
-          if (q0 + c0 + u < nrhs) X[(size_t)(q0 + c0 + u) * n + row] = make_float2(-out[i][u].x, -out[i][u].y);
-    }
-    __threadfence();
-    __syncthreads();
-    if (tid == 0) atomicExch(flags + b * nch + ch, 1);  // published (also after an abandoned wait, so no CTA hangs)
   }
+}
+
+// Y (n x nrhs, ld ldy) <- rows perm of B (n x nrhs, ld n); rows n..ldy-1 zero.
+__global__ void k_gather_rows(const float2* __restrict__ B, int n, int nrhs, const int* __restrict__ perm,
+                              float2* __restrict__ Y, int ldy) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x, q = blockIdx.y;
+  if (r >= ldy || q >= nrhs) return;
+  Y[(size_t)q * ldy + r] = r < n ? B[(size_t)q * n + (perm ? perm[r] : r)] : make_float2(0.0f, 0.0f);
+}
+
+// X (n x nrhs, ld n) <- the first n rows of Y (ld ldy).
+__global__ void k_copy_rows(const float2* __restrict__ Y, int ldy, int n, int nrhs, float2* __restrict__ X) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x, q = blockIdx.y;
+  if (r >= n || q >= nrhs) return;
+  X[(size_t)q * n + r] = Y[(size_t)q * ldy + r];
 }
 
 // ---------------------------------------------------------------------------
@@ -474,16 +457,20 @@ int gemm(const Gemm& g, int m, int n, int k, float alpha, const float* A, int ld
   return s == CUBLAS_STATUS_SUCCESS ? 0 : 10 + (int)s;
 }
 
-// Workspace offsets (floats): W1 (2kNB x n, column-major), Ehat and Lhat
-// (2n x 2kNB, row-major), the expanded inverses of a panel's diagonal blocks
-// (kPB each, L^-1 row-major, U^-1 column-major), E2 (2kNB x 2kNB (kPB - 1),
-// row-major), Ebig (2n x 2kNB kPB, row-major), then the complex inverses of
-// every diagonal block (kNB x kNB each, L then U), the forward solution of
-// the solve (n x nrhs) and the solve's flags and ticket.
+// Workspace offsets (floats, each a multiple of 4): W1 (2kNB x n,
+// column-major), Ehat and Lhat (2n x 2kNB, row-major), the expanded inverses
+// of a panel's diagonal blocks (kPB each, L^-1 row-major, U^-1
+// column-major), E2 (2kNB x 2kNB (kPB - 1), row-major), Ebig (2n x 2kNB kPB,
+// row-major), the complex inverses of every diagonal block (kNB x kNB each, L
+// then U), the expanded inverses of every panel's diagonal block (kPLd x
+// kPLd each, L then U), then the solve's two right-hand-side arrays (n
+// rounded up to even x nrhs, complex).
 struct Layout {
-  size_t W1, Ehat, Lhat, invL, invU, E2, Ebig, invLc, invUc, T, flags, total;
+  size_t W1, Ehat, Lhat, invL, invU, E2, Ebig, invLc, invUc, invLp, invUp, Y, Z, total;
+  int nl;
   Layout(int n, int nrhs) {
-    const size_t K2 = 2 * kNB, nblk = (size_t)(n + kNB - 1) / kNB, nch = (size_t)(nrhs + kNC - 1) / kNC;
+    const size_t K2 = 2 * kNB, nblk = (size_t)(n + kNB - 1) / kNB, np = (size_t)(n + kPW - 1) / kPW;
+    nl = n + (n & 1);
     W1 = 0;
     Ehat = W1 + K2 * n;
     Lhat = Ehat + 2 * (size_t)n * K2;
@@ -493,9 +480,11 @@ struct Layout {
     Ebig = E2 + K2 * K2 * (kPB - 1);
     invLc = Ebig + 2 * (size_t)n * K2 * kPB;  // complex from here on; offsets stay in floats
     invUc = invLc + 2 * nblk * kNB * kNB;
-    T = invUc + 2 * nblk * kNB * kNB;
-    flags = T + 2 * (size_t)n * std::max(nrhs, 1);
-    total = flags + ((nblk * nch + 4) + 3) / 4 * 4;  // ints, one float each
+    invLp = invUc + 2 * nblk * kNB * kNB;
+    invUp = invLp + np * kPLd * kPLd;
+    Y = invUp + np * kPLd * kPLd;
+    Z = Y + 2 * (size_t)nl * std::max(nrhs, 1);
+    total = Z + 2 * (size_t)nl * std::max(nrhs, 1);
   }
 };
 
@@ -593,6 +582,13 @@ int mixed_lu_factor(cudaStream_t st, cublasHandle_t blas, bool own_gemm, cublasC
     if ((rc = gemm(g, 2 * wt, wt, 2 * pw, -1.0f, Ebig, 2 * pw, Upt, ldr, 1.0f, Att, ldr, false)))
       return code(rc, 6, pb * kPB);
   }
+  // the panels' diagonal-block inverses for the solves
+  if (cudaFuncSetAttribute(k_panel_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize, kInvSmem) != cudaSuccess)
+    return 1;
+  const int np = (n + kPW - 1) / kPW;
+  k_panel_inverse<<<dim3((unsigned)np, 2), 256, kInvSmem, st>>>(A, lda, n, invLc, invUc, ws + L.invLp, ws + L.invUp);
+  *launches += 1;
+  if (cudaGetLastError() != cudaSuccess) return 1;
   return 0;
 }
 
@@ -615,31 +611,55 @@ void mixed_lu_gemm_shapes(int n, std::vector<int>& shapes) {
   }
 }
 
-int mixed_lu_solve(cudaStream_t st, int n, int lda, int nrhs, const float2* A, const int* perm, float2* X,
-                   float2* work, int* dflag, long long* launches) {
+int mixed_lu_solve(cudaStream_t st, cublasHandle_t blas, bool own_gemm, cublasComputeType_t ct, int n, int lda,
+                   int nrhs, const float2* A, const int* perm, float2* X, float2* work, int* dflag,
+                   long long* launches, long long* lib_calls) {
   if (nrhs <= 0) return 0;
-  if (cudaFuncSetAttribute(k_trsm_block, cudaFuncAttributeMaxDynamicSharedMemorySize, kTrsmSmem) != cudaSuccess)
-    return 1;
   const Layout L(n, nrhs);
   float* ws = (float*)work;
-  const int nblk = (n + kNB - 1) / kNB, nch = (nrhs + kNC - 1) / kNC;
-  const float2* invLc = (const float2*)(ws + L.invLc);
-  const float2* invUc = (const float2*)(ws + L.invUc);
-  float2* T = (float2*)(ws + L.T);
-  int* flags = (int*)(ws + L.flags);
-  unsigned int* ticket = (unsigned int*)(flags + nblk * nch);
-  // a few CTAs: enough to overlap the block rows' sums, few enough that
-  // waiting CTAs leave the GPU to the other frequencies in flight
-  const unsigned grid = (unsigned)std::min(nblk * nch, 32);
-  // forward: T = L^-1 P X; backward: X = U^-1 T
-  if (cudaMemsetAsync(flags, 0, (size_t)(nblk * nch + 1) * sizeof(int), st) != cudaSuccess) return 1;
-  k_trsm_block<<<grid, 256, kTrsmSmem, st>>>(A, lda, n, nrhs, nblk, nch, true, invLc, perm, X, T, flags, ticket,
-                                             dflag);
+  const int nl = L.nl, ldy = 2 * nl, np = (n + kPW - 1) / kPW;
+  float2* Y = (float2*)(ws + L.Y);  // Y, then Z: n rounded up to even x nrhs, complex
+  float* Yr = ws + L.Y;  // the real views: 2 nl x nrhs, column-major
+  float* Zr = ws + L.Z;
+  float* Ebig = ws + L.Ebig;
+  Gemm g{own_gemm, blas, ct, st, dflag, launches, lib_calls};
+  auto expand = [&](int r0, int c0, int w, int kc, int lde) {
+    dim3 grid((unsigned)((w + 31) / 32), (unsigned)((kc + 31) / 32));
+    k_expand_rm<<<grid, 256, 0, st>>>(A, lda, r0, c0, w, kc, Ebig, lde);
+    *launches += 1;
+    return cudaGetLastError() == cudaSuccess;
+  };
+  const dim3 rows((unsigned)((nl + 255) / 256), (unsigned)nrhs);
+  k_gather_rows<<<rows, 256, 0, st>>>(X, n, nrhs, perm, Y, nl);  // Y = P X
+  *launches += 1;
   if (cudaGetLastError() != cudaSuccess) return 1;
-  if (cudaMemsetAsync(flags, 0, (size_t)(nblk * nch + 1) * sizeof(int), st) != cudaSuccess) return 1;
-  k_trsm_block<<<grid, 256, kTrsmSmem, st>>>(A, lda, n, nrhs, nblk, nch, false, invUc, perm, T, X, flags, ticket,
-                                             dflag);
-  if (cudaGetLastError() != cudaSuccess) return 1;
-  *launches += 2;
-  return 0;
+  int rc;
+  // forward, Z = L^-1 Y: per panel Z_p = L_pp^-1 Y_p, then Y below -= L_(below, p) Z_p
+  for (int p = 0; p < np; ++p) {
+    const int p0 = p * kPW, p1 = std::min(n, p0 + kPW), pw = p1 - p0, lde = (2 * pw + 3) / 4 * 4;
+    if ((rc = gemm(g, 2 * pw, nrhs, 2 * pw, 1.0f, ws + L.invLp + (size_t)p * kPLd * kPLd, kPLd, Yr + 2 * p0, ldy,
+                   0.0f, Zr + 2 * p0, ldy, false)))
+      return 10 + rc;
+    if (p1 < n) {
+      if (!expand(p1, p0, n - p1, pw, lde)) return 1;
+      if ((rc = gemm(g, 2 * (n - p1), nrhs, 2 * pw, -1.0f, Ebig, lde, Zr + 2 * p0, ldy, 1.0f, Yr + 2 * p1, ldy,
+                     false)))
+        return 10 + rc;
+    }
+  }
+  // backward, Y = U^-1 Z: per panel from the last, Y_p = U_pp^-1 Z_p, then Z above -= U_(above, p) Y_p
+  for (int p = np - 1; p >= 0; --p) {
+    const int p0 = p * kPW, p1 = std::min(n, p0 + kPW), pw = p1 - p0, lde = (2 * pw + 3) / 4 * 4;
+    if ((rc = gemm(g, 2 * pw, nrhs, 2 * pw, 1.0f, ws + L.invUp + (size_t)p * kPLd * kPLd, kPLd, Zr + 2 * p0, ldy,
+                   0.0f, Yr + 2 * p0, ldy, false)))
+      return 10 + rc;
+    if (p0 > 0) {
+      if (!expand(0, p0, p0, pw, lde)) return 1;
+      if ((rc = gemm(g, 2 * p0, nrhs, 2 * pw, -1.0f, Ebig, lde, Yr + 2 * p0, ldy, 1.0f, Zr, ldy, false)))
+        return 10 + rc;
+    }
+  }
+  k_copy_rows<<<dim3((unsigned)((n + 255) / 256), (unsigned)nrhs), 256, 0, st>>>(Y, nl, n, nrhs, X);
+  *launches += 1;
+  return cudaGetLastError() == cudaSuccess ? 0 : 1;
 }

@@ -26,12 +26,16 @@ inline int mixed_lu_ld(int n) { return n + (n & 1); }
 int mixed_lu_factor(cudaStream_t st, cublasHandle_t blas, bool own_gemm, cublasComputeType_t ct, int n, int lda,
                     float2* A, int* perm, float2* work, int* dinfo, long long* launches, long long* lib_calls);
 
-// X (n x nrhs, ld n) <- (P^T L U)^-1 X with the factors of mixed_lu_factor,
-// by the library's block triangular-solve kernels (one launch per triangle).
-// dflag: the error word (bit 1 set if a wait on another block gave up).
-// Returns 0 or 1 on a launch error.
-int mixed_lu_solve(cudaStream_t st, int n, int lda, int nrhs, const float2* A, const int* perm, float2* X,
-                   float2* work, int* dflag, long long* launches);
+// X (n x nrhs, ld n) <- (P^T L U)^-1 X with the factors of mixed_lu_factor:
+// per 256-column panel one GEMM with the panel's diagonal-block inverse
+// (formed by the factorisation) and one with the panel's column of L (or U)
+// for the rest, on the same GEMM as the factorisation (own_gemm: the
+// library's tcgen05 kernel; otherwise cuBLAS with compute type ct).
+// dflag: the tensor-core kernels' error word (nonzero if a pipeline wait gave
+// up).  Returns 0, 1 on a CUDA or launch error, or 10 + a GEMM's status.
+int mixed_lu_solve(cudaStream_t st, cublasHandle_t blas, bool own_gemm, cublasComputeType_t ct, int n, int lda,
+                   int nrhs, const float2* A, const int* perm, float2* X, float2* work, int* dflag,
+                   long long* launches, long long* lib_calls);
 
 // The (m, n, k) shapes of the real GEMMs mixed_lu_factor runs for order n,
 // three ints each (the input of the GEMM autotuner).

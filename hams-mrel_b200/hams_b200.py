@@ -23,7 +23,7 @@ LU_BLOCK_TF32, LU_BLOCK_EMU, LU_LIBRARY = 0, 1, 2
 SOLVER_LU, SOLVER_GMRES = 1, 2
 # The surrogate form's defaults: network for pairs farther apart than 3 source-panel sizes, over
 # the network's whole K = k0 h tanh(k0 h) domain, each frequency judged by the series against the
-# 1e-4 bar (hams_ctx_set_surrogate_tolerance) and re-solved with the series above it.
+# 1e-4 bar (hams_ctx_set_surrogate_tolerance) and taken back by the series above it.
 SURROGATE_FAR = 3.0
 SURROGATE_K_RANGE = (0.04, 40.0)
 SURROGATE_TOL = 1e-4

@@ -150,13 +150,13 @@ def combine(bodies):
 
 
 def case_c1():
-    """one cylinder R=5, T=10, 800 panels, infinite depth."""
+    """One cylinder R=5, T=10, 800 panels, infinite depth."""
     return dict(name="c1", bodies=[cylinder(5.0, 10.0, 40, 15, 5)], centres=[(0.0, 0.0, 0.0)], depth=-1.0,
                 omegas=np.linspace(0.1, 3.0, 30), betas_deg=[0.0])
 
 
 def case_c2():
-    """3 x 3 cylinders R=4, T=8 at 20 m, 600 panels each, h = 50 m."""
+    """3 x 3 cylinders R=4, T=8 at 20 m, 600 panels each (5,400), h = 50 m."""
     bodies, centres = [], []
     for iy in range(3):
         for ix in range(3):
@@ -168,7 +168,7 @@ def case_c2():
 
 
 def case_c5():
-    """BASELINE config 5: 6 x 6 cylinders R=3, T=6 at 12 m, 560 panels each (20,160), h = 40 m."""
+    """6 x 6 cylinders R=3, T=6 at 12 m, 560 panels each (20,160), h = 40 m."""
     bodies, centres = [], []
     for iy in range(6):
         for ix in range(6):
@@ -180,7 +180,7 @@ def case_c5():
 
 
 def case_c3(seed):
-    """BASELINE config 3, case `seed`: one or two random bodies, half of the cases with lids."""
+    """Heterogeneous case `seed` of 128: one or two random bodies, half of the cases with lids."""
     rng = np.random.Generator(np.random.PCG64(seed))
     nbody = 1 if rng.random() < 0.5 else 2
     lid = rng.random() < 0.5

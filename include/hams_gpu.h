@@ -289,8 +289,12 @@ int hams_ctx_set_surrogate_range(hams_ctx *ctx, double kmin, double kmax);
  * first order through the factorisation already made and the force
  * reductions, giving the estimated error of added mass, damping and
  * excitation.  When the largest (times a safety factor calibrated on the
- * 5,400-panel array) exceeds tol, the frequency is assembled again with the
- * series and re-solved; hams_last_note says so and hams_last_timings reports
+ * 5,400-panel array) exceeds tol, the series takes the frequency back: its
+ * far pairs are evaluated again with the series and the solution is refined
+ * (FP64 residuals) from the network's, with the network's factors as the
+ * preconditioner -- no second factorisation; should that refinement stall,
+ * the series' matrix is factored.  hams_last_note says which ("refined to
+ * the series" or "re-solved with the series") and hams_last_timings reports
  * the estimates.  The probe goes through the same system, so it is amplified
  * where the system amplifies: the long-wave damping (a small imaginary part
  * of large potentials) and the bands around irregular frequencies, which
@@ -312,7 +316,7 @@ int hams_ctx_set_surrogate_tolerance(hams_ctx *ctx, double tol);
  * (hams_ctx_set_surrogate_tolerance): [20] the network's sampled relative
  * error on the far-pair entries of A, [21] of S, [22..24] the estimated
  * relative error of added mass, damping and excitation, [25] the estimate
- * the decision uses, [26] 1 if the frequency was re-solved with the series,
+ * the decision uses, [26] 1 if the series took the frequency back,
  * [27] the pairs sampled.  n is the capacity of ms (28 fills all). Returns the number
  * written. */
 int hams_last_timings(hams_ctx *ctx, double *ms, int32_t n);

@@ -1,4 +1,4 @@
-"""Full-size parity of BASELINE workloads against the oracle.
+"""Full-size parity of the benchmark workloads against the oracle.
 
 The smaller parity tests (test_gpu_parity.py) use coarsened meshes; these run
 the benchmark geometries at their full panel counts, one frequency at a time,

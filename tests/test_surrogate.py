@@ -156,7 +156,7 @@ def test_surrogate_assembly_against_series_and_gain():
         for a, b in zip(got, ref[om]):
             assert rel(a, b) < 1e-4
         if t["judge_resolved"]:
-            assert t["judge_estimate"] > 1e-4 and "re-solved with the series" in mix.note()
+            assert t["judge_estimate"] > 1e-4 and "surrogate estimate" in mix.note()
             continue
         kept += 1
         assert t["pairs_surrogate"] > 0.5 * n_series
@@ -181,3 +181,34 @@ def test_surrogate_assembly_against_series_and_gain():
     for a, b in zip(again, ref[1.5]):
         assert np.array_equal(a, b)
     ctx.close()
+
+
+@pytest.mark.gpu
+def test_series_takes_back_a_frequency_without_refactoring():
+    """A frequency the judgement gives back to the series: the far pairs again from the series, then
+    refinement from the network's solution with the network's factors.  The outputs are the series'
+    (the mixed form without the network, refined to the same tolerance) to 1e-6, and the library
+    says which way it went."""
+    betas = np.radians([0.0, 45.0])
+    plain = _array_context(hams_b200.PREC_MIXED)
+    mix = _array_context(hams_b200.PREC_MIXED)
+    mix.set_surrogate(train_surrogate.load(), 3.0)
+    mix.set_surrogate_tolerance(1e-12)  # every frequency goes back to the series
+    for om in (0.5, 1.5, 2.3):
+        w = hams_b200.wave_properties(om, 50.0, 9.81)
+        ref = plain.solve_frequency(w, betas)
+        got = mix.solve_frequency(w, betas)
+        t = mix.timings()
+        assert t["judge_resolved"] and t["pairs_surrogate"] > 0
+        assert "refined to the series" in mix.note()
+        for a, b in zip(got, ref):
+            assert rel(a, b) < 1e-6
+    # a batch takes the same way frequency by frequency
+    ws = [hams_b200.wave_properties(om, 50.0, 9.81) for om in (0.5, 1.5, 2.3)]
+    ra = plain.solve_batch(ws, betas)
+    rb = mix.solve_batch(ws, betas)
+    for a, b in zip(rb, ra):
+        assert rel(a, b) < 1e-6
+    assert mix.note().count("refined to the series") == 3
+    plain.close()
+    mix.close()
