@@ -69,9 +69,10 @@ WORKLOAD = "3x3 cylinder array R=4 T=8 spacing 20 m, 5400 quad panels, depth 50 
 EIGENE_FP64_FLOPS_PER_PAIR = 44_410
 EIGENE_DRAM_BYTES_PER_PAIR = 2_381
 # DRAM bytes per pair of the surrogate kernel: ncu's dram__bytes_read.sum +
-# dram__bytes_write.sum on the 3,240-panel profiling case (642.0 MB for
-# 10,233,540 pairs), scaled to a full launch by its pair count.
-SG_DRAM_BYTES_PER_PAIR = 62.73
+# dram__bytes_write.sum on the 3,240-panel profiling case with identical body
+# blocks (125.5 MB for 3,210,660 pairs), scaled to a full launch by its pair
+# count.
+SG_DRAM_BYTES_PER_PAIR = 39.10
 
 
 # A coarser copy of the array (3,240 panels, 10.2 M far pairs) that profilers

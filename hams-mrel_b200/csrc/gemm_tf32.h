@@ -27,8 +27,10 @@ int gemm_tf32_variant(cudaStream_t st, int variant, int m, int n, int k, float a
 // class of (m, n, k) on this device (M by powers of two of 128-row tiles, N of
 // 64-column tiles, K by 128), or a size heuristic for a class not measured.
 // gemm_tf32_autotune measures the classes of the nshape shapes (m, n, k) not
-// measured yet, each on scratch operands of its largest shape (three timed
-// runs per variant on stream st), and records the fastest.  Returns 0 or 1.
+// measured yet, each on scratch operands of its largest shape (the variants
+// in turn for six rounds on stream st, each launch timed alone, the first
+// round a warm-up), and records the variant with the fastest launch.
+// Returns 0 or 1.
 int gemm_tf32_pick(int m, int n, int k);
 int gemm_tf32_autotune(cudaStream_t st, int nshape, const int* shapes);
 int gemm_tf32_tuned_count();

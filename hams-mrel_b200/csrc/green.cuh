@@ -469,6 +469,73 @@ __device__ inline double aquad(const F& f, double a, double b, double eps, int* 
   return sum;
 }
 
+// The quadrature of the LINTON branch, as a policy: one thread per pair
+// (aquad), or one warp per pair (WarpQuad: the fifteen Kronrod nodes of an
+// interval evaluated by fifteen lanes, every lane then forms the same 7- and
+// 15-point sums in the reference's order, so the bisection decisions are the
+// same on all lanes; the interval stack is in the warp's shared memory).
+struct ThreadQuad {
+  template <class F>
+  __device__ double operator()(const F& f, double a, double b, double eps, int* overflow) const {
+    return aquad(f, a, b, eps, overflow);
+  }
+};
+
+struct WarpQuad {
+  double* sa;  // kQuadStack interval bounds each, this warp's shared memory
+  double* sb;
+  int lane;
+  template <class F>
+  __device__ double operator()(const F& f, double a, double b, double eps, int* overflow) const {
+    int sp = 1;
+    double sum = 0.0;
+    if (lane == 0) {
+      sa[0] = a;
+      sb[0] = b;
+    }
+    __syncwarp();
+    while (sp > 0) {
+      --sp;
+      const double x0 = sa[sp], x1 = sb[sp], hw = (x1 - x0) / 2.0;
+      double fv = 0.0;
+      if (lane < 15) {  // Kronrod node lane + 1; the even ones are the Gauss nodes
+        const int kk = lane + 1;
+        const double c = (kk % 2 == 0) ? c_xgq[kk / 2 - 1] : c_xkq[kk - 1];
+        fv = f(0.5 * (x1 + x0 + (x1 - x0) * c));
+      }
+      double v[15];
+#pragma unroll
+      for (int k = 0; k < 15; ++k) v[k] = __shfl_sync(0xffffffffu, fv, k);
+      double gi = 0.0, gk = 0.0;
+#pragma unroll
+      for (int q = 0; q < 7; ++q) gi = gi + c_wgq[q] * hw * v[2 * q + 1];
+#pragma unroll
+      for (int kk = 1; kk <= 15; ++kk) gk = gk + c_wkq[kk - 1] * hw * v[kk - 1];
+      const double err = pow(200.0 * fabs(gk - gi), 1.5);
+      __syncwarp();  // every lane has read the interval before it is overwritten
+      if (err > eps && fabs(x0 - x1) > eps) {
+        if (sp + 2 > kQuadStack) {
+          *overflow = 1;
+          sum += gk;
+          continue;
+        }
+        const double xm = (x0 + x1) / 2.0;
+        if (lane == 0) {
+          sa[sp] = xm;  // right half below, left half on top
+          sb[sp] = x1;
+          sa[sp + 1] = x0;
+          sb[sp + 1] = xm;
+        }
+        sp += 2;
+        __syncwarp();
+      } else {
+        sum += gk;
+      }
+    }
+    return sum;
+  }
+};
+
 // SA0/DSA0/SAM/DSAM series (FinGreen3D.f90:1389-1740)
 __device__ inline double sa0(double r, double pa, double wk) {
   const double ga = 0.5772156649015328, pi = 3.141592653589793, eps = HAMS_F4(1.E-6);
@@ -523,8 +590,9 @@ __device__ inline double dsam(double r, double pa, double wvn) {
 }
 
 // COEF / DCOEF coefficient of eigenmode i (1-based), FinGreen3D.f90:1168-1388
+template <class Q>
 __device__ inline void lin_coef(int i, double r, double pa, double a, const double* __restrict__ wvn, double wk,
-                                double& cof, double& dcof, int* overflow) {
+                                double& cof, double& dcof, int* overflow, const Q& quad) {
   const double pi = 3.141592653589793, eps = HAMS_F4(1.E-6), step = 100.0;
   double dnt = pa * pa / 4.0;
   if (i == 1) {
@@ -537,8 +605,8 @@ __device__ inline void lin_coef(int i, double r, double pa, double a, const doub
     } else {
       double j0, j1, y0, y1;
       jy01b(wk * r, j0, j1, y0, y1);
-      cof = -y0 / 4.0 - aquad([=](double t) { return lin_f(1, r, wk, 1, t); }, 0.0, dnt, eps, overflow);
-      dcof = wk * y1 / 4.0 - aquad([=](double t) { return lin_f(2, r, wk, 1, t); }, 0.0, dnt, eps, overflow);
+      cof = -y0 / 4.0 - quad([=](double t) { return lin_f(1, r, wk, 1, t); }, 0.0, dnt, eps, overflow);
+      dcof = wk * y1 / 4.0 - quad([=](double t) { return lin_f(2, r, wk, 1, t); }, 0.0, dnt, eps, overflow);
     }
     return;
   }
@@ -552,10 +620,10 @@ __device__ inline void lin_coef(int i, double r, double pa, double a, const doub
   } else {
     double p1 = dnt + step;
     for (int it = 0; fabs(lin_f(1, r, km, i, p1)) > eps && it < 100000; ++it) p1 = p1 + step;
-    cof = aquad([=](double t) { return lin_f(1, r, km, i, t); }, dnt, p1, eps, overflow);
+    cof = quad([=](double t) { return lin_f(1, r, km, i, t); }, dnt, p1, eps, overflow);
     p1 = dnt + step;
     for (int it = 0; fabs(lin_f(2, r, km, i, p1)) > eps && it < 100000; ++it) p1 = p1 + step;
-    dcof = aquad([=](double t) { return lin_f(2, r, km, i, t); }, dnt, p1, eps, overflow);
+    dcof = quad([=](double t) { return lin_f(2, r, km, i, t); }, dnt, p1, eps, overflow);
   }
 }
 
@@ -565,8 +633,9 @@ __device__ __forceinline__ cplx nm_mode(double h, cplx k) {  // NM, FinGreen3D.f
   return cmk(h / 2.0 * (1.0 + q.re), h / 2.0 * q.im);
 }
 
+template <class Q = ThreadQuad>
 __device__ inline void linton(double r, double zf, double zp, double v, double wk, const double* __restrict__ wvn,
-                              double h, cplx g[3], int* overflow) {
+                              double h, cplx g[3], int* overflow, const Q& quad = Q{}) {
   const double pi = 3.141592653589793, eps = HAMS_F4(1.E-6);
   double a;
   if (v < 0.02) a = 3324.2 * (v * v * v) - 258.89 * (v * v) + 8.3958 * v + 1.3208;
@@ -582,7 +651,7 @@ __device__ inline void linton(double r, double zf, double zp, double v, double w
   g[0] = g[1] = g[2] = cmk(0.0, 0.0);
   for (int i = 1; i <= 20; ++i) {
     double cof, dcof;
-    lin_coef(i, r, pa, a, wvn, wk, cof, dcof, overflow);
+    lin_coef(i, r, pa, a, wvn, wk, cof, dcof, overflow, quad);
     cplx km = (i == 1) ? cmk(0.0, -wk) : cmk(wvn[i - 1], 0.0);
     cplx nmk = nm_mode(h, km);
     cplx c1 = ccos_(cmk(km.re * (zf + h), km.im * (zf + h)));
@@ -625,9 +694,9 @@ __device__ inline void linton(double r, double zf, double zp, double v, double w
     es2 = es2 - e1 / (4.0 * pi * (sr1 * sr1)) * dsr1z + d1 / (4.0 * pi * sr1 * pa) * dsr1z +
           dsr2z / (4.0 * pi * (sr2 * sr2));
   }
-  double q1 = aquad([=](double t) { return lin_g(1, v, r, zf, zp, h, t); }, 0.0, pa / 2.0, eps, overflow);
-  double q2 = aquad([=](double t) { return lin_g(2, v, r, zf, zp, h, t); }, 0.0, pa / 2.0, eps, overflow);
-  double q3 = aquad([=](double t) { return lin_g(3, v, r, zf, zp, h, t); }, 0.0, pa / 2.0, eps, overflow);
+  double q1 = quad([=](double t) { return lin_g(1, v, r, zf, zp, h, t); }, 0.0, pa / 2.0, eps, overflow);
+  double q2 = quad([=](double t) { return lin_g(2, v, r, zf, zp, h, t); }, 0.0, pa / 2.0, eps, overflow);
+  double q3 = quad([=](double t) { return lin_g(3, v, r, zf, zp, h, t); }, 0.0, pa / 2.0, eps, overflow);
   g[0].re = g[0].re - es0 - v / 2.0 / pi * q1;
   g[1].re = g[1].re - es1 + v / 2.0 / pi * q2;
   g[2].re = g[2].re - es2 - v / 2.0 / pi * q3;
@@ -688,6 +757,20 @@ __device__ inline grn4 fingreen3d(double xq, double xp, double yq, double yp, do
   else if constexpr (BR == kPidcock) pidcock(rr, zq, zp, v, wk, wvn, h, fg, *sc, md, overflow);
   else if constexpr (BR == kEigenE) eigene(rr, zq, zp, wk, wvn, h, fg, *sc, md, overflow);
   else eigen(rr, zq, zp, wk, wvn, h, fg, md);
+  return finish_green(fg, xpq, ypq, zq, zp, rr, r, r1, flag);
+}
+
+// FINGREEN3D of the LINTON branch with the quadrature policy quad
+// (WarpQuad: every lane of a warp calls it for the same pair).
+template <class Q>
+__device__ inline grn4 fingreen3d_linton(double xq, double xp, double yq, double yp, double zq, double zp, double v,
+                                         const double* __restrict__ wvn, double h, int flag, int* overflow,
+                                         const Q& quad) {
+  double xpq = xq - xp, ypq = yq - yp, zpq = zq + zp;
+  double rr = sqrt(xpq * xpq + ypq * ypq);
+  double r = sqrt(rr * rr + (zp - zq) * (zp - zq)), r1 = sqrt(rr * rr + zpq * zpq);
+  cplx fg[3];
+  linton(rr, zq, zp, v, wvn[0], wvn, h, fg, overflow, quad);
   return finish_green(fg, xpq, ypq, zq, zp, rr, r, r1, flag);
 }
 

@@ -3,15 +3,17 @@
 // the fifth-generation tensor cores.
 //
 // A CTA runs kWG warpgroups; each takes tiles of 128 panel pairs, one pair
-// per thread.  The first layer (4 inputs) runs in FP32 on the CUDA cores;
-// the three 128 x 128 hidden layers and the output layer run as
-// tcgen05.mma (FP16 operands, FP32 accumulation, M = 128 pairs) issued by
-// one thread of the warpgroup, with the activations of the tile and all
-// weights in shared memory in the canonical K-major layout and the
-// accumulator in tensor memory.  After each layer the warpgroup reads its
-// 128 x 128 accumulator back with tcgen05.ld (thread t owns TMEM lane t =
-// pair t), adds the bias, applies SiLU, and writes the FP16 activations over
-// the tile for the next layer.  While one warpgroup runs its epilogue the
+// per thread.  Every layer runs as tcgen05.mma (FP16 operands, FP32
+// accumulation, M = 128 pairs) issued by one thread of the warpgroup, with
+// the activations of the tile and all weights in shared memory in the
+// canonical K-major layout and the accumulator in tensor memory: the first
+// layer (4 inputs and the bias) as one K = 16 product of the inputs and
+// weights split into FP16 parts (FP32 accuracy, green_sg.h), the three
+// 128 x 128 hidden layers and the output layer as eight K = 16 products
+// plus one for the bias (a block of ones times the bias split in two).
+// After each layer the warpgroup reads its 128 x 128 accumulator back with
+// tcgen05.ld (thread t owns TMEM lane t = pair t), applies SiLU, and writes
+// the FP16 activations over the tile for the next layer.  While one warpgroup runs its epilogue the
 // other's MMAs run.  Each thread then finishes its pair in FP64: the exact
 // propagating mode (FinGreen3D.f90:311-322), the surrogate's evanescent part,
 // the point-source terms by the near/far flag, and A, S as the series kernels
@@ -31,10 +33,8 @@ namespace {
 constexpr int kWG = 3;                 // warpgroups per CTA, one 128-pair tile in flight each
 constexpr int kThreads = 128 * kWG;
 constexpr int kCols = kWG <= 2 ? 256 : 512;  // TMEM columns (power of two): 128 f32 columns per warpgroup
-constexpr int kOffAct = kSgHalves * 2;                    // activation tiles, one per warpgroup
-constexpr int kOffW0 = kOffAct + kWG * kSgOperandBytes;   // first layer, f32
-constexpr int kOffBias = kOffW0 + sg::kWidth * sg::kIn * 4;
-constexpr int kOffBar = kOffBias + ((kSgBias * 4 + 15) / 16) * 16;  // one mbarrier per warpgroup
+constexpr int kOffAct = (kSgImageBytes + 1023) / 1024 * 1024;  // activation tiles, one per warpgroup
+constexpr int kOffBar = kOffAct + kWG * kSgOperandBytes;  // one mbarrier per warpgroup
 constexpr int kOffTmem = kOffBar + 8 * kWG;                          // TMEM base written by tcgen05.alloc
 constexpr int kSmemBytes = kOffTmem + 16;
 static_assert(kCols >= 128 * kWG, "tensor memory for the accumulators");
@@ -50,6 +50,12 @@ constexpr uint32_t kIdescHidden = idesc_f16(128), kIdescOut = idesc_f16(kSgOutRo
 // offset), 8-row groups 2048 B apart (stride byte offset), version 1
 __device__ __forceinline__ uint64_t sdesc(uint32_t saddr) {
   return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)(128 >> 4) << 16) | ((uint64_t)(2048 >> 4) << 32) |
+         (1ull << 46);
+}
+// the same for the 16-column ones and bias blocks (sg_small_off): 8-row
+// groups 256 B apart
+__device__ __forceinline__ uint64_t sdesc_small(uint32_t saddr) {
+  return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)(128 >> 4) << 16) | ((uint64_t)(256 >> 4) << 32) |
          (1ull << 46);
 }
 
@@ -137,19 +143,13 @@ __global__ void __launch_bounds__(kThreads, 1) k_green_sg(DevGeom g, WaveDev w, 
                                                           const double* __restrict__ rs, const double* __restrict__ rd,
                                                           double2* __restrict__ A, double2* __restrict__ S, int* err) {
   extern __shared__ __align__(1024) unsigned char smem[];
-  const float* sW0 = reinterpret_cast<const float*>(smem + kOffW0);  // 128 x 4, column-major
-  const float* sB = reinterpret_cast<const float*>(smem + kOffBias);
   uint64_t* bars = reinterpret_cast<uint64_t*>(smem + kOffBar);
   uint32_t* tslot = reinterpret_cast<uint32_t*>(smem + kOffTmem);
   const int tid = threadIdx.x, warp = tid >> 5, wg = warp >> 2, t = tid & 127;
   {
     const uint4* src = reinterpret_cast<const uint4*>(sp.wh);
     uint4* dst = reinterpret_cast<uint4*>(smem);
-    for (int e = tid; e < kSgHalves / 8; e += kThreads) dst[e] = src[e];
-    float* w0 = reinterpret_cast<float*>(smem + kOffW0);
-    float* b = reinterpret_cast<float*>(smem + kOffBias);
-    for (int e = tid; e < sg::kWidth * sg::kIn; e += kThreads) w0[e] = sp.w0[e];
-    for (int e = tid; e < kSgBias; e += kThreads) b[e] = sp.bias[e];
+    for (int e = tid; e < kSgImageBytes / 16; e += kThreads) dst[e] = src[e];
   }
   if (tid == 0) {
     for (int k = 0; k < kWG; ++k) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&bars[k])));
@@ -207,36 +207,51 @@ __global__ void __launch_bounds__(kThreads, 1) k_green_sg(DevGeom g, WaveDev w, 
     const double X = rr / h;
     float f[sg::kIn];
     sg::features(X, (zq + h) / h, (zp + h) / h, K, f);
-    // layer 0 in FP32 into row t of the activation tile
-#pragma unroll 2
-    for (int q = 0; q < 16; ++q) {
-      uint32_t hv[4];
+    // the first layer's operand row (green_sg.h) into K columns 0..15 of the tile
+    {
+      uint32_t hv[8];
+      __half fh[sg::kIn], fl[sg::kIn];
 #pragma unroll
-      for (int e = 0; e < 4; ++e) {
-        const int o = 8 * q + 2 * e;
-        float v0 = sB[o], v1 = sB[o + 1];
-#pragma unroll
-        for (int k = 0; k < sg::kIn; ++k) {
-          v0 = fmaf(sW0[o + sg::kWidth * k], f[k], v0);
-          v1 = fmaf(sW0[o + 1 + sg::kWidth * k], f[k], v1);
-        }
-        hv[e] = pack2(silu(v0), silu(v1));
+      for (int k = 0; k < sg::kIn; ++k) {
+        fh[k] = __float2half_rn(f[k]);
+        fl[k] = __float2half_rn(f[k] - __half2float(fh[k]));
       }
-      *reinterpret_cast<uint4*>(act + sg_core_off(t, 8 * q)) = make_uint4(hv[0], hv[1], hv[2], hv[3]);
+      auto pk = [](__half a, __half b) {
+        __half2 v = __halves2half2(a, b);
+        return *reinterpret_cast<uint32_t*>(&v);
+      };
+      const __half one = __float2half_rn(1.0f), zero = __float2half_rn(0.0f);
+      hv[0] = pk(fh[0], fh[1]);
+      hv[1] = pk(fh[2], fh[3]);
+      hv[2] = pk(fl[0], fl[1]);
+      hv[3] = pk(fl[2], fl[3]);
+      hv[4] = pk(fh[0], fh[1]);
+      hv[5] = pk(fh[2], fh[3]);
+      hv[6] = pk(one, one);
+      hv[7] = pk(zero, zero);
+      *reinterpret_cast<uint4*>(act + sg_core_off(t, 0)) = make_uint4(hv[0], hv[1], hv[2], hv[3]);
+      *reinterpret_cast<uint4*>(act + sg_core_off(t, 8)) = make_uint4(hv[4], hv[5], hv[6], hv[7]);
     }
-    // layers 1..3 (N = 128) and the output layer (N = 16, three columns used)
+    // layer 0 (K = 16), layers 1..3 (N = 128) and the output layer (N = 16, three columns used)
     float y[3] = {0.0f, 0.0f, 0.0f};
     bool ok = true;
-    for (int l = 1; l <= sg::kHidden; ++l) {
+    for (int l = 0; l <= sg::kHidden; ++l) {
       proxy_fence();
       tc_fence_before();
       wg_sync(bar_id);
       if (t == 0) {
         tc_fence_after();
-        const uint32_t wb = w_sa + (uint32_t)((l - 1) * kSgOperandBytes);
-        const uint32_t id = l < sg::kHidden ? kIdescHidden : kIdescOut;
+        if (l == 0) {
+          umma_f16(tacc, sdesc(act_sa), sdesc_small(w_sa + kSgW0Off), kIdescHidden, 0);
+        } else {
+          const uint32_t wb = w_sa + (uint32_t)((l - 1) * kSgOperandBytes);
+          const uint32_t id = l < sg::kHidden ? kIdescHidden : kIdescOut;
 #pragma unroll
-        for (int s = 0; s < 8; ++s) umma_f16(tacc, sdesc(act_sa + 256 * s), sdesc(wb + 256 * s), id, s > 0);
+          for (int s = 0; s < 8; ++s) umma_f16(tacc, sdesc(act_sa + 256 * s), sdesc(wb + 256 * s), id, s > 0);
+          // + the bias: ones (128 x 16) times the layer's bias block
+          umma_f16(tacc, sdesc_small(w_sa + kSgOnesOff),
+                   sdesc_small(w_sa + (uint32_t)(kSgBiasBlkOff + (l - 1) * kSgBiasBlkBytes)), id, 1);
+        }
         umma_commit(bar);
       }
       const bool done = mbar_wait(bar, phase);
@@ -247,7 +262,6 @@ __global__ void __launch_bounds__(kThreads, 1) k_green_sg(DevGeom g, WaveDev w, 
       }
       tc_fence_after();
       if (l < sg::kHidden) {
-        const float* bl = sB + l * sg::kWidth;
 #pragma unroll 1
         for (int c = 0; c < 128; c += 32) {
           uint32_t v0[16], v1[16];
@@ -257,10 +271,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_green_sg(DevGeom g, WaveDev w, 
           uint32_t hv[16];
 #pragma unroll
           for (int e = 0; e < 8; ++e) {
-            hv[e] = pack2(silu(__uint_as_float(v0[2 * e]) + bl[c + 2 * e]),
-                          silu(__uint_as_float(v0[2 * e + 1]) + bl[c + 2 * e + 1]));
-            hv[8 + e] = pack2(silu(__uint_as_float(v1[2 * e]) + bl[c + 16 + 2 * e]),
-                              silu(__uint_as_float(v1[2 * e + 1]) + bl[c + 16 + 2 * e + 1]));
+            hv[e] = pack2(silu(__uint_as_float(v0[2 * e])), silu(__uint_as_float(v0[2 * e + 1])));
+            hv[8 + e] = pack2(silu(__uint_as_float(v1[2 * e])), silu(__uint_as_float(v1[2 * e + 1])));
           }
 #pragma unroll
           for (int q = 0; q < 4; ++q)
@@ -271,8 +283,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_green_sg(DevGeom g, WaveDev w, 
         uint32_t v[4];
         tmem_ld4(tld, v);
         tmem_wait_ld();
-        const float* bo = sB + sg::kHidden * sg::kWidth;
-        for (int k = 0; k < 3; ++k) y[k] = __uint_as_float(v[k]) + bo[k];
+        for (int k = 0; k < 3; ++k) y[k] = __uint_as_float(v[k]);
       }
     }
     if (!ok) {
@@ -331,7 +342,7 @@ void pack_surrogate(const float* P, std::vector<__half>& wh, std::vector<float>&
   // the output layer's three left zero; the layers that feed a SiLU (all but
   // the output layer) halved, so that the kernel's accumulators are z / 2
   auto scale = [](int l) { return l < sg::kLayers - 1 ? 0.5f : 1.0f; };
-  wh.assign(kSgHalves, __float2half(0.0f));
+  wh.assign(kSgImageBytes / 2, __float2half(0.0f));
   for (int l = 1; l < sg::kLayers; ++l) {
     const int fi = sg::layer_in(l), fo = sg::layer_out(l);
     __half* dst = wh.data() + (size_t)(l - 1) * (kSgOperandBytes / 2);
@@ -344,4 +355,36 @@ void pack_surrogate(const float* P, std::vector<__half>& wh, std::vector<float>&
   bias.assign(kSgBias, 0.0f);
   for (int l = 0; l < sg::kLayers; ++l)
     for (int o = 0; o < sg::layer_out(l); ++o) bias[l * sg::kWidth + o] = scale(l) * P[sg::b_off(l) + o];
+  // the ones block and the bias blocks of layers 1..3 and the output layer
+  for (int r = 0; r < 128; ++r)
+    for (int k = 0; k < 2; ++k) wh[(kSgOnesOff + sg_small_off(r, k)) / 2] = __float2half(1.0f);
+  auto split = [](float x, __half& hi, __half& lo) {
+    hi = __float2half_rn(x);
+    lo = __float2half_rn(x - __half2float(hi));
+  };
+  for (int o = 0; o < sg::kWidth; ++o) {  // the first layer's block (green_sg.h)
+    __half* row[16];
+    for (int k = 0; k < 16; ++k) row[k] = &wh[(kSgW0Off + sg_small_off(o, k)) / 2];
+    for (int k = 0; k < sg::kIn; ++k) {
+      __half hi, lo;
+      split(w0[o + sg::kWidth * k], hi, lo);
+      *row[k] = hi;
+      *row[4 + k] = hi;
+      *row[8 + k] = lo;
+    }
+    __half hi, lo;
+    split(bias[o], hi, lo);
+    *row[12] = hi;
+    *row[13] = lo;
+  }
+  for (int l = 1; l < sg::kLayers; ++l) {
+    const int off = kSgBiasBlkOff + (l - 1) * kSgBiasBlkBytes;
+    for (int o = 0; o < sg::layer_out(l); ++o) {
+      const float b = bias[l * sg::kWidth + o];
+      const __half hi = __float2half_rn(b);
+      const __half lo = __float2half_rn(b - __half2float(hi));
+      wh[(off + sg_small_off(o, 0)) / 2] = hi;
+      wh[(off + sg_small_off(o, 1)) / 2] = lo;
+    }
+  }
 }

@@ -19,13 +19,37 @@ constexpr int kSgOperandBytes = 128 * 128 * 2;
 // output layer: 16 rows (3 used) x 128
 constexpr int kSgOutRows = 16;
 constexpr int kSgOutBytes = kSgOutRows * 128 * 2;
-// hidden layers 1..3 then the output layer, as one image copied to shared memory
+// hidden layers 1..3 then the output layer
 constexpr int kSgHalves = ((sg::kHidden - 1) * kSgOperandBytes + kSgOutBytes) / 2;
 constexpr int kSgBias = sg::kHidden * sg::kWidth + 8;
+// The biases of layers 1..3 and of the output layer enter through the tensor
+// cores: one more K = 16 product per layer, a 128 x 16 block of ones (columns
+// 0 and 1 one, the rest zero) times a bias block (row o: the layer's bias o
+// split into two FP16 parts, hi = fp16(b), lo = fp16(b - hi), in columns 0
+// and 1).  These small operands use the same core matrices with 8-row groups
+// 256 bytes apart; byte offset of element (row, k < 16):
+__host__ __device__ constexpr int sg_small_off(int row, int k) {
+  return (row >> 3) * 256 + (k >> 3) * 128 + (row & 7) * 16 + (k & 7) * 2;
+}
+constexpr int kSgOnesBytes = 128 * 16 * 2;
+constexpr int kSgBiasBlkBytes = 128 * 16 * 2;        // hidden layers
+constexpr int kSgBiasOutBytes = kSgOutRows * 16 * 2;  // output layer
+constexpr int kSgOnesOff = kSgHalves * 2;             // byte offsets in the image
+constexpr int kSgBiasBlkOff = kSgOnesOff + kSgOnesBytes;
+// The first layer (4 inputs) is one K = 16 product as well, at FP32
+// accuracy from FP16 parts: the pair's row is (f_hi[0..3], f_lo[0..3],
+// f_hi[0..3], 1, 1, 0, 0) and output o's row (w_hi[0..3], w_hi[0..3],
+// w_lo[0..3], b_hi, b_lo, 0, 0), x_hi = fp16(x), x_lo = fp16(x - x_hi), so
+// that the product is w f + b up to the w_lo f_lo term (~2^-22 relative).
+constexpr int kSgW0Off = kSgBiasBlkOff + (sg::kHidden - 1) * kSgBiasBlkBytes + kSgBiasOutBytes;
+constexpr int kSgW0Bytes = 128 * 16 * 2;
+// the whole image copied to shared memory: weights, ones, bias blocks, first layer
+constexpr int kSgImageBytes = kSgW0Off + kSgW0Bytes;
+static_assert(kSgImageBytes % 16 == 0, "image copied in 16-byte pieces");
 
 // device copy of a trained network, in the kernel's layout
 struct SgDev {
-  const __half* wh;    // kSgHalves: the weight image
+  const __half* wh;    // kSgImageBytes / 2: the weight image (weights, ones, bias blocks)
   const float* w0;     // first layer, 128 x 4 column-major
   const float* bias;   // kSgBias: layer l at l * 128, output layer at 4 * 128
   double mean[sg::kOut], scale[sg::kOut];

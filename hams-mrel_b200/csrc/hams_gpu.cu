@@ -32,6 +32,7 @@
 #include <cstdio>
 #include <complex>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <thread>
 #include <string>
@@ -283,59 +284,82 @@ __global__ void k_probe_scales(const double* __restrict__ acc, double* __restric
 // B (tn x nrhs, ld tn) -= PA X with PA the error probe of A and X (n x nrhs,
 // ld n, complex64), the probe never stored; FP32 products and sums (the
 // result is an error estimate).  A block: 32 rows x 64 right-hand sides, j
-// in tiles of 32 through shared memory, each thread 2 rows x 4 right-hand
-// sides.  Grid: ceil(tn / 32) blocks of 256 threads.
-constexpr int kPrRows = 32, kPrCols = 64, kPrJ = 32;
-__global__ void __launch_bounds__(256) k_probe_apply(DevGeom g, const unsigned char* __restrict__ map,
-                                                     const double* __restrict__ scale, const double2* __restrict__ A,
-                                                     const float2* __restrict__ X, int nrhs,
-                                                     double2* __restrict__ B) {
-  __shared__ float sP[kPrJ][kPrRows];
-  __shared__ float2 sX[kPrJ][kPrCols];
+// in tiles of 32 through double-buffered shared memory, the next tile's
+// values loaded into registers while the current one is applied; each of
+// the 256 threads owns 2 rows x 4 right-hand sides.  Grid: ceil(tn / 32).
+constexpr int kPrRows = 32, kPrCols = 64, kPrJ = 32, kPrXLd = kPrCols + 2, kPrThreads = 256;
+__global__ void __launch_bounds__(kPrThreads) k_probe_apply(DevGeom g, const unsigned char* __restrict__ map,
+                                                            const double* __restrict__ scale,
+                                                            const double2* __restrict__ A,
+                                                            const float2* __restrict__ X, int nrhs,
+                                                            double2* __restrict__ B) {
+  __shared__ __align__(16) float sP[2][kPrJ][kPrRows];
+  __shared__ __align__(16) float2 sX[2][kPrJ][kPrXLd];
   __shared__ float sScale[kJCells];
   const int t = threadIdx.x, i0 = blockIdx.x * kPrRows, rg = t & 15, cg = t >> 4;
-  for (int c = t; c < kJCells; c += blockDim.x) sScale[c] = (float)scale[2 * c];
+  for (int c = t; c < kJCells; c += kPrThreads) sScale[c] = (float)scale[2 * c];
+  __syncthreads();
+  constexpr int kLP = kPrJ * kPrRows / kPrThreads, kLX = kPrJ * kPrCols / kPrThreads;  // loads per thread
+  const int il = t & 31, jq = t >> 5;  // loader roles: row il of the P tile; X tile row il, columns jq + 8 q
   for (int k0 = 0; k0 < nrhs; k0 += kPrCols) {
     float2 a[2][4];
 #pragma unroll
     for (int r = 0; r < 2; ++r)
 #pragma unroll
       for (int q = 0; q < 4; ++q) a[r][q] = make_float2(0.0f, 0.0f);
-    for (int j0 = 0; j0 < g.n; j0 += kPrJ) {
-      __syncthreads();
-      {
-        const int il = t & 31, i = i0 + il;
+    float pv[kLP];
+    float2 xv[kLX];
+    auto load = [&](int j0) {
+      const int i = i0 + il;
 #pragma unroll
-        for (int q = 0; q < kPrJ / 8; ++q) {
-          const int jl = (t >> 5) + 8 * q, j = j0 + jl;
-          float v = 0.0f;
-          if (i < g.tn && j < g.n) {
-            const size_t p = (size_t)i + (size_t)j * g.tn;
-            const unsigned char cell = map[p];
-            if (cell != kNoCell) v = sScale[cell] * (float)A[p].x;
-          }
-          sP[jl][il] = v;
+      for (int q = 0; q < kLP; ++q) {
+        const int j = j0 + jq + 8 * q;
+        float v = 0.0f;
+        if (i < g.tn && j < g.n) {
+          const size_t p = (size_t)i + (size_t)j * g.tn;
+          const unsigned char cell = map[p];
+          if (cell != kNoCell) v = sScale[cell] * (float)A[p].x;
         }
-        const int jl = t & 31, j = j0 + jl;
-#pragma unroll
-        for (int q = 0; q < kPrCols / 8; ++q) {
-          const int kl = (t >> 5) + 8 * q, k = k0 + kl;
-          sX[jl][kl] = (j < g.n && k < nrhs) ? X[(size_t)j + (size_t)k * g.n] : make_float2(0.0f, 0.0f);
-        }
+        pv[q] = v;
       }
-      __syncthreads();
+      const int j = j0 + il;
+#pragma unroll
+      for (int q = 0; q < kLX; ++q) {
+        const int k = k0 + jq + 8 * q;
+        xv[q] = (j < g.n && k < nrhs) ? X[(size_t)j + (size_t)k * g.n] : make_float2(0.0f, 0.0f);
+      }
+    };
+    auto store = [&](int buf) {
+#pragma unroll
+      for (int q = 0; q < kLP; ++q) sP[buf][jq + 8 * q][il] = pv[q];
+#pragma unroll
+      for (int q = 0; q < kLX; ++q) sX[buf][il][jq + 8 * q] = xv[q];
+    };
+    load(0);
+    store(0);
+    __syncthreads();
+    int buf = 0;
+    for (int j0 = 0; j0 < g.n; j0 += kPrJ) {
+      const bool more = j0 + kPrJ < g.n;
+      if (more) load(j0 + kPrJ);  // in flight while the current tile is applied
 #pragma unroll 8
       for (int jl = 0; jl < kPrJ; ++jl) {
-        const float p0 = sP[jl][2 * rg], p1 = sP[jl][2 * rg + 1];
+        const float2 p = *reinterpret_cast<const float2*>(&sP[buf][jl][2 * rg]);
+        const float4 x01 = *reinterpret_cast<const float4*>(&sX[buf][jl][4 * cg]);
+        const float4 x23 = *reinterpret_cast<const float4*>(&sX[buf][jl][4 * cg + 2]);
+        const float2 x[4] = {make_float2(x01.x, x01.y), make_float2(x01.z, x01.w), make_float2(x23.x, x23.y),
+                             make_float2(x23.z, x23.w)};
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
-          const float2 x = sX[jl][4 * cg + q];
-          a[0][q].x = fmaf(p0, x.x, a[0][q].x);
-          a[0][q].y = fmaf(p0, x.y, a[0][q].y);
-          a[1][q].x = fmaf(p1, x.x, a[1][q].x);
-          a[1][q].y = fmaf(p1, x.y, a[1][q].y);
+          a[0][q].x = fmaf(p.x, x[q].x, a[0][q].x);
+          a[0][q].y = fmaf(p.x, x[q].y, a[0][q].y);
+          a[1][q].x = fmaf(p.y, x[q].x, a[1][q].x);
+          a[1][q].y = fmaf(p.y, x[q].y, a[1][q].y);
         }
       }
+      if (more) store(buf ^ 1);  // the other buffer: its last readers passed the barrier below
+      __syncthreads();
+      buf ^= 1;
     }
 #pragma unroll
     for (int r = 0; r < 2; ++r) {
@@ -349,6 +373,7 @@ __global__ void __launch_bounds__(256) k_probe_apply(DevGeom g, const unsigned c
         }
       }
     }
+    __syncthreads();  // the buffers are reloaded for the next chunk of right-hand sides
   }
 }
 
@@ -375,6 +400,40 @@ __global__ void __launch_bounds__(128, BR == hams::kEigen ? 8 : 1) k_green_fin(D
     if (o) atomicOr(ovf, 1);
   }
   store_pair(g, p, i, j, G, rs, rd, A, S);
+}
+
+// The LINTON branch with one warp per pair: the pair's adaptive
+// Gauss-Kronrod integrals spread their nodes over the warp's lanes
+// (hams::WarpQuad); lane 0 stores the pair.  The branch has few pairs (the
+// panels of one vertical column of a body), each a long chain of FP64
+// quadrature, so a thread per pair leaves most of the GPU idle.  128 threads
+// per CTA, 4 pairs.
+constexpr int kLintonWarps = 4;
+__global__ void __launch_bounds__(32 * kLintonWarps) k_green_linton(DevGeom g, WaveDev w, const double* __restrict__ wvn,
+                                                                  const uint32_t* __restrict__ pairs, long long count,
+                                                                  const double* __restrict__ rs,
+                                                                  const double* __restrict__ rd,
+                                                                  double2* __restrict__ A, double2* __restrict__ S,
+                                                                  int* ovf) {
+  __shared__ double stack[kLintonWarps][2][hams::kQuadStack];
+  const int lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
+  const long long t = (long long)blockIdx.x * kLintonWarps + wl;
+  if (t >= count) return;  // the whole warp
+  size_t p = pairs[t];
+  int i = (int)(p % (size_t)g.tn), j = (int)(p / (size_t)g.tn);
+  int flag = near_flag(g, i, j);
+  double xp = g.fxyz[i], yp = g.fxyz[i + g.tn], zp = g.fxyz[i + 2 * g.tn];
+  double xq = g.xq[j], yq = g.xq[j + g.n], zq = g.xq[j + 2 * g.n];
+  grn4 G;
+  if (w.limit) {
+    G = hams::green_limit(w.limit == 2, xq, xp, yq, yp, zq, zp, flag);
+  } else {
+    int o = 0;
+    const hams::WarpQuad quad{stack[wl][0], stack[wl][1], lane};
+    G = hams::fingreen3d_linton(xq, xp, yq, yp, zq, zp, w.v, wvn, w.h, flag, &o, quad);
+    if (o && lane == 0) atomicOr(ovf, 1);
+  }
+  if (lane == 0) store_pair(g, p, i, j, G, rs, rd, A, S);
 }
 
 __global__ void __launch_bounds__(128) k_green_inf(DevGeom g, WaveDev w, const unsigned char* __restrict__ copied,
@@ -549,29 +608,26 @@ __global__ void __launch_bounds__(128) k_rhs_partial(DevGeom g, const double2* _
   int j0 = chunks[c].x, j1 = chunks[c].y;
   int nk = 6 + nbeta;
   double2* out = part + ((size_t)c * g.tn + i) * nk;
+  // one pass over the chunk's entries of S for the radiation sums and the
+  // first 8 headings (each sum in the order of j, as before), one more per
+  // further 8 headings
   double rr[6] = {0, 0, 0, 0, 0, 0}, ri[6] = {0, 0, 0, 0, 0, 0};
-  for (int j = j0; j < j1; ++j) {
-    double2 s = S[(size_t)i + (size_t)j * g.tn];
-    if (PROBE) {
-      const unsigned char cell = map[(size_t)i + (size_t)j * g.tn];
-      s = make_double2(cell != kNoCell ? scale[2 * cell + 1] * s.x : 0.0, 0.0);
-    }
-#pragma unroll
-    for (int m = 0; m < 6; ++m) {
-      double nm = g.nrm[j + (size_t)m * g.n];
-      rr[m] += s.x * nm;
-      ri[m] += s.y * nm;
-    }
-  }
-  for (int m = 0; m < 6; ++m) out[m] = make_double2(rr[m], ri[m]);
-  for (int b0 = 0; b0 < nbeta; b0 += 8) {
+  for (int b0 = 0; b0 == 0 || b0 < nbeta; b0 += 8) {
     double dr[8] = {0, 0, 0, 0, 0, 0, 0, 0}, di[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-    int nbb = min(8, nbeta - b0);
+    const int nbb = max(0, min(8, nbeta - b0));
     for (int j = j0; j < j1; ++j) {
       double2 s = S[(size_t)i + (size_t)j * g.tn];
       if (PROBE) {
         const unsigned char cell = map[(size_t)i + (size_t)j * g.tn];
         s = make_double2(cell != kNoCell ? scale[2 * cell + 1] * s.x : 0.0, 0.0);
+      }
+      if (b0 == 0) {
+#pragma unroll
+        for (int m = 0; m < 6; ++m) {
+          double nm = g.nrm[j + (size_t)m * g.n];
+          rr[m] += s.x * nm;
+          ri[m] += s.y * nm;
+        }
       }
 #pragma unroll
       for (int b = 0; b < 8; ++b)
@@ -581,6 +637,8 @@ __global__ void __launch_bounds__(128) k_rhs_partial(DevGeom g, const double2* _
           di[b] -= s.x * wv.y + s.y * wv.x;
         }
     }
+    if (b0 == 0)
+      for (int m = 0; m < 6; ++m) out[m] = make_double2(rr[m], ri[m]);
     for (int b = 0; b < nbb; ++b) out[6 + b0 + b] = make_double2(dr[b], di[b]);
   }
 }
@@ -755,6 +813,78 @@ __global__ void k_colnorm_ratio(const double2* __restrict__ r, const double2* __
 // host side
 // ---------------------------------------------------------------------------
 constexpr int kBins = 7;
+
+// The device memory of contexts and lanes comes from a process-wide cache
+// per device: a buffer a context frees (its stream synchronised) is kept and
+// handed to the next allocation of a size it fits (at most twice that size),
+// so that contexts created one after another -- a sweep of decks, the
+// heterogeneous cases, a context rebuilt for new options -- take neither
+// cudaMalloc nor cudaFree (which waits for the whole device) again.  The
+// cache holds at most a third of the device's memory; an allocation that
+// fails releases the device's cached buffers and tries once more.
+namespace devcache {
+struct Dev {
+  std::multimap<size_t, void*> free;  // bytes -> block
+  size_t cached = 0, cap = 0;
+};
+std::mutex mu;
+std::map<int, Dev> devs;
+
+inline size_t round_bytes(size_t b) { return b < (1u << 20) ? (b + 255) / 256 * 256 : (b + (2u << 20) - 1) / (2u << 20) * (2u << 20); }
+
+void* take(size_t bytes) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  const size_t want = round_bytes(bytes);
+  {
+    std::lock_guard<std::mutex> lock(mu);
+    Dev& d = devs[dev];
+    auto it = d.free.lower_bound(want);
+    if (it != d.free.end() && it->first <= 2 * want) {
+      void* p = it->second;
+      d.cached -= it->first;
+      d.free.erase(it);
+      return p;
+    }
+  }
+  void* p = nullptr;
+  if (cudaMalloc(&p, want) == cudaSuccess) return p;
+  cudaGetLastError();
+  {  // out of memory: give the cached blocks back and try once more
+    std::lock_guard<std::mutex> lock(mu);
+    Dev& d = devs[dev];
+    for (auto& f : d.free) cudaFree(f.second);
+    d.free.clear();
+    d.cached = 0;
+  }
+  p = nullptr;
+  if (cudaMalloc(&p, want) == cudaSuccess) return p;
+  cudaGetLastError();
+  return nullptr;
+}
+
+// The block p (of `bytes`, as requested from take) back to the cache; the
+// caller guarantees that no work in flight still uses it.
+void give(void* p, size_t bytes) {
+  if (!p) return;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  const size_t have = round_bytes(bytes);
+  std::lock_guard<std::mutex> lock(mu);
+  Dev& d = devs[dev];
+  if (d.cap == 0) {
+    size_t fr = 0, tot = 0;
+    d.cap = cudaMemGetInfo(&fr, &tot) == cudaSuccess ? tot / 3 : (size_t)8 << 30;
+  }
+  if (d.cached + have > d.cap) {
+    cudaFree(p);
+    return;
+  }
+  d.free.emplace(have, p);
+  d.cached += have;
+}
+}  // namespace devcache
+
 template <class T>
 struct DBuf {
   T* p = nullptr;
@@ -766,26 +896,28 @@ struct DBuf {
   ~DBuf() { release(); }
   int alloc(size_t count) {
     if (count <= n && p) return 0;
-    if (p && own) cudaFree(p);
-    p = nullptr;
-    n = 0;
-    own = true;
+    // the old block may still be in use by queued work: wait, as cudaFree did
+    if (p && own) cudaDeviceSynchronize();
+    release(true);
     if (count == 0) return 0;
-    if (cudaMalloc(&p, count * sizeof(T)) != cudaSuccess) {
-      p = nullptr;
-      return fail(HAMS_ERR_NOMEM, "cudaMalloc of %zu bytes failed", count * sizeof(T));
-    }
+    p = static_cast<T*>(devcache::take(count * sizeof(T)));
+    if (!p) return fail(HAMS_ERR_NOMEM, "cudaMalloc of %zu bytes failed", count * sizeof(T));
     n = count;
     return 0;
   }
   void view(const DBuf& o) {
-    release();
+    release(true);
     p = o.p;
     n = o.n;
     own = false;
   }
-  void release() {
-    if (p && own) cudaFree(p);
+  // idle: nothing queued uses the buffer any more (the owner's stream is
+  // synchronised); otherwise the device is synchronised first
+  void release(bool idle = false) {
+    if (p && own) {
+      if (!idle) cudaDeviceSynchronize();
+      devcache::give(p, n * sizeof(T));
+    }
     p = nullptr;
     n = 0;
     own = true;
@@ -883,6 +1015,12 @@ struct hams_ctx {
   DBuf<double2> sg_g1, sg_g2;  // the sampled A and S entries from the network, then from the series
   DBuf<unsigned char> sg_map;  // the judgement's cell of every pair the network evaluates (k_probe_map)
   DBuf<double> sg_scale;       // this frequency's probe scale per cell (k_probe_scales)
+  // the judgement's probe in the first refinement sweep: pending (requested
+  // for this solve), folded (done: dX in jdX), its right-hand sides jB
+  bool judge_pending = false, judge_folded = false;
+  int judge_nbeta = 0;
+  DBuf<double2> jB;
+  DBuf<float2> jdX;
   DBuf<double> sg_red, sg_cells, outbuf2;
   double sg_judge[8] = {};  // e_A, e_S, kappa_A, kappa_B, kappa_X, estimate, re-solved with the series, samples
   std::string note;  // what the last solve changed on its own (fallbacks), or empty
@@ -904,32 +1042,54 @@ extern "C" const char* hams_last_error(void) { return g_err.c_str(); }
 // error reporting for the other translation units of the library
 int hams_set_error(int code, const char* msg) { return fail(code, "%s", msg); }
 
+static bool handles_to_pool(hams_ctx* c);
+static void release_handle_pool();
+
+extern "C" void hams_release_cached(void) {
+  int cur = 0;
+  cudaGetDevice(&cur);
+  {
+    std::lock_guard<std::mutex> lock(devcache::mu);
+    for (auto& d : devcache::devs) {
+      cudaSetDevice(d.first);
+      for (auto& f : d.second.free) cudaFree(f.second);
+      d.second.free.clear();
+      d.second.cached = 0;
+    }
+  }
+  release_handle_pool();
+  cudaSetDevice(cur);
+}
+
 extern "C" void hams_ctx_destroy(hams_ctx* c) {
   if (!c) return;
   cudaSetDevice(c->dev);
   for (hams_ctx* l : c->lanes) hams_ctx_destroy(l);
   c->lanes.clear();
   if (c->st) cudaStreamSynchronize(c->st);
-  c->xq.release(); c->fxyz.release(); c->ds.release(); c->pnsz.release(); c->nrm.release(); c->vtx.release();
-  c->ncn.release(); c->body.release(); c->bstart.release(); c->rs.release(); c->rd.release(); c->pairs.release();
-  c->chunks.release(); c->chunk_body.release(); c->A.release(); c->S.release(); c->B.release(); c->part.release();
-  c->wd.release(); c->C.release(); c->D.release(); c->X.release(); c->R.release(); c->Af.release(); c->Xf.release();
-  c->wvn.release(); c->beta.release(); c->outbuf.release(); c->colratio.release(); c->ipiv.release();
-  c->info.release(); c->ovf.release(); c->work.release(); c->work32.release(); c->luw.release(); c->perm.release();
-  c->mt_pm.release(); c->mt_ac.release(); c->mt_fld.release(); c->mt_fldt.release(); c->mt_src.release();
-  c->mt_srct.release();
+  // the context's stream is idle: its buffers go back to the cache without a device-wide wait
+  auto rel = [](auto&... b) { (b.release(true), ...); };
+  rel(c->fp_x, c->fp_sld, c->fp_S, c->fp_D, c->fp_bc, c->fp_pot, c->fp_out, c->hxp, c->hyp, c->hw);
+  rel(c->xq, c->fxyz, c->ds, c->pnsz, c->nrm, c->vtx, c->ncn, c->body, c->bstart, c->rs, c->rd, c->pairs);
+  rel(c->blk_copied, c->blk_list, c->chunks, c->chunk_body, c->A, c->S, c->B, c->part, c->wd, c->C, c->D, c->X, c->R);
+  rel(c->Af, c->Xf, c->luw, c->gv, c->gw, c->gz, c->gy, c->gpre, c->gnrm, c->gpiv, c->perm);
+  rel(c->wvn, c->beta, c->outbuf, c->colratio, c->mt_pm, c->mt_ac, c->mt_fld, c->mt_fldt, c->mt_src, c->mt_srct);
+  rel(c->ipiv, c->info, c->ovf, c->work, c->work32, c->sg_wh, c->sg_w0, c->sg_bias, c->sg_samp, c->sg_g1, c->sg_g2);
+  rel(c->sg_map, c->sg_scale, c->jB, c->jdX, c->sg_red, c->sg_cells, c->outbuf2);
   hmat::free_dev(c->hm);
-  for (auto& e : c->ev)
-    if (e) cudaEventDestroy(e);
-  for (auto& e : c->evb)
-    if (e) cudaEventDestroy(e);
-  for (auto& e : c->marks)
-    if (e) cudaEventDestroy(e);
-  if (c->evf) cudaEventDestroy(c->evf);
-  if (c->evc) cudaEventDestroy(c->evc);
-  if (c->solver) cusolverDnDestroy(c->solver);
-  if (c->blas) cublasDestroy(c->blas);
-  if (c->st) cudaStreamDestroy(c->st);
+  if (!handles_to_pool(c)) {
+    for (auto& e : c->ev)
+      if (e) cudaEventDestroy(e);
+    for (auto& e : c->evb)
+      if (e) cudaEventDestroy(e);
+    for (auto& e : c->marks)
+      if (e) cudaEventDestroy(e);
+    if (c->evf) cudaEventDestroy(c->evf);
+    if (c->evc) cudaEventDestroy(c->evc);
+    if (c->solver) cusolverDnDestroy(c->solver);
+    if (c->blas) cublasDestroy(c->blas);
+    if (c->st) cudaStreamDestroy(c->st);
+  }
   delete c;
 }
 
@@ -1096,9 +1256,84 @@ static int ctx_frequency_buffers(hams_ctx* c) {
   return 0;
 }
 
+// Streams, library handles and events of destroyed contexts and lanes, per
+// device, for the next ones (cuBLAS and cuSOLVER handles are slow to create;
+// the library leaves their settings at the defaults except the stream, which
+// stays bound to the handle's own stream).
+struct HandleSet {
+  cudaStream_t st;
+  cublasHandle_t blas;
+  cusolverDnHandle_t solver;
+  cudaEvent_t ev[6], evb[6], marks[8], evf, evc;
+};
+static std::mutex g_hpool_mu;
+static std::map<int, std::vector<HandleSet>> g_hpool;
+constexpr size_t kHandlePoolMax = 32;  // per device
+
+static bool handles_from_pool(hams_ctx* c) {
+  std::lock_guard<std::mutex> lock(g_hpool_mu);
+  auto& v = g_hpool[c->dev];
+  if (v.empty()) return false;
+  const HandleSet h = v.back();
+  v.pop_back();
+  c->st = h.st;
+  c->blas = h.blas;
+  c->solver = h.solver;
+  for (int k = 0; k < 6; ++k) c->ev[k] = h.ev[k], c->evb[k] = h.evb[k];
+  for (int k = 0; k < 8; ++k) c->marks[k] = h.marks[k];
+  c->evf = h.evf;
+  c->evc = h.evc;
+  return true;
+}
+
+// The handles of c (its stream synchronised) back to the pool; false if the
+// pool is full (the caller destroys them).
+static bool handles_to_pool(hams_ctx* c) {
+  if (!c->st || !c->blas || !c->solver || !c->evf || !c->evc) return false;
+  for (int k = 0; k < 6; ++k)
+    if (!c->ev[k] || !c->evb[k]) return false;
+  for (int k = 0; k < 8; ++k)
+    if (!c->marks[k]) return false;
+  std::lock_guard<std::mutex> lock(g_hpool_mu);
+  auto& v = g_hpool[c->dev];
+  if (v.size() >= kHandlePoolMax) return false;
+  HandleSet h;
+  h.st = c->st;
+  h.blas = c->blas;
+  h.solver = c->solver;
+  for (int k = 0; k < 6; ++k) h.ev[k] = c->ev[k], h.evb[k] = c->evb[k];
+  for (int k = 0; k < 8; ++k) h.marks[k] = c->marks[k];
+  h.evf = c->evf;
+  h.evc = c->evc;
+  v.push_back(h);
+  return true;
+}
+
+static void release_handle_pool() {
+  std::lock_guard<std::mutex> lock(g_hpool_mu);
+  for (auto& d : g_hpool) {
+    cudaSetDevice(d.first);
+    for (auto& h : d.second) {
+      for (auto e : h.ev) cudaEventDestroy(e);
+      for (auto e : h.evb) cudaEventDestroy(e);
+      for (auto e : h.marks) cudaEventDestroy(e);
+      cudaEventDestroy(h.evf);
+      cudaEventDestroy(h.evc);
+      cusolverDnDestroy(h.solver);
+      cublasDestroy(h.blas);
+      cudaStreamDestroy(h.st);
+    }
+    d.second.clear();
+  }
+}
+
 // Stream, library handles and events of a context, on its device.
 static int ctx_handles(hams_ctx* c) {
   if (cudaSetDevice(c->dev) != cudaSuccess) return fail(HAMS_ERR_CUDA, "cudaSetDevice(%d) failed", c->dev);
+  if (handles_from_pool(c)) {
+    cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, c->dev);
+    return 0;
+  }
   if (cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking) != cudaSuccess)
     return fail(HAMS_ERR_CUDA, "stream creation failed");
   if (cublasCreate(&c->blas) != CUBLAS_STATUS_SUCCESS) return fail(HAMS_ERR_CUDA, "cublasCreate failed");
@@ -1382,7 +1617,10 @@ static int assemble_dev(hams_ctx* c, const hams_wave* w, int nbeta, bool force_s
       const uint32_t* lst = c->pairs.p + c->bin_off[br];
       unsigned blocks = (unsigned)((cnt + 127) / 128);
       switch (br) {
-        case 0: k_green_fin<0><<<blocks, 128, 0, c->st>>>(c->g, wd, c->wvn.p, c->mt, lst, cnt, c->rs.p, c->rd.p, c->A.p, c->S.p, c->ovf.p); break;
+        case 0:
+          k_green_linton<<<(unsigned)((cnt + kLintonWarps - 1) / kLintonWarps), 32 * kLintonWarps, 0, c->st>>>(
+              c->g, wd, c->wvn.p, lst, cnt, c->rs.p, c->rd.p, c->A.p, c->S.p, c->ovf.p);
+          break;
         case 1:
         case 2: launch_green_series(br, blocks, c->st, c->g, wd, c->wvn.p, c->mt, lst, cnt, c->rs.p, c->rd.p, c->A.p, c->S.p, c->ovf.p); break;
         default: k_green_fin<3><<<blocks, 128, 0, c->st>>>(c->g, wd, c->wvn.p, c->mt, lst, cnt, c->rs.p, c->rd.p, c->A.p, c->S.p, c->ovf.p); break;
@@ -1475,6 +1713,10 @@ static int mixed_apply(hams_ctx* c, int nrhs) {
   return 0;
 }
 
+// The surrogate judgement's probe right-hand sides at the solution X:
+// out (n x nrhs) = dB - dA X, xs a complex64 scratch of n x nrhs.
+static int judge_rhs(hams_ctx* c, int nbeta, const double2* X, double2* out, float2* xs);
+
 // FP64 iterative refinement of X (n x nrhs) for M X = rhs (ld ldr = n) with
 // the complex64 factors in Af: R = rhs - M X, X += (L U)^-1 R until the
 // residual of every column is below refine_tol of that column's scale.  X
@@ -1514,11 +1756,26 @@ static int mixed_refine(hams_ctx* c, const double2* M, const double2* rhs, int l
     if (it >= maxit) return fail(HAMS_ERR_NUMERIC, "iterative refinement: %.3e after %d sweeps", worst, it);
     if (it > 4 && worst > 0.5 * prev) return fail(HAMS_ERR_NUMERIC, "iterative refinement stalled at %.3e", worst);
     prev = worst;
+    // the surrogate judgement's probe rides on the first sweep: its right-hand
+    // sides dB - dA X (at this X, to first order the same estimate) go through
+    // the same solve as the residual
+    const bool fold = c->judge_pending;
+    if (fold) {
+      TRY(c->jdX.alloc(nx));
+      TRY(c->jB.alloc(nx));
+      TRY(judge_rhs(c, c->judge_nbeta, c->X.p, c->jB.p, c->jdX.p));
+    }
     k_z2c<<<592, 256, 0, c->st>>>(c->R.p, c->Xf.p, nx);
-    TRY(launch_check(c));
-    TRY(mixed_apply(c, nrhs));
+    if (fold) k_z2c<<<592, 256, 0, c->st>>>(c->jB.p, c->Xf.p + nx, nx);
+    TRY(launch_check(c, fold ? 2 : 1));
+    TRY(mixed_apply(c, fold ? 2 * nrhs : nrhs));
     k_c2z_add<<<592, 256, 0, c->st>>>(c->Xf.p, c->X.p, nx);
     TRY(launch_check(c));
+    if (fold) {
+      CU(cudaMemcpyAsync(c->jdX.p, c->Xf.p + nx, nx * sizeof(float2), cudaMemcpyDeviceToDevice, c->st));
+      c->judge_pending = false;
+      c->judge_folded = true;
+    }
   }
   return 0;
 }
@@ -1533,7 +1790,7 @@ static int mixed_solve(hams_ctx* c, double2* M, const double2* rhs, int ldr, int
   const int n = c->n, lda = mixed_lu_ld(n);
   const size_t nx = (size_t)n * nrhs;
   TRY(c->Af.alloc((size_t)lda * n));
-  TRY(c->Xf.alloc(nx));
+  TRY(c->Xf.alloc(c->judge_pending ? 2 * nx : nx));  // room for the judgement's probe in the first sweep
   TRY(c->R.alloc(nx));
   TRY(c->colratio.alloc(nrhs));
   CU(cudaMemcpy2DAsync(c->X.p, (size_t)n * 16, rhs, (size_t)ldr * 16, (size_t)n * 16, nrhs, cudaMemcpyDeviceToDevice, c->st));
@@ -1542,7 +1799,7 @@ static int mixed_solve(hams_ctx* c, double2* M, const double2* rhs, int ldr, int
   const bool block = kind != HAMS_LU_LIBRARY;
   c->lu_used = kind;
   if (block) {
-    TRY(c->luw.alloc(mixed_lu_workspace_elems(n, nrhs)));
+    TRY(c->luw.alloc(mixed_lu_workspace_elems(n, c->judge_pending ? 2 * nrhs : nrhs)));
     TRY(c->perm.alloc(n));
     long long la = 0, lb = 0;
     // TF32: the library's tcgen05 GEMM; the FP32 emulation on BF16 tensor cores is cuBLAS's
@@ -1874,6 +2131,9 @@ static int solve_dev(hams_ctx* c, int nrhs, int* info_host) {
     if (rc != HAMS_ERR_NUMERIC) return rc;
     c->note += (c->note.empty() ? "" : "; ") + std::string("block LU replaced by the library LU: ") + g_err;
     g_err.clear();
+    // a probe the block LU's sweep carried is redone with the library's factors
+    c->judge_pending = c->judge_pending || c->judge_folded;
+    c->judge_folded = false;
   }
   return mixed_solve(c, M, rhs, ldr, nrhs, HAMS_LU_LIBRARY, info_host);
 }
@@ -1945,10 +2205,8 @@ constexpr double kJudgeSafety = 1.0;
 //          to the output.
 // The estimate is kJudgeSafety times the largest of the three.  A, S and X
 // are kept, B is overwritten.  Requires the mixed solve's factors.
-static int surrogate_judge(hams_ctx* c, const hams_wave* w, int nbeta) {
-  const int n = c->n, tn = c->tn, nb = c->nb, ndof = 6 * nb, nrhs = ndof + nbeta;
-  const double eps = 1.0;  // the probe is the modelled error itself
-  WaveDev wd = wave_dev(c, w);
+static int judge_rhs(hams_ctx* c, int nbeta, const double2* X, double2* out, float2* xs) {
+  const int n = c->n, tn = c->tn, nb = c->nb, nrhs = 6 * nb + nbeta;
   if (!c->sg_map.p) return fail(HAMS_ERR_ARG, "surrogate judgement without its cell map");
   TRY(c->sg_scale.alloc(2 * kJCells));
   k_probe_scales<<<1, 256, 0, c->st>>>(c->sg_cells.p, c->sg_scale.p);
@@ -1956,19 +2214,25 @@ static int surrogate_judge(hams_ctx* c, const hams_wave* w, int nbeta) {
   const int nch = (int)c->chunks_h.size();
   k_rhs_partial<true><<<dim3((tn + 127) / 128, nch), 128, 0, c->st>>>(c->g, c->S.p, c->chunks.p, c->wd.p, nbeta,
                                                                       c->part.p, c->sg_map.p, c->sg_scale.p);
-  k_rhs_final<<<(tn + 127) / 128, 128, 0, c->st>>>(tn, nb, nch, c->chunk_body.p, c->part.p, nbeta, c->B.p);
-  // r = dB - dA X (X rounded to complex64 in R's storage), then dX = (L U)^-1 r
+  k_rhs_final<<<(tn + 127) / 128, 128, 0, c->st>>>(tn, nb, nch, c->chunk_body.p, c->part.p, nbeta, out);
+  // out = dB - dA X, X rounded to complex64 in xs
+  const size_t nx = (size_t)n * nrhs;
+  k_z2c<<<592, 256, 0, c->st>>>(X, xs, nx);
+  k_probe_apply<<<(tn + kPrRows - 1) / kPrRows, kPrThreads, 0, c->st>>>(c->g, c->sg_map.p, c->sg_scale.p, c->A.p, xs,
+                                                                         nrhs, out);
+  return launch_check(c, 5);
+}
+
+// The estimate from dX (complex64, n x nrhs): the forces of X + dX against
+// those of X (outbuf), relative per output.
+static int judge_finish(hams_ctx* c, const hams_wave* w, int nbeta, const float2* dX) {
+  const int n = c->n, nb = c->nb, ndof = 6 * nb, nrhs = ndof + nbeta;
+  const double eps = 1.0;  // the probe is the modelled error itself
+  WaveDev wd = wave_dev(c, w);
   const size_t nx = (size_t)n * nrhs;
   TRY(c->R.alloc(nx));
-  float2* xs = reinterpret_cast<float2*>(c->R.p);
-  k_z2c<<<592, 256, 0, c->st>>>(c->X.p, xs, nx);
-  k_probe_apply<<<(tn + kPrRows - 1) / kPrRows, 256, 0, c->st>>>(c->g, c->sg_map.p, c->sg_scale.p, c->A.p, xs,
-                                                                  nrhs, c->B.p);
-  k_z2c<<<592, 256, 0, c->st>>>(c->B.p, c->Xf.p, nx);  // tn == n: B is n x nrhs, contiguous
-  TRY(launch_check(c, 6));
-  TRY(mixed_apply(c, nrhs));
   CU(cudaMemcpyAsync(c->R.p, c->X.p, nx * 16, cudaMemcpyDeviceToDevice, c->st));
-  k_c2z_add<<<592, 256, 0, c->st>>>(c->Xf.p, c->R.p, nx);
+  k_c2z_add<<<592, 256, 0, c->st>>>(dX, c->R.p, nx);
   TRY(launch_check(c));
   const size_t tot = 2 * (size_t)ndof * ndof + 2 * (size_t)ndof * std::max(nbeta, 1);
   TRY(c->outbuf2.alloc(tot));
@@ -2004,6 +2268,21 @@ static int surrogate_judge(hams_ctx* c, const hams_wave* w, int nbeta) {
   return 0;
 }
 
+// The judgement after the solve.  When the mixed solve's first refinement
+// sweep already carried the probe (mixed_refine, judge_pending), dX is in
+// jdX; otherwise (no sweep was needed) the probe gets its own solve.
+static int surrogate_judge(hams_ctx* c, const hams_wave* w, int nbeta) {
+  if (c->judge_folded) return judge_finish(c, w, nbeta, c->jdX.p);
+  const int n = c->n, nrhs = 6 * c->nb + nbeta;
+  const size_t nx = (size_t)n * nrhs;
+  TRY(c->R.alloc(nx));
+  TRY(judge_rhs(c, nbeta, c->X.p, c->B.p, reinterpret_cast<float2*>(c->R.p)));
+  k_z2c<<<592, 256, 0, c->st>>>(c->B.p, c->Xf.p, nx);  // tn == n: B is n x nrhs, contiguous
+  TRY(launch_check(c));
+  TRY(mixed_apply(c, nrhs));
+  return judge_finish(c, w, nbeta, c->Xf.p);
+}
+
 // A frequency the judgement gave to the series, without a new factorisation:
 // the far pairs again from the series (the near pairs of A and S are the
 // series' already), the block copies and right-hand sides again, then FP64
@@ -2027,13 +2306,20 @@ static int solve_one(hams_ctx* c, const hams_wave* w, int nbeta, const double* b
   CU(cudaEventRecord(c->evc, c->st));
   for (double& v : c->sg_judge) v = 0.0;
   TRY(assemble_dev(c, w, nbeta));
+  const bool judged = c->sg_used && c->sg_tol > 0.0 && c->sg_ns4 + c->sg_ns5 > 0 &&
+                      c->opts.precision == HAMS_PREC_MIXED && c->opts.solver != HAMS_SOLVER_GMRES && c->nl == 0;
+  c->judge_pending = judged;
+  c->judge_folded = false;
+  c->judge_nbeta = nbeta;
   int info = 0;
-  TRY(solve_dev(c, ndof + nbeta, &info));
+  const int src = solve_dev(c, ndof + nbeta, &info);
+  c->judge_pending = false;
+  TRY(src);
   CU(cudaEventRecord(c->ev[3], c->st));
   TRY(forces_dev(c, w, nbeta));
-  if (c->sg_used && c->sg_tol > 0.0 && c->sg_ns4 + c->sg_ns5 > 0 && c->opts.precision == HAMS_PREC_MIXED &&
-      c->opts.solver != HAMS_SOLVER_GMRES && c->nl == 0) {
+  if (judged) {
     TRY(surrogate_judge(c, w, nbeta));
+    c->judge_folded = false;
     if (c->sg_judge[5] > c->sg_tol) {  // the series takes this frequency
       const std::string keep = c->note;
       const char* how = "refined to the series";

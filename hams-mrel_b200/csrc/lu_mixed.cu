@@ -457,6 +457,21 @@ int gemm(const Gemm& g, int m, int n, int k, float alpha, const float* A, int ld
   return s == CUBLAS_STATUS_SUCCESS ? 0 : 10 + (int)s;
 }
 
+// X (m x n, column-major, ld ldx, m <= 128) <- T X with T (m x m, row-major,
+// ld ldt).  The library's kernel runs it in place: C is one 128-row tile, so
+// each CTA reads its own columns of X whole (TMA) before its epilogue writes
+// them, and no two CTAs share a column.  cuBLAS gives no such guarantee, so
+// there the product goes through W (m x n, ld m) and is copied back.
+int gemm_rows_inplace(const Gemm& g, int m, int n, const float* T, int ldt, float* X, int ldx, float* W) {
+  if (g.own) return gemm(g, m, n, m, 1.0f, T, ldt, X, ldx, 0.0f, X, ldx, false);
+  int rc = gemm(g, m, n, m, 1.0f, T, ldt, X, ldx, 0.0f, W, m, false);
+  if (rc) return rc;
+  return cudaMemcpy2DAsync(X, (size_t)ldx * 4, W, (size_t)m * 4, (size_t)m * 4, n, cudaMemcpyDeviceToDevice, g.st) ==
+                 cudaSuccess
+             ? 0
+             : 1;
+}
+
 // Workspace offsets (floats, each a multiple of 4): W1 (2kNB x n,
 // column-major), Ehat and Lhat (2n x 2kNB, row-major), the expanded inverses
 // of a panel's diagonal blocks (kPB each, L^-1 row-major, U^-1
@@ -543,11 +558,8 @@ int mixed_lu_factor(cudaStream_t st, cublasHandle_t blas, bool own_gemm, cublasC
         float* Akj = Ar + (size_t)k1 * ldr + 2 * k0;  // real 2nbk x wp, ld 2 lda
         float* Aij = Ar + (size_t)k1 * ldr + 2 * k1;  // real 2wr x wp, ld 2 lda
         // U_kj = L_kk^-1 A_kj and A_ij -= L_ik U_kj inside the panel
-        if ((rc = gemm(g, k2, wp, k2, 1.0f, iL, K2, Akj, ldr, 0.0f, W1, K2, false))) return code(rc, 1, b);
-        if ((rc = gemm(g, 2 * wr, wp, k2, -1.0f, Lhat, K2, W1, K2, 1.0f, Aij, ldr, false))) return code(rc, 3, b);
-        if (cudaMemcpy2DAsync(Akj, (size_t)ldr * 4, W1, (size_t)K2 * 4, (size_t)k2 * 4, wp, cudaMemcpyDeviceToDevice,
-                              st) != cudaSuccess)
-          return 1;
+        if ((rc = gemm_rows_inplace(g, k2, wp, iL, K2, Akj, ldr, W1))) return code(rc, 1, b);
+        if ((rc = gemm(g, 2 * wr, wp, k2, -1.0f, Lhat, K2, Akj, ldr, 1.0f, Aij, ldr, false))) return code(rc, 3, b);
       }
       {  // L_ik into A
         dim3 grid((unsigned)((wr + 31) / 32), (unsigned)((nbk + 31) / 32));
@@ -569,11 +581,7 @@ int mixed_lu_factor(cudaStream_t st, cublasHandle_t blas, bool own_gemm, cublasC
         if (!expand(k0, p0, nbk, wl, E2, 2 * wl)) return 1;
         if ((rc = gemm(g, k2, wt, 2 * wl, -1.0f, E2, 2 * wl, Upt, ldr, 1.0f, Akt, ldr, false))) return code(rc, 4, b);
       }
-      if ((rc = gemm(g, k2, wt, k2, 1.0f, invL + (size_t)s * K2 * K2, K2, Akt, ldr, 0.0f, W1, K2, false)))
-        return code(rc, 5, b);
-      if (cudaMemcpy2DAsync(Akt, (size_t)ldr * 4, W1, (size_t)K2 * 4, (size_t)k2 * 4, wt, cudaMemcpyDeviceToDevice,
-                            st) != cudaSuccess)
-        return 1;
+      if ((rc = gemm_rows_inplace(g, k2, wt, invL + (size_t)s * K2 * K2, K2, Akt, ldr, W1))) return code(rc, 5, b);
     }
     // the trailing update of the whole panel at once: A_tt -= L_t,panel U_panel,t
     const int pw = p1 - p0;

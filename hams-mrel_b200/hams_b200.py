@@ -77,6 +77,8 @@ def load_library(path=LIB_PATH):
     lib.hams_wave_properties.argtypes = [c_int, c_dbl, c_dbl, c_dbl, c_int, ctypes.POINTER(HamsWave)]
     lib.hams_ctx_create.argtypes = [ctypes.POINTER(HamsGeom), ctypes.POINTER(HamsOpts), ctypes.POINTER(ctypes.c_void_p)]
     lib.hams_ctx_destroy.argtypes = [ctypes.c_void_p]
+    lib.hams_release_cached.argtypes = []
+    lib.hams_release_cached.restype = None
     lib.hams_solve_frequency.argtypes = [ctypes.c_void_p, ctypes.POINTER(HamsWave), c_int, P_dbl, P_dbl, P_dbl, P_dbl]
     lib.hams_solve_batch.argtypes = [ctypes.c_void_p, c_int, ctypes.POINTER(HamsWave), c_int, P_dbl, P_dbl, P_dbl,
                                      P_dbl]
@@ -363,6 +365,12 @@ def diag_gemm_tf32_time(m, n, k, variant=-1, reps=10, device=0):
 # ---------------------------------------------------------------------------
 def _f(a):
     return a.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+
+
+def release_cached():
+    """Give the device memory, streams and library handles that closed contexts left to the library
+    (kept for the next contexts) back to the driver."""
+    load_library().hams_release_cached()
 
 
 def surrogate_param_count():

@@ -165,7 +165,16 @@ int hams_body_blocks(const hams_geom *geo, double tol, int32_t *rep);
  * pair and sorts the pairs by Green-function branch.  Replaces the setup of
  * HAMS_Prog.f90:423-570 on the device side. */
 int hams_ctx_create(const hams_geom *geom, const hams_opts *opts, hams_ctx **out);
+/* Destroys a context and its batch lanes.  Their device buffers, streams and
+ * cuBLAS/cuSOLVER handles are kept by the library (per device, at most a
+ * third of the device's memory and 32 handle sets) for the contexts created
+ * after it, so that a sequence of contexts allocates and creates handles
+ * once; hams_release_cached returns them. */
 void hams_ctx_destroy(hams_ctx *ctx);
+/* Frees the device memory and destroys the streams and handles that destroyed
+ * contexts left to the library (no counterpart in the reference).  Call it
+ * with no context in use on the device whose memory is wanted elsewhere. */
+void hams_release_cached(void);
 
 /*
  * One frequency, all headings: the body of HAMS_Prog.f90:615-723 --
