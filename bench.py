@@ -460,7 +460,9 @@ def gpu_arm(args):
             "e2e": {"value": ws * args.steps / e2e_s, "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h,
                     "includes": "host geometry prep, context set-up (upload, Rankine tables, pair sort, surrogate "
-                                "upload) and K frequency solves through the C ABI from host buffers",
+                                "upload; device buffers, streams and library handles from the library's caches, "
+                                "which the timed context destroyed before left) and K frequency solves through "
+                                "the C ABI from host buffers",
                     "parts_rank0": {k: round(v, 4) for k, v in e2e_parts.items()}},
             "forms": forms}
     if "fp64" in forms and args.form != "fp64":

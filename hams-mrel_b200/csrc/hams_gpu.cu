@@ -409,6 +409,11 @@ __global__ void __launch_bounds__(128, BR == hams::kEigen ? 8 : 1) k_green_fin(D
 // quadrature, so a thread per pair leaves most of the GPU idle.  128 threads
 // per CTA, 4 pairs.
 constexpr int kLintonWarps = 4;
+// Below this many LINTON pairs per SM the warp-per-pair kernel runs (on the
+// 5,400-panel 3 x 3 array: 4,200 pairs with body blocks 1.5 ms against 6.5 ms
+// for a thread per pair at 0.2 rad/s; all 37,800 pairs 9.2 ms against 3.7 ms,
+// mean over frequencies).
+constexpr int kLintonWarpPairsPerSm = 64;
 __global__ void __launch_bounds__(32 * kLintonWarps) k_green_linton(DevGeom g, WaveDev w, const double* __restrict__ wvn,
                                                                   const uint32_t* __restrict__ pairs, long long count,
                                                                   const double* __restrict__ rs,
@@ -1618,8 +1623,14 @@ static int assemble_dev(hams_ctx* c, const hams_wave* w, int nbeta, bool force_s
       unsigned blocks = (unsigned)((cnt + 127) / 128);
       switch (br) {
         case 0:
-          k_green_linton<<<(unsigned)((cnt + kLintonWarps - 1) / kLintonWarps), 32 * kLintonWarps, 0, c->st>>>(
-              c->g, wd, c->wvn.p, lst, cnt, c->rs.p, c->rd.p, c->A.p, c->S.p, c->ovf.p);
+          // few pairs (body blocks): a warp per pair for latency; many: a thread per pair, whose
+          // one wave over the GPU costs less than the warps' redundant lanes
+          if (cnt < (long long)c->sms * kLintonWarpPairsPerSm)
+            k_green_linton<<<(unsigned)((cnt + kLintonWarps - 1) / kLintonWarps), 32 * kLintonWarps, 0, c->st>>>(
+                c->g, wd, c->wvn.p, lst, cnt, c->rs.p, c->rd.p, c->A.p, c->S.p, c->ovf.p);
+          else
+            k_green_fin<0><<<blocks, 128, 0, c->st>>>(c->g, wd, c->wvn.p, c->mt, lst, cnt, c->rs.p, c->rd.p, c->A.p,
+                                                      c->S.p, c->ovf.p);
           break;
         case 1:
         case 2: launch_green_series(br, blocks, c->st, c->g, wd, c->wvn.p, c->mt, lst, cnt, c->rs.p, c->rd.p, c->A.p, c->S.p, c->ovf.p); break;
