@@ -1027,7 +1027,7 @@ struct hams_ctx {
   DBuf<double2> jB;
   DBuf<float2> jdX;
   DBuf<double> sg_red, sg_cells, outbuf2;
-  double sg_judge[8] = {};  // e_A, e_S, kappa_A, kappa_B, kappa_X, estimate, re-solved with the series, samples
+  double sg_judge[8] = {};  // e_A, e_S, kappa_A, kappa_B, kappa_X, estimate, taken back by the series, samples
   std::string note;  // what the last solve changed on its own (fallbacks), or empty
   bool unfolded = false;  // built from a half mesh (ISX or ISY = 1), see unfold_symmetry
 };

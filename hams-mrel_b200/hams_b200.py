@@ -288,8 +288,8 @@ class Context:
         _check(lib.hams_ctx_set_surrogate_range(self._h, float(kmin), float(kmax)))
 
     def set_surrogate_tolerance(self, tol):
-        """The series judges each frequency the network serves; above tol the frequency is re-solved
-        with the series (0 switches the judgement off)."""
+        """The series judges each frequency the network serves; above tol the series takes the frequency
+        back (0 switches the judgement off)."""
         _check(load_library().hams_ctx_set_surrogate_tolerance(self._h, float(tol)))
 
     def set_field_points(self, xfp):

@@ -11,7 +11,7 @@ with LAPACK zgetrf/zgetrs as the solve the reference calls through MKL):
   * the 5,400-panel 3 x 3 array of cylinders in 50 m of water: the plain fp64
     form within 1e-6 and the surrogate form as the benchmark runs it
     (network far pairs over the network's whole K domain, each frequency
-    judged by the series and re-solved with it above the 1e-4 bar, identical
+    judged by the series and taken back by it above the 1e-4 bar, identical
     body blocks, complex64 panel LU with FP64 refinement) within 1e-4, at the
     lowest and highest frequencies of the sweep, one in the middle and one in
     the band before the cylinders' irregular frequency;
