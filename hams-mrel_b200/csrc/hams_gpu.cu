@@ -929,6 +929,16 @@ struct DBuf {
   }
 };
 
+// A recorded launch sequence of the block LU (opts.lu_graph): the graph of
+// one call of the factorisation or of a solve, valid while the pointers it
+// was recorded with stay the same.
+struct LuGraph {
+  cudaGraphExec_t exec = nullptr;
+  const void* key[4] = {};  // the buffers the recording used
+  int nrhs = 0;
+  long long launches = 0;
+};
+
 struct hams_ctx {
   int dev = 0;
   cudaStream_t st = nullptr;
@@ -1020,6 +1030,9 @@ struct hams_ctx {
   DBuf<double2> sg_g1, sg_g2;  // the sampled A and S entries from the network, then from the series
   DBuf<unsigned char> sg_map;  // the judgement's cell of every pair the network evaluates (k_probe_map)
   DBuf<double> sg_scale;       // this frequency's probe scale per cell (k_probe_scales)
+  // the block LU's recorded graphs (opts.lu_graph): the factorisation, the solve per right-hand-side count
+  LuGraph lu_factor_graph;
+  std::map<int, LuGraph> lu_solve_graph;
   // the judgement's probe in the first refinement sweep: pending (requested
   // for this solve), folded (done: dX in jdX), its right-hand sides jB
   bool judge_pending = false, judge_folded = false;
@@ -1072,6 +1085,9 @@ extern "C" void hams_ctx_destroy(hams_ctx* c) {
   for (hams_ctx* l : c->lanes) hams_ctx_destroy(l);
   c->lanes.clear();
   if (c->st) cudaStreamSynchronize(c->st);
+  if (c->lu_factor_graph.exec) cudaGraphExecDestroy(c->lu_factor_graph.exec);
+  for (auto& g : c->lu_solve_graph)
+    if (g.second.exec) cudaGraphExecDestroy(g.second.exec);
   // the context's stream is idle: its buffers go back to the cache without a device-wide wait
   auto rel = [](auto&... b) { (b.release(true), ...); };
   rel(c->fp_x, c->fp_sld, c->fp_S, c->fp_D, c->fp_bc, c->fp_pot, c->fp_out, c->hxp, c->hyp, c->hw);
@@ -1707,6 +1723,47 @@ static int assemble_dev(hams_ctx* c, const hams_wave* w, int nbeta, bool force_s
 }
 
 // Xf (n x nrhs) <- (L U)^-1 Xf with the factors the last mixed solve left in Af.
+// Runs body (the launches of one factorisation or solve on c->st) as a CUDA
+// graph: recorded on first use (or when the buffers moved), replayed after.
+// A recording the runtime refuses turns the option off for the context and
+// runs body directly.
+template <class F>
+static int lu_graph_run(hams_ctx* c, LuGraph& gr, const void* k0, const void* k1, const void* k2, const void* k3,
+                        int nrhs, long long* launches, F&& body) {
+  const void* key[4] = {k0, k1, k2, k3};
+  bool same = gr.exec && gr.nrhs == nrhs;
+  for (int q = 0; q < 4 && same; ++q) same = gr.key[q] == key[q];
+  if (!same) {
+    if (gr.exec) cudaGraphExecDestroy(gr.exec);
+    gr.exec = nullptr;
+    cudaGraph_t g = nullptr;
+    if (cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+      cudaGetLastError();
+      c->opts.lu_graph = 0;
+      return body(launches);
+    }
+    long long la = 0;
+    const int rc = body(&la);
+    const cudaError_t e = cudaStreamEndCapture(c->st, &g);
+    if (rc || e != cudaSuccess || !g || cudaGraphInstantiate(&gr.exec, g, 0) != cudaSuccess) {
+      if (g) cudaGraphDestroy(g);
+      cudaGetLastError();
+      gr.exec = nullptr;
+      c->opts.lu_graph = 0;  // run directly from now on
+      c->note += (c->note.empty() ? "" : "; ") + std::string("block LU graph not recorded: launched directly");
+      g_err.clear();
+      return body(launches);
+    }
+    cudaGraphDestroy(g);
+    for (int q = 0; q < 4; ++q) gr.key[q] = key[q];
+    gr.nrhs = nrhs;
+    gr.launches = la;
+  }
+  if (cudaGraphLaunch(gr.exec, c->st) != cudaSuccess) return fail(HAMS_ERR_CUDA, "block LU graph launch failed");
+  *launches += gr.launches;
+  return 0;
+}
+
 static int mixed_apply(hams_ctx* c, int nrhs) {
   const int n = c->n, lda = mixed_lu_ld(n);
   if (c->lu_used == HAMS_LU_LIBRARY) {
@@ -1716,8 +1773,18 @@ static int mixed_apply(hams_ctx* c, int nrhs) {
     return 0;
   }
   long long la = 0, lb = 0;
-  const int rc = mixed_lu_solve(c->st, c->blas, c->lu_used == HAMS_LU_BLOCK_TF32, CUBLAS_COMPUTE_32F_EMULATED_16BFX9,
-                                n, lda, nrhs, c->Af.p, c->perm.p, c->Xf.p, c->luw.p, c->info.p + 1, &la, &lb);
+  const bool own = c->lu_used == HAMS_LU_BLOCK_TF32;
+  auto body = [&](long long* l) {
+    return mixed_lu_solve(c->st, c->blas, own, CUBLAS_COMPUTE_32F_EMULATED_16BFX9, n, lda, nrhs, c->Af.p, c->perm.p,
+                          c->Xf.p, c->luw.p, c->info.p + 1, l, &lb);
+  };
+  int rc;
+  if (own && c->opts.lu_graph == 1) {
+    LuGraph& gr = c->lu_solve_graph[nrhs];
+    rc = lu_graph_run(c, gr, c->Af.p, c->perm.p, c->Xf.p, c->luw.p, nrhs, &la, body);
+  } else {
+    rc = body(&la);
+  }
   c->launches += la;
   c->lib_calls += lb;
   if (rc) return fail(HAMS_ERR_CUDA, "block LU solve failed (%d)", rc);
@@ -1815,8 +1882,13 @@ static int mixed_solve(hams_ctx* c, double2* M, const double2* rhs, int ldr, int
     long long la = 0, lb = 0;
     // TF32: the library's tcgen05 GEMM; the FP32 emulation on BF16 tensor cores is cuBLAS's
     const bool own = kind == HAMS_LU_BLOCK_TF32;
-    int rc = mixed_lu_factor(c->st, c->blas, own, CUBLAS_COMPUTE_32F_EMULATED_16BFX9, n, lda, c->Af.p, c->perm.p,
-                             c->luw.p, c->info.p, &la, &lb);
+    auto body = [&](long long* l) {
+      return mixed_lu_factor(c->st, c->blas, own, CUBLAS_COMPUTE_32F_EMULATED_16BFX9, n, lda, c->Af.p, c->perm.p,
+                             c->luw.p, c->info.p, l, &lb);
+    };
+    int rc = (own && c->opts.lu_graph == 1)
+                 ? lu_graph_run(c, c->lu_factor_graph, c->Af.p, c->perm.p, c->luw.p, c->info.p, 0, &la, body)
+                 : body(&la);
     c->launches += la;
     c->lib_calls += lb;
     if (rc == 1) return fail(HAMS_ERR_NUMERIC, "block LU: CUDA failed");

@@ -45,7 +45,7 @@ class HamsOpts(ctypes.Structure):
                 ("irsp", c_int), ("precision", c_int), ("device", c_int), ("refine_tol", c_dbl),
                 ("refine_max", c_int), ("lu_kind", c_int), ("batch_lanes", c_int),
                 ("solver", c_int), ("gmres_restart", c_int), ("gmres_maxit", c_int), ("gmres_tol", c_dbl),
-                ("aca_tol", c_dbl), ("gmres_dense", c_int), ("body_blocks", c_int), ("reserved", c_int * 2)]
+                ("aca_tol", c_dbl), ("gmres_dense", c_int), ("body_blocks", c_int), ("lu_graph", c_int), ("reserved", c_int)]
 
 
 class HamsWave(ctypes.Structure):
@@ -184,7 +184,7 @@ class Context:
     def __init__(self, geom, depth, rho=1000.0, g=9.80665, isol=1, irsp=0, precision=PREC_FP64, device=0,
                  xw=(0.0, 0.0), amp=1.0, refine_tol=0.0, refine_max=0, lu_kind=0,
                  batch_lanes=0, solver=SOLVER_LU, gmres_restart=0, gmres_maxit=0, gmres_tol=0.0, aca_tol=0.0,
-                 gmres_dense=0, body_blocks=0):
+                 gmres_dense=0, body_blocks=0, lu_graph=0):
         lib = load_library()
         self._keep = {}
         f = lambda k, dt: self._keep.setdefault(k, np.asfortranarray(geom[k], dtype=dt))
@@ -205,7 +205,8 @@ class Context:
                      precision=int(precision), device=int(device), refine_tol=float(refine_tol),
                      refine_max=int(refine_max), lu_kind=int(lu_kind), batch_lanes=int(batch_lanes), solver=int(solver),
                      gmres_restart=int(gmres_restart), gmres_maxit=int(gmres_maxit), gmres_tol=float(gmres_tol),
-                     aca_tol=float(aca_tol), gmres_dense=int(gmres_dense), body_blocks=int(body_blocks))
+                     aca_tol=float(aca_tol), gmres_dense=int(gmres_dense), body_blocks=int(body_blocks),
+                     lu_graph=int(lu_graph))
         o.xw[0], o.xw[1] = xw
         self.depth, self.g = float(depth), float(g)
         self._h = ctypes.c_void_p()

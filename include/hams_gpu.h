@@ -120,7 +120,14 @@ typedef struct hams_opts {
                        (field body, source body) block once and copy it to
                        the blocks of identical body pairs (hams_body_blocks);
                        without lids only.  0: every pair (the reference)     */
-  int32_t reserved[2];
+  int32_t lu_graph; /* mixed, HAMS_LU_BLOCK_TF32: 1 records the block LU's
+                       factorisation and triangular solves as CUDA graphs
+                       (once per frequency lane and right-hand-side count) and
+                       replays them -- a lower latency for one frequency at a
+                       time; with several frequencies in flight the replays
+                       overlap less than direct launches, so batches leave it
+                       at 0 (launched directly)                             */
+  int32_t reserved;
 } hams_opts;
 
 /* One frequency after CalWaveProperts (ImplementSubs.f90:40): V = w^2/g
