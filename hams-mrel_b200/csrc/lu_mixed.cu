@@ -12,7 +12,8 @@
 //       k_diag_lu    one CTA factors A_kk = P_k^T L_kk U_kk in shared memory
 //                    with partial pivoting inside the block, and forms
 //                    L_kk^-1 and U_kk^-1;
-//       k_apply_perm applies P_k to the rest of block row k;
+//       k_perm_expand applies P_k to the rest of block row k and expands the
+//                    block column below for the GEMMs;
 //       GEMM         L_ik = A_ik U_kk^-1 below the block, U_kj = L_kk^-1 A_kj
 //                    and A_ij -= L_ik U_kj for the panel's columns only;
 //     GEMM           the panel's U rows for the columns right of it, by
@@ -82,15 +83,19 @@ __device__ __forceinline__ float2 cmac(float2 s, float2 a, float2 b) {
   return make_float2(s.x + a.x * b.x - a.y * b.y, s.y + a.x * b.y + a.y * b.x);
 }
 
+// Barrier of one 128-thread half of the block (named barrier bar, 1 or 2).
+__device__ __forceinline__ void group_sync(int bar) { asm volatile("bar.sync %0, 128;" ::"r"(bar) : "memory"); }
+
 // Inverse of the unit lower (lower) or the upper triangle of T (kNB x kNB,
 // ld kLd) into X: the 8 x 8 diagonal blocks by substitution, then three
 // doubling levels X21 = -X22 (L21 X11) (lower) or X12 = -X11 (U12 X22)
-// (upper), each product spread over the block's 256 threads; W holds the
-// inner products of one level (at most 32 columns).
-__device__ void tri_inverse(const float2* T, float2* X, float2* W, bool lower) {
-  const int tid = threadIdx.x;
-  for (int e = tid; e < kNB * kNB; e += 256) X[(e / kNB) * kLd + e % kNB] = make_float2(0.0f, 0.0f);
-  __syncthreads();
+// (upper), each product spread over 128 threads (tid 0..127 of one half of
+// the block, synchronised by the named barrier bar, so that the two halves
+// form the two inverses at once); W holds the inner products of one level
+// (at most 32 columns).
+__device__ void tri_inverse(const float2* T, float2* X, float2* W, bool lower, int tid, int bar) {
+  for (int e = tid; e < kNB * kNB; e += 128) X[(e / kNB) * kLd + e % kNB] = make_float2(0.0f, 0.0f);
+  group_sync(bar);
   if (tid < kNB) {
     const int c = tid, b0 = c & ~7;
     if (lower) {
@@ -115,10 +120,10 @@ __device__ void tri_inverse(const float2* T, float2* X, float2* W, bool lower) {
       }
     }
   }
-  __syncthreads();
+  group_sync(bar);
   for (int sz = 8; sz < kNB; sz *= 2) {
     const int tot = (kNB / (2 * sz)) * sz * sz;
-    for (int e = tid; e < tot; e += 256) {
+    for (int e = tid; e < tot; e += 128) {
       const int q = e / (sz * sz), rem = e % (sz * sz), c = rem / sz, i = rem % sz, b0 = 2 * sz * q;
       float2 acc = make_float2(0.0f, 0.0f);
       if (lower)  // W = L21 X11
@@ -127,8 +132,8 @@ __device__ void tri_inverse(const float2* T, float2* X, float2* W, bool lower) {
         for (int k = 0; k <= c; ++k) acc = cmac(acc, T[(b0 + sz + k) * kLd + b0 + i], X[(b0 + sz + c) * kLd + b0 + sz + k]);
       W[(q * sz + c) * kLd + i] = acc;
     }
-    __syncthreads();
-    for (int e = tid; e < tot; e += 256) {
+    group_sync(bar);
+    for (int e = tid; e < tot; e += 128) {
       const int q = e / (sz * sz), rem = e % (sz * sz), c = rem / sz, i = rem % sz, b0 = 2 * sz * q;
       float2 acc = make_float2(0.0f, 0.0f);
       if (lower) {  // X21 = -X22 W
@@ -139,7 +144,7 @@ __device__ void tri_inverse(const float2* T, float2* X, float2* W, bool lower) {
         X[(b0 + sz + c) * kLd + b0 + i] = make_float2(-acc.x, -acc.y);
       }
     }
-    __syncthreads();
+    group_sync(bar);
   }
 }
 
@@ -158,7 +163,7 @@ __global__ void __launch_bounds__(256) k_diag_lu(float2* A, int lda, int k0, int
   float2* T = sm;                  // [col * kLd + row]
   float2* X = sm + kNB * kLd;      // L^-1
   float2* Y = sm + 2 * kNB * kLd;  // U^-1
-  float2* W = sm + 3 * kNB * kLd;  // inversion scratch (32 columns)
+  float2* W = sm + 3 * kNB * kLd;  // inversion scratch (32 columns for each inverse)
   __shared__ int piv[kNB];
   __shared__ int prm[kNB];
   const int tid = threadIdx.x, tx = tid % 16, ty = tid / 16;
@@ -237,8 +242,12 @@ __global__ void __launch_bounds__(256) k_diag_lu(float2* A, int lda, int k0, int
       prm[piv[j]] = t;
     }
   }
-  tri_inverse(T, X, W, true);
-  tri_inverse(T, Y, W, false);
+  __syncthreads();  // the factors and prm are complete
+  if (tid < 128)
+    tri_inverse(T, X, W, true, tid, 1);
+  else
+    tri_inverse(T, Y, W + 32 * kLd, false, tid - 128, 2);
+  __syncthreads();
   for (int e = tid; e < nbk * nbk; e += 256) {
     int r = e % nbk, c = e / nbk;
     A[(size_t)(k0 + c) * lda + k0 + r] = T[c * kLd + r];
@@ -284,18 +293,36 @@ __global__ void __launch_bounds__(256) k_extract_l(const float* __restrict__ Lha
     if (i0 + tx < wr && c0 + c < nbk) A[(size_t)(k0 + c0 + c) * lda + k1 + i0 + tx] = tile[tx][c];
 }
 
-// Rows k0..k0+nbk-1 of every column outside the diagonal block take the
-// block's permutation: row k0+i receives old row perm[k0+i].
-__global__ void k_apply_perm(float2* A, int lda, int n, int k0, int nbk, const int* __restrict__ perm) {
+// Two independent steps after a diagonal block, in one launch of 256-thread
+// blocks.  The first pblocks blocks: rows k0..k0+nbk-1 of every column
+// outside the diagonal block take the block's permutation (row k0+i receives
+// old row perm[k0+i]).  The others: Ehat (2wr x 2nbk, row-major, ld lde) <-
+// the real expansion of the block column below the diagonal block (rows
+// k0+nbk.., columns k0..k0+nbk-1), as k_expand_rm.  The permutation writes
+// only rows of the diagonal block outside its columns, the expansion reads
+// only its columns below it.
+__global__ void __launch_bounds__(256) k_perm_expand(float2* A, int lda, int n, int k0, int nbk,
+                                                     const int* __restrict__ perm, int pblocks, int wr,
+                                                     float* __restrict__ E, int lde) {
   __shared__ float2 tile[kNB][33];
-  const int c0 = blockIdx.x * 32, tx = threadIdx.x % 32, ty = threadIdx.x / 32;  // 256 threads: 8 x 32
-  const int c = c0 + tx;
-  const bool live = c < n && (c < k0 || c >= k0 + nbk);
-  for (int i = ty; i < nbk; i += 8)
-    if (live) tile[i][tx] = A[(size_t)c * lda + perm[k0 + i]];
+  const int tx = threadIdx.x % 32, ty = threadIdx.x / 32;  // 8 x 32
+  if ((int)blockIdx.x < pblocks) {
+    const int c = blockIdx.x * 32 + tx;
+    const bool live = c < n && (c < k0 || c >= k0 + nbk);
+    for (int i = ty; i < nbk; i += 8)
+      if (live) tile[i][tx] = A[(size_t)c * lda + perm[k0 + i]];
+    __syncthreads();
+    for (int i = ty; i < nbk; i += 8)
+      if (live) A[(size_t)c * lda + k0 + i] = tile[i][tx];
+    return;
+  }
+  const int b = blockIdx.x - pblocks, nbx = (wr + 31) / 32, r0 = k0 + nbk;
+  const int i0 = (b % nbx) * 32, q0 = (b / nbx) * 32;
+  for (int c = ty; c < 32; c += 8)
+    if (i0 + tx < wr && q0 + c < nbk) tile[c][tx] = A[(size_t)(k0 + q0 + c) * lda + r0 + i0 + tx];
   __syncthreads();
-  for (int i = ty; i < nbk; i += 8)
-    if (live) A[(size_t)c * lda + k0 + i] = tile[i][tx];
+  for (int r = ty; r < 32; r += 8)
+    if (i0 + r < wr && q0 + tx < nbk) put_expanded_rm(E, lde, i0 + r, q0 + tx, tile[tx][r]);
 }
 
 // ---------------------------------------------------------------------------
@@ -509,7 +536,7 @@ size_t mixed_lu_workspace_elems(int n, int nrhs) { return Layout(n, nrhs).total 
 
 int mixed_lu_factor(cudaStream_t st, cublasHandle_t blas, bool own_gemm, cublasComputeType_t ct, int n, int lda,
                     float2* A, int* perm, float2* work, int* dinfo, long long* launches, long long* lib_calls) {
-  const int smem = (3 * kNB + 32) * kLd * (int)sizeof(float2);
+  const int smem = (3 * kNB + 64) * kLd * (int)sizeof(float2);  // T, L^-1, U^-1, two 32-column scratches
   if (cudaFuncSetAttribute(k_diag_lu, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess) return 1;
   if (lda < n || (lda & 1)) return 1;
   const int K2 = 2 * kNB, PW = kPB * kNB;
@@ -547,11 +574,13 @@ int mixed_lu_factor(cudaStream_t st, cublasHandle_t blas, bool own_gemm, cublasC
       float* iU = invU + (size_t)s * K2 * K2;
       k_diag_lu<<<1, 256, smem, st>>>(A, lda, k0, nbk, perm, iL, iU, invLc + (size_t)b * kNB * kNB,
                                       invUc + (size_t)b * kNB * kNB, dinfo);
-      k_apply_perm<<<(n + 31) / 32, 256, 0, st>>>(A, lda, n, k0, nbk, perm);
+      {  // the block's permutation and the expansion of its column below, one launch
+        const int pb = (n + 31) / 32, nex = wr > 0 ? ((wr + 31) / 32) * ((nbk + 31) / 32) : 0;
+        k_perm_expand<<<pb + nex, 256, 0, st>>>(A, lda, n, k0, nbk, perm, pb, wr, Ehat, K2);
+      }
       *launches += 2;
       if (cudaGetLastError() != cudaSuccess) return 1;
       if (wr <= 0) break;
-      if (!expand(k1, k0, wr, nbk, Ehat, K2)) return 1;
       // L_ik^ = A_ik^ U_kk^-1^ (row-major: the left operand of the update below)
       if ((rc = gemm(g, 2 * wr, k2, k2, 1.0f, Ehat, K2, iU, K2, 0.0f, Lhat, K2, true))) return code(rc, 2, b);
       if (wp > 0) {
